@@ -1,0 +1,234 @@
+/*
+ * simox_gpu.h -- C ABI of the B200 force / charge / integrate path for SIMOX.
+ *
+ * Drop-in boundary for the per-step subroutines that SIMOX's Fortran main loop
+ * (main.f90:29-34 start-up, main.f90:41-61 regular loop, main.f90:63-84
+ * oxidation loop) calls by reference.  Every entry point below names the
+ * reference subroutine it replaces.  A Fortran ISO_C_BINDING shim with the same
+ * subroutine names copies the PTCL array of derived types field-wise into the
+ * plain arrays used here (the reference types are not BIND(C)).
+ *
+ * Conventions
+ *  - Every function returns an int status: SIMOX_OK (0) or a negative
+ *    SIMOX_E_* code.  simox_status_string() gives the text, and for the codes
+ *    that correspond to a reference STOP the text is that STOP message.
+ *  - Atom arrays are in the caller's (original) atom order, 0-based.
+ *    Vectors (positions, velocities, forces) are interleaved [n][3] doubles,
+ *    i.e. q(i)%xx(1:3) of the reference stored contiguously per atom.
+ *  - Species ids are the reference's: Al=1, Ni=2, Fe=3, O=4, H=5.
+ *  - Units are the reference's: Angstrom, eV, amu, e, time unit 10.1805 fs.
+ *  - A context owns device-resident state (positions, velocities, forces,
+ *    charges, cell lists, PME grids) and one CUDA stream.  Contexts are not
+ *    thread-safe, like the reference's serial code.
+ *  - Energies are accumulated in FP64 in both precision modes.
+ */
+#ifndef SIMOX_GPU_H
+#define SIMOX_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- limits and constants (datafmt.f90:20-31) -------------------------- */
+#define SIMOX_NATOM   5     /* Al, Ni, Fe, O, H                 datafmt.f90:29 */
+#define SIMOX_NMETAL  3     /* Al, Ni, Fe                       datafmt.f90:30 */
+#define SIMOX_NRDF    200   /* radial distribution bins         datafmt.f90:31 */
+#define SIMOX_NPT_MAX 500   /* reference per-cell atom limit    datafmt.f90:20 */
+#define SIMOX_NNB_MAX 500   /* reference per-atom neighbour limit datafmt.f90:22 */
+/* RDF histogram: rdf[(id_i-1) + 5*(id_j-1) + 25*bin], bin = INT(r/dr) in
+ * [0, SIMOX_NRDF+1]; the Fortran array pair%rdf(5,5,201) is the same memory
+ * shifted by one bin (Fortran index k <-> C bin k). */
+#define SIMOX_RDF_LEN (SIMOX_NATOM * SIMOX_NATOM * (SIMOX_NRDF + 2))
+
+/* ---- status codes ------------------------------------------------------ */
+#define SIMOX_OK                 0
+#define SIMOX_E_ARG             -1  /* bad argument / null pointer */
+#define SIMOX_E_CUDA            -2  /* CUDA runtime or cuFFT failure */
+#define SIMOX_E_NOMEM           -3  /* device allocation failed */
+#define SIMOX_E_CELL_OVERFLOW   -4  /* "=== Cell particle limit crashed !!! ===" cellsort.f90:75 */
+#define SIMOX_E_NBR_OVERFLOW    -5  /* "=== neighbor particle limit crashed !!! === " ctip.f90:153 / force.f90:79 */
+#define SIMOX_E_UNKNOWN_PAIR    -6  /* "=== Unknown particle pair ===" force.f90:73 */
+#define SIMOX_E_UNKNOWN_ELEMENT -7  /* "# Unknown element" force.f90:346 */
+#define SIMOX_E_BRENT           -8  /* "# **** Brent solver limit breached *** " ctip.f90:302 */
+#define SIMOX_E_CELL_TOO_SMALL  -9  /* "==== Error - unitcell is too small ..." main.f90:271 */
+#define SIMOX_E_CAPACITY       -10  /* more atoms than the context was created for */
+#define SIMOX_E_POSITION       -11  /* a coordinate is not finite or far outside the box */
+#define SIMOX_E_CG_LIMIT       -12  /* CG iteration cap reached (cap is opt-in; reference has none) */
+#define SIMOX_E_FFT_SIZE       -13  /* PME grid dimension not usable */
+#define SIMOX_E_STATE          -14  /* call order violated (e.g. FORCE before CELL_SORT) */
+#define SIMOX_E_NO_DEVICE      -15  /* no CUDA device / library built without one */
+#define SIMOX_E_UNSUPPORTED    -16  /* hetero-metal pair forms (METAL_HETERO, AL_NI,
+                                       eam.f90:38-168) are not on the GPU path */
+
+/* ---- precision modes --------------------------------------------------- */
+#define SIMOX_FP64   0   /* every term in FP64 (the FP64 GPU oracle path) */
+#define SIMOX_MIXED  1   /* pair terms and PME grids FP32; sums, energies,
+                            CG dots, residuals and projection FP64 */
+
+/* ---- option flags (simox_setup.flags) ----------------------------------- */
+#define SIMOX_FLAG_REFERENCE_LIMITS 0x1  /* enforce Nnb_max = 500 like the reference */
+
+/* ---- potential parameters: derived types of datafmt.f90:54-74 ---------- */
+typedef struct {            /* TYPE METL  datafmt.f90:65-68 */
+    double r_e, f_e, rho_e, rho_s, alpha, beta, A, B, kappa, lambda;
+    double Fn[4], Fm[4], Fp[4];
+    double eta, Fe;
+} simox_metl;
+
+typedef struct {            /* TYPE POTN  datafmt.f90:54-56 */
+    double xm, qmin, qmax, chi, J, xi, Z;
+    double fafb[SIMOX_NATOM][4];   /* fafb[j-1][k-1] = param(i)%fafb(j,k) */
+} simox_potn;
+
+typedef struct {            /* TYPE OXID  datafmt.f90:70-74 */
+    double r_e[SIMOX_NATOM], alph[SIMOX_NATOM], beta[SIMOX_NATOM];
+    double A[SIMOX_NATOM], B[SIMOX_NATOM], kapp[SIMOX_NATOM], lamb[SIMOX_NATOM];
+    double F0[4], F1[4], F2[4], F3[4], F4[4];
+    double re[5], rmax[5];
+    double fe, gamm, nu;
+} simox_oxid;
+
+typedef struct {
+    simox_metl eam[SIMOX_NMETAL];
+    simox_potn param[SIMOX_NATOM];
+    simox_oxid oxygn;
+} simox_potential;
+
+/* ---- system set-up: the parts of AMNT/STAT that fix array shapes -------- */
+typedef struct {
+    int    n_atoms;      /* Nset%Npt_all                                        */
+    int    capacity;     /* atoms the context can hold (>= n_atoms; 0 = n_atoms) */
+    double box[3];       /* Nset%box (Angstrom); positions live in [-L/2, L/2)  */
+    int    fft[3];       /* Nset%fft: PME grid K1 x K2 x K3                     */
+    int    pme_order;    /* B-spline order: 4 (reference, cubic), 6 or 8         */
+    double rcut;         /* sys%Rcut; Ewald a = 3.8/Rcut (main.f90:254)          */
+    int    precision;    /* SIMOX_FP64 or SIMOX_MIXED                            */
+    int    npt_max;      /* per-cell capacity (0 = SIMOX_NPT_MAX)                */
+    int    nnb_max;      /* per-atom neighbour capacity (0 = 1024)               */
+    int    device;       /* CUDA device ordinal                                  */
+    int    flags;        /* SIMOX_FLAG_*                                         */
+} simox_setup;
+
+/* Energies of TYPE STAT (datafmt.f90:59-63), all FP64, eV. */
+typedef struct {
+    double Eself, Edir, Erec, Epair, Egroup, Ectip;
+    double mv2;          /* sum m v^2 (amu A^2 / time-unit^2 = eV)                 */
+} simox_energies;
+
+/* Outcome of one CTIP_SOLVER call. */
+typedef struct {
+    int    n_cg;         /* nonlinear-CG iterations (ctip.f90:169-190)           */
+    int    n_line;       /* line-search (Brent) evaluations summed over iterations */
+    double error;        /* final MAXVAL(|p|)*|alpha|                             */
+    double q_sum;        /* total charge after the solve                          */
+} simox_ctip_report;
+
+/* Options of the device-resident main loop (main.f90:40-84, TAG_SET main.f90:376). */
+typedef struct {
+    double dt;           /* time step in internal units (fs / 10.180505306645389) */
+    int    thermostat;   /* 0 = NVE (VV_NVE2), 1 = Berendsen (VV_NVT2_BEREND)     */
+    double T_given;      /* target temperature in eV (K * kB)                     */
+    int    freq_new;     /* charges when MOD(step, freq_new) == 1; <= 0: never    */
+    int    freq_sort;    /* cell sort when MOD(step, freq_sort) == 0              */
+    int    reflect;      /* 1 = VV_NVE1_REFLECT (oxidation mode top wall)         */
+    int    charge_every_step; /* 1 = CTIP on every step (driver flag)             */
+    int    accumulate_rdf;    /* 1 = accumulate the RDF histogram in FORCE        */
+} simox_md_opts;
+
+typedef struct simox_ctx simox_ctx;
+
+/* ---- parameter tables --------------------------------------------------- */
+/* POTENTIAL_SETUP (datafmt.f90:142-262): fills the hard-coded Al/Ni/Fe/O/H
+ * tables and the Slater fafb coefficients.  Host-only; needs no GPU. */
+int simox_default_potential(simox_potential* pot);
+
+/* Text of a status code; reference STOP message where one exists. */
+const char* simox_status_string(int status);
+
+/* Library / build description string (host-only). */
+const char* simox_version(void);
+
+/* ---- context lifetime (READ_INPUT allocation, main.f90:96-260) ---------- */
+int simox_create(const simox_setup* setup, const simox_potential* pot, simox_ctx** out);
+int simox_destroy(simox_ctx* ctx);
+
+/* Host <-> device state copies.  x, v, f: [n][3]; q: [n]; id: [n].
+ * Any pointer may be NULL to skip that field (id is required on the first
+ * set_state).  n may differ from the previous call (NEW_O2, datafmt.f90:98)
+ * up to the capacity. */
+int simox_set_state(simox_ctx* ctx, int n, const int* id, const double* x,
+                    const double* v, const double* f, const double* q);
+int simox_get_state(simox_ctx* ctx, int n, int* id, double* x, double* v,
+                    double* f, double* q);
+int simox_get_natoms(simox_ctx* ctx, int* n);
+
+/* ---- cells: cellsort.f90 ------------------------------------------------ */
+/* CELL_HIERARCHY (cellsort.f90:3-36): the 13-cell half stencil, 1-based cell
+ * ids, pair[(id-1)*13 + n-1] = cell(id)%pair(n).  ncell_out[3] = Nset%Ncell. */
+int simox_cell_hierarchy(simox_ctx* ctx, int* ncell_out, int* pair);
+/* CELL_SORT (cellsort.f90:53-80): bins atoms on the device; cell membership
+ * and in-cell order are bit-exact to the reference. */
+int simox_cell_sort(simox_ctx* ctx);
+/* Exports the bins in the reference layout: npt[c] = cell(c+1)%Npt and
+ * link[c*link_stride + k] = cell(c+1)%link(k+1) (1-based atom ids). */
+int simox_get_cells(simox_ctx* ctx, int* npt, int* link, int link_stride);
+
+/* ---- forces and charges: force.f90, ctip.f90 ---------------------------- */
+/* PME_SELF (force.f90:467-517): sets a = 3.8/Rcut, the Ewald self energy and
+ * the reciprocal kernel psi (psi(0) = 0, tin-foil). */
+int simox_pme_self(simox_ctx* ctx, simox_energies* e);
+/* Copies the psi table (K1*K2*K3, x fastest) for checking. */
+int simox_get_psi(simox_ctx* ctx, double* psi);
+/* CTIP_SOLVER (ctip.f90:3-212): nonlinear CG charge equilibration with the
+ * reference's Sigma-g ratio, mean projection, Brent line search on [-1,1]
+ * and MAXVAL(|alpha p|) < 1e-3 stop.  Matrix-free: the short-range Slater and
+ * erfc couplings are recomputed per pair, the long-range part is the PME
+ * potential.  Writes the charges and e->Eself.  max_cg <= 0: no cap. */
+int simox_ctip_solve(simox_ctx* ctx, int max_cg, simox_energies* e, simox_ctip_report* rep);
+/* FORCE (force.f90:3-361): EAM density, embedding, pair, Ewald real-space and
+ * CTIP short-range forces; overwrites forces; sets Epair, Edir, Ectip, Egroup.
+ * rdf: NULL, or a host histogram of SIMOX_RDF_LEN ints that is incremented. */
+int simox_force(simox_ctx* ctx, simox_energies* e, int* rdf);
+/* PME (force.f90:364-464): reciprocal-space forces added to the forces, the
+ * mean PME force removed, Erec set. */
+int simox_pme(simox_ctx* ctx, simox_energies* e);
+/* Per-atom EAM density and embedding derivative of the last FORCE call
+ * (rho, dF/drho) in original atom order, for checking. */
+int simox_get_eam(simox_ctx* ctx, double* rho, double* dFdrho);
+
+/* ---- integrator: vverlet.f90 -------------------------------------------- */
+int simox_vv_nve1(simox_ctx* ctx, double dt);                      /* vverlet.f90:74-96   */
+int simox_vv_nve1_reflect(simox_ctx* ctx, double dt);              /* vverlet.f90:100-129 */
+int simox_vv_nve2(simox_ctx* ctx, double dt, double* mv2);         /* vverlet.f90:132-157 */
+int simox_vv_nvt2_berend(simox_ctx* ctx, double dt, double T_given, double* mv2); /* vverlet.f90:160-208 */
+
+/* ---- device-resident main loop (main.f90:40-84) -------------------------
+ * Runs steps first_step .. first_step+nsteps-1 of the reference loop on the
+ * device: VV1, CELL_SORT, CTIP_SOLVER (TAG_SET rule), FORCE, PME, VV2/NVT.
+ * last: energies of the final step (may be NULL). rdf: as simox_force. */
+int simox_md_run(simox_ctx* ctx, const simox_md_opts* opts, int first_step,
+                 int nsteps, simox_energies* last, int* rdf);
+
+/* ---- timing and counters ------------------------------------------------ */
+/* CUDA events on the context's stream around a region of calls. */
+int simox_timer_begin(simox_ctx* ctx);
+int simox_timer_end(simox_ctx* ctx, float* ms);
+/* Per-kernel-family event timing (off by default).  After enabling, each
+ * instrumented launch is bracketed by events on the context's stream. */
+int simox_profile_enable(simox_ctx* ctx, int on);
+/* names: '\n'-separated kernel family names written into buf (may be NULL);
+ * ms[k], launches[k] filled for k < cap; *count = number of families. */
+int simox_profile_read(simox_ctx* ctx, char* buf, int buflen, double* ms,
+                       long long* launches, int cap, int* count);
+int simox_profile_reset(simox_ctx* ctx);
+/* Total kernels this context has launched since creation. */
+int simox_launch_count(simox_ctx* ctx, long long* n);
+/* Wait for the context's stream. */
+int simox_sync(simox_ctx* ctx);
+/* Neighbour statistics of the last list build: max and total list length. */
+int simox_neighbor_stats(simox_ctx* ctx, int* max_nnb, long long* total_nnb);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SIMOX_GPU_H */

@@ -1,0 +1,330 @@
+"""Python mirror of SIMOX's per-step subroutine interface over the C ABI.
+
+Each method of :class:`Simox` is one Fortran subroutine of the reference's
+main loop (main.f90:29-34, 41-61, 63-84), with the same name and the same
+meaning of arguments and results; the state that the Fortran passes by
+reference (``q`` particles, ``cell``, ``psi``, ``sys`` energies) lives on the
+device inside the context.  Errors are raised as :class:`SimoxError` carrying
+the reference's STOP text where one exists.
+
+The product path is ``libsimox_b200.so`` only: importing this module on a
+machine without the built library, or calling a compute method without a GPU,
+raises -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _abi
+from ._abi import (CtipReport, Energies, MdOpts, Potential, Setup, SIMOX_FP64, SIMOX_MIXED,
+                   status_text)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsimox_b200.so")
+_lib = None
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_vp = C.c_void_p
+
+
+class SimoxError(RuntimeError):
+    def __init__(self, code: int, where: str = ""):
+        self.code = int(code)
+        super().__init__(f"{where}: status {code}: {status_text(code)}")
+
+
+def lib():
+    """Load libsimox_b200.so (built in-tree by ``simox_b200.build``)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing; run python -m simox_b200.build")
+    L = C.CDLL(LIB_PATH)
+    sig = {
+        "simox_default_potential": [C.POINTER(Potential)],
+        "simox_status_string": [C.c_int],
+        "simox_version": [],
+        "simox_create": [C.POINTER(Setup), C.POINTER(Potential), C.POINTER(_vp)],
+        "simox_destroy": [_vp],
+        "simox_set_state": [_vp, C.c_int, _ip, _dp, _dp, _dp, _dp],
+        "simox_get_state": [_vp, C.c_int, _ip, _dp, _dp, _dp, _dp],
+        "simox_get_natoms": [_vp, _ip],
+        "simox_cell_hierarchy": [_vp, _ip, _ip],
+        "simox_cell_sort": [_vp],
+        "simox_get_cells": [_vp, _ip, _ip, C.c_int],
+        "simox_pme_self": [_vp, C.POINTER(Energies)],
+        "simox_get_psi": [_vp, _dp],
+        "simox_ctip_solve": [_vp, C.c_int, C.POINTER(Energies), C.POINTER(CtipReport)],
+        "simox_force": [_vp, C.POINTER(Energies), _ip],
+        "simox_pme": [_vp, C.POINTER(Energies)],
+        "simox_get_eam": [_vp, _dp, _dp],
+        "simox_vv_nve1": [_vp, C.c_double],
+        "simox_vv_nve1_reflect": [_vp, C.c_double],
+        "simox_vv_nve2": [_vp, C.c_double, _dp],
+        "simox_vv_nvt2_berend": [_vp, C.c_double, C.c_double, _dp],
+        "simox_md_run": [_vp, C.POINTER(MdOpts), C.c_int, C.c_int, C.POINTER(Energies), _ip],
+        "simox_timer_begin": [_vp],
+        "simox_timer_end": [_vp, C.POINTER(C.c_float)],
+        "simox_profile_enable": [_vp, C.c_int],
+        "simox_profile_read": [_vp, C.c_char_p, C.c_int, _dp, C.POINTER(C.c_longlong), C.c_int, _ip],
+        "simox_profile_reset": [_vp],
+        "simox_launch_count": [_vp, C.POINTER(C.c_longlong)],
+        "simox_sync": [_vp],
+        "simox_neighbor_stats": [_vp, _ip, C.POINTER(C.c_longlong)],
+    }
+    for name, args in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = C.c_char_p if name in ("simox_status_string", "simox_version") else C.c_int
+    _lib = L
+    return L
+
+
+def default_potential() -> Potential:
+    """POTENTIAL_SETUP (datafmt.f90:142-262) from the library."""
+    P = Potential()
+    _check(lib().simox_default_potential(C.byref(P)), "POTENTIAL_SETUP")
+    return P
+
+
+def _check(st: int, where: str):
+    if st != 0:
+        raise SimoxError(st, where)
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def _i(a):
+    return a.ctypes.data_as(_ip) if a is not None else None
+
+
+def _f64(a, shape=None):
+    if a is None:
+        return None
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a.reshape(shape) if shape is not None else a
+
+
+class Simox:
+    """One device context: the arrays READ_INPUT allocates (main.f90:96-260).
+
+    Parameters mirror the reference's set-up: ``box`` (Nset%box), ``fft``
+    (Nset%fft), ``rcut`` (sys%Rcut), plus the build's options ``order`` (PME
+    B-spline order; 4 is the reference's), ``precision`` ("fp64" or "mixed")
+    and capacities.
+    """
+
+    def __init__(self, ids, x, box, fft, rcut=10.0, q=None, v=None, f=None, order=4,
+                 precision="fp64", capacity=0, npt_max=0, nnb_max=0, device=0, flags=0,
+                 potential: Potential | None = None):
+        self._ctx = _vp()
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        n = len(ids)
+        s = Setup()
+        s.n_atoms = n
+        s.capacity = int(capacity)
+        s.box[:] = [float(b) for b in box]
+        s.fft[:] = [int(k) for k in fft]
+        s.pme_order = int(order)
+        s.rcut = float(rcut)
+        s.precision = {"fp64": SIMOX_FP64, "mixed": SIMOX_MIXED}[precision] if isinstance(precision, str) \
+            else int(precision)
+        s.npt_max = int(npt_max)
+        s.nnb_max = int(nnb_max)
+        s.device = int(device)
+        s.flags = int(flags)
+        self.setup = s
+        self.precision = precision
+        self.potential = potential if potential is not None else default_potential()
+        _check(lib().simox_create(C.byref(s), C.byref(self.potential), C.byref(self._ctx)), "simox_create")
+        self.n = n
+        self.set_state(ids=ids, x=x, v=v, f=f, q=q)
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if self._ctx:
+            lib().simox_destroy(self._ctx)
+            self._ctx = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- state ------------------------------------------------------------
+    def set_state(self, ids=None, x=None, v=None, f=None, q=None):
+        n = len(ids) if ids is not None else self.n
+        ids = np.ascontiguousarray(ids, dtype=np.int32) if ids is not None else None
+        x, v, f = _f64(x, (n, 3)), _f64(v, (n, 3)), _f64(f, (n, 3))
+        q = _f64(q)
+        _check(lib().simox_set_state(self._ctx, n, _i(ids), _d(x), _d(v), _d(f), _d(q)), "set_state")
+        self.n = n
+
+    def get_state(self):
+        n = self.n
+        ids = np.zeros(n, np.int32)
+        x = np.zeros((n, 3))
+        v = np.zeros((n, 3))
+        f = np.zeros((n, 3))
+        q = np.zeros(n)
+        _check(lib().simox_get_state(self._ctx, n, _i(ids), _d(x), _d(v), _d(f), _d(q)), "get_state")
+        return dict(ids=ids, x=x, v=v, f=f, q=q)
+
+    # -- cellsort.f90 -----------------------------------------------------
+    def cell_hierarchy(self):
+        """CELL_HIERARCHY: (Ncell[3], pair[ncell, 13]) with 1-based ids."""
+        nc = np.zeros(3, np.int32)
+        lib().simox_cell_hierarchy(self._ctx, _i(nc), None)
+        pair = np.zeros((int(np.prod(nc)), 13), np.int32)
+        _check(lib().simox_cell_hierarchy(self._ctx, _i(nc), _i(pair)), "CELL_HIERARCHY")
+        return nc, pair
+
+    def cell_sort(self):
+        """CELL_SORT (cellsort.f90:53-80)."""
+        _check(lib().simox_cell_sort(self._ctx), "CELL_SORT")
+
+    def get_cells(self, link_stride=None):
+        """cell(:)%Npt and cell(:)%link in the reference layout (1-based ids)."""
+        nc, _ = self.cell_hierarchy()
+        ncell = int(np.prod(nc))
+        stride = int(link_stride or self.setup.npt_max or _abi.NPT_MAX)
+        npt = np.zeros(ncell, np.int32)
+        link = np.zeros((ncell, stride), np.int32)
+        _check(lib().simox_get_cells(self._ctx, _i(npt), _i(link), stride), "get_cells")
+        return npt, link
+
+    # -- force.f90 / ctip.f90 ---------------------------------------------
+    def pme_self(self) -> float:
+        """PME_SELF: psi table and sys%Eself; returns Eself."""
+        e = Energies()
+        _check(lib().simox_pme_self(self._ctx, C.byref(e)), "PME_SELF")
+        return e.Eself
+
+    def get_psi(self):
+        K = list(self.setup.fft)
+        psi = np.zeros(K[0] * K[1] * K[2])
+        _check(lib().simox_get_psi(self._ctx, _d(psi)), "get_psi")
+        return psi
+
+    def ctip_solver(self, max_cg: int = 0):
+        """CTIP_SOLVER: new charges on the device; returns (Eself, report dict)."""
+        e = Energies()
+        r = CtipReport()
+        st = lib().simox_ctip_solve(self._ctx, int(max_cg), C.byref(e), C.byref(r))
+        if st not in (0, _abi.SIMOX_E_CG_LIMIT) or (st != 0 and max_cg <= 0):
+            raise SimoxError(st, "CTIP_SOLVER")
+        return e.Eself, dict(n_cg=r.n_cg, n_line=r.n_line, error=r.error, q_sum=r.q_sum)
+
+    def force(self, rdf: np.ndarray | None = None):
+        """FORCE: overwrites forces; returns dict(Epair, Edir, Ectip, Egroup).
+        ``rdf`` (int32, SIMOX_RDF_LEN) is incremented like pair%rdf."""
+        e = Energies()
+        if rdf is not None:
+            assert rdf.dtype == np.int32 and rdf.size == _abi.RDF_LEN and rdf.flags.c_contiguous
+        _check(lib().simox_force(self._ctx, C.byref(e), _i(rdf)), "FORCE")
+        return dict(Epair=e.Epair, Edir=e.Edir, Ectip=e.Ectip, Egroup=e.Egroup)
+
+    def pme(self) -> float:
+        """PME: adds reciprocal forces, removes the mean; returns Erec."""
+        e = Energies()
+        _check(lib().simox_pme(self._ctx, C.byref(e)), "PME")
+        return e.Erec
+
+    def get_eam(self):
+        rho = np.zeros(self.n)
+        dF = np.zeros(self.n)
+        _check(lib().simox_get_eam(self._ctx, _d(rho), _d(dF)), "get_eam")
+        return rho, dF
+
+    # -- vverlet.f90 --------------------------------------------------------
+    def vv_nve1(self, dt: float, reflect: bool = False):
+        fn = lib().simox_vv_nve1_reflect if reflect else lib().simox_vv_nve1
+        _check(fn(self._ctx, float(dt)), "VV_NVE1")
+
+    def vv_nve2(self, dt: float) -> float:
+        mv2 = C.c_double(0.0)
+        _check(lib().simox_vv_nve2(self._ctx, float(dt), C.byref(mv2)), "VV_NVE2")
+        return mv2.value
+
+    def vv_nvt2_berend(self, dt: float, T_given: float) -> float:
+        mv2 = C.c_double(0.0)
+        _check(lib().simox_vv_nvt2_berend(self._ctx, float(dt), float(T_given), C.byref(mv2)), "VV_NVT2_BEREND")
+        return mv2.value
+
+    # -- main loop ----------------------------------------------------------
+    def md_run(self, nsteps: int, dt: float, first_step: int = 1, thermostat: bool = False,
+               T_given: float = 0.0, freq_new: int = 0, freq_sort: int = 1, reflect: bool = False,
+               charge_every_step: bool = False, rdf: np.ndarray | None = None):
+        """Steps first_step..first_step+nsteps-1 of main.f90:40-84 on the device."""
+        o = MdOpts()
+        o.dt = float(dt)
+        o.thermostat = 1 if thermostat else 0
+        o.T_given = float(T_given)
+        o.freq_new = int(freq_new)
+        o.freq_sort = int(freq_sort)
+        o.reflect = 1 if reflect else 0
+        o.charge_every_step = 1 if charge_every_step else 0
+        o.accumulate_rdf = 1 if rdf is not None else 0
+        e = Energies()
+        _check(lib().simox_md_run(self._ctx, C.byref(o), int(first_step), int(nsteps), C.byref(e), _i(rdf)),
+               "md_run")
+        return e.as_dict()
+
+    # -- timing ---------------------------------------------------------------
+    def timer_begin(self):
+        _check(lib().simox_timer_begin(self._ctx), "timer_begin")
+
+    def timer_end(self) -> float:
+        ms = C.c_float(0.0)
+        _check(lib().simox_timer_end(self._ctx, C.byref(ms)), "timer_end")
+        return ms.value
+
+    def profile(self, on: bool = True):
+        _check(lib().simox_profile_enable(self._ctx, 1 if on else 0), "profile_enable")
+
+    def profile_reset(self):
+        _check(lib().simox_profile_reset(self._ctx), "profile_reset")
+
+    def profile_read(self):
+        cap = 128
+        buf = C.create_string_buffer(8192)
+        ms = np.zeros(cap)
+        nl = (C.c_longlong * cap)()
+        cnt = C.c_int(0)
+        _check(lib().simox_profile_read(self._ctx, buf, 8192, _d(ms), nl, cap, C.byref(cnt)), "profile_read")
+        names = buf.value.decode().split("\n")[: cnt.value]
+        return {nm: (float(ms[k]), int(nl[k])) for k, nm in enumerate(names)}
+
+    def launch_count(self) -> int:
+        n = C.c_longlong(0)
+        _check(lib().simox_launch_count(self._ctx, C.byref(n)), "launch_count")
+        return n.value
+
+    def sync(self):
+        _check(lib().simox_sync(self._ctx), "sync")
+
+    def neighbor_stats(self):
+        mx = C.c_int(0)
+        tot = C.c_longlong(0)
+        _check(lib().simox_neighbor_stats(self._ctx, C.byref(mx), C.byref(tot)), "neighbor_stats")
+        return mx.value, tot.value
+
+
+def from_system(sys_, precision="fp64", **kw) -> Simox:
+    """Context for a :class:`simox_b200.systems.AtomSystem`."""
+    return Simox(sys_.ids, sys_.x, sys_.box, sys_.fft, rcut=sys_.rcut, q=sys_.q, v=sys_.v,
+                 order=sys_.order, precision=precision, **kw)

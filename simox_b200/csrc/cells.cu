@@ -1,0 +1,381 @@
+// cells.cu -- CELL_HIERARCHY / CELL_SORT (cellsort.f90) and the neighbour-list
+// build of the pair loops (force.f90:41-58,146-162; ctip.f90:64-80,116-130).
+//
+// Binning is a counting sort: cell id per atom with the reference's FP64
+// arithmetic (xx = x + L/2; INT(xx/Lcell); MOD(id + Ncell, Ncell)), an atomic
+// histogram, an exclusive scan, a scatter and a per-cell rank sort that puts
+// each cell's atoms in ascending original index -- the order CELL_SORT's
+// serial loop appends them (cellsort.f90:68-76).  Membership and order are
+// therefore bit-exact.
+//
+// The neighbour list is a full list (each pair in both rows) in cell-sorted
+// index space.  One CTA per home cell stages the 27 stencil cells' atoms in
+// shared memory as FP32 offsets from the home-cell centre; each thread owns a
+// home atom and tests every staged candidate with an FP32 distance.  Pairs
+// within a relative band of 4e-5 around Rcut^2 are re-tested with the
+// reference's exact FP64 expression (dx - L*DNINT(dx/L), r2 summed without
+// FMA), so list membership equals the reference's r2 < Rcut2 test.
+#include "simox_internal.cuh"
+
+#include <algorithm>
+#include <cstring>
+
+namespace sx {
+
+constexpr int LB_THREADS = 128;
+constexpr int LB_TILE = 2048;
+
+// ---------------------------------------------------------------------------
+// CELL_HIERARCHY cellsort.f90:3-36 (host): 13-cell half stencil, 1-based ids
+static int id_cell(const int nc[3], int i, int j, int k) {
+    int l = (i - 1 + nc[0]) % nc[0];
+    int m = (j - 1 + nc[1]) % nc[1];
+    int n = (k - 1 + nc[2]) % nc[2];
+    return l + m * nc[0] + n * nc[0] * nc[1] + 1;
+}
+
+int list_prepare(simox_ctx* c);
+
+int build_cell_tables(simox_ctx* c) {
+    const int* nc = c->nc;
+    const int ncell = c->ncell;
+    std::vector<int>& P = c->h_pair13;
+    P.assign((size_t)ncell * 13, 0);
+    static const int off[13][3] = {{-1, -1, -1}, {0, -1, -1}, {1, -1, -1}, {-1, 0, -1}, {0, 0, -1},
+                                   {1, 0, -1},   {-1, 1, -1}, {0, 1, -1},  {1, 1, -1},  {-1, -1, 0},
+                                   {0, -1, 0},   {1, -1, 0},  {-1, 0, 0}};
+    for (int i = 1; i <= nc[0]; i++)
+        for (int j = 1; j <= nc[1]; j++)
+            for (int k = 1; k <= nc[2]; k++) {
+                int id = id_cell(nc, i, j, k);
+                for (int n = 0; n < 13; n++)
+                    P[(size_t)(id - 1) * 13 + n] = id_cell(nc, i + off[n][0], j + off[n][1], k + off[n][2]);
+            }
+    // Full stencil with multiplicity: self, the 13 forward cells, and every
+    // cell whose forward list names this one.  dir: 0 self, 1 forward
+    // (this atom is the reference's "i"), 2 reverse.
+    std::vector<int> E((size_t)ncell * kEntries, 0);
+    std::vector<int> fill(ncell, 0);
+    for (int cc = 0; cc < ncell; cc++) {
+        E[(size_t)cc * kEntries + fill[cc]++] = cc;
+        for (int n = 0; n < 13; n++) E[(size_t)cc * kEntries + fill[cc]++] = (P[(size_t)cc * 13 + n] - 1) | (1 << 28);
+    }
+    for (int cc = 0; cc < ncell; cc++)
+        for (int n = 0; n < 13; n++) {
+            int t = P[(size_t)cc * 13 + n] - 1;
+            if (fill[t] >= kEntries) return SIMOX_E_CELL_TOO_SMALL;
+            E[(size_t)t * kEntries + fill[t]++] = cc | (2 << 28);
+        }
+    for (int cc = 0; cc < ncell; cc++)
+        if (fill[cc] != kEntries) return SIMOX_E_CELL_TOO_SMALL;
+    if (int st = list_prepare(c)) return st;
+    cudaError_t e1 = cudaMemcpyAsync(c->pair13, P.data(), P.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream);
+    cudaError_t e2 = cudaMemcpyAsync(c->entries, E.data(), E.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream);
+    if (e1 != cudaSuccess || e2 != cudaSuccess) return SIMOX_E_CUDA;
+    return cuda_status(cudaStreamSynchronize(c->stream));
+}
+
+// ---------------------------------------------------------------------------
+// CELL_SORT kernels
+__global__ void bin_atoms_kernel(int n, const double* __restrict__ x, double3 hbox, double3 lc, int3 nc,
+                                 int* __restrict__ cell_of, int* __restrict__ count, int* __restrict__ status) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int id[3];
+    const double hb[3] = {hbox.x, hbox.y, hbox.z};
+    const double l[3] = {lc.x, lc.y, lc.z};
+    const int m[3] = {nc.x, nc.y, nc.z};
+    bool bad = false;
+    for (int d = 0; d < 3; d++) {
+        double xx = __dadd_rn(x[3 * i + d], hb[d]);     // xx = x + hbox   cellsort.f90:69
+        double t = __ddiv_rn(xx, l[d]);                 // xx/Lcell        cellsort.f90:70
+        if (!(fabs(t) < 1.0e9)) { bad = true; id[d] = 0; continue; }
+        int v = __double2int_rz(t);                     // INT(): toward zero
+        v = (v + m[d]) % m[d];                          // MOD(id+Ncell, Ncell) cellsort.f90:71
+        if (v < 0) { bad = true; v = 0; }
+        id[d] = v;
+    }
+    if (bad) atomicOr(status, ST_POSITION);
+    int cell = id[0] + id[1] * m[0] + id[2] * m[0] * m[1];
+    cell_of[i] = cell;
+    atomicAdd(count + cell, 1);
+}
+
+__global__ void scan_cells_kernel(const int* __restrict__ count, int* __restrict__ start, int* __restrict__ fill,
+                                  int ncell, int npt_max, int* __restrict__ status) {
+    __shared__ int sm[1024];
+    __shared__ int carry;
+    const int t = threadIdx.x;
+    if (t == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < ncell; base += 1024) {
+        int v = base + t < ncell ? count[base + t] : 0;
+        if (v > npt_max) atomicOr(status, ST_CELL_OVERFLOW);
+        sm[t] = v;
+        __syncthreads();
+        for (int off = 1; off < 1024; off <<= 1) {
+            int add = t >= off ? sm[t - off] : 0;
+            __syncthreads();
+            sm[t] += add;
+            __syncthreads();
+        }
+        int excl = sm[t] - v + carry;
+        if (base + t < ncell) { start[base + t] = excl; fill[base + t] = excl; }
+        __syncthreads();
+        if (t == 1023) carry += sm[1023];
+        __syncthreads();
+    }
+    if (t == 0) start[ncell] = carry;
+}
+
+__global__ void scatter_atoms_kernel(int n, const int* __restrict__ cell_of, int* __restrict__ fill,
+                                     int* __restrict__ sorted) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int slot = atomicAdd(fill + cell_of[i], 1);
+    sorted[slot] = i;
+}
+
+// Rank sort inside each cell: ascending original index (= CELL_SORT order).
+__global__ void cell_rank_sort_kernel(const int* __restrict__ start, int* __restrict__ sorted, int npt_max) {
+    extern __shared__ int buf[];
+    const int cc = blockIdx.x;
+    const int s0 = start[cc], n = start[cc + 1] - s0;
+    if (n <= 1 || n > npt_max) return;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) buf[k] = sorted[s0 + k];
+    __syncthreads();
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        int v = buf[k], rank = 0;
+        for (int m = 0; m < n; m++) rank += buf[m] < v;
+        sorted[s0 + rank] = v;
+    }
+}
+
+int cell_sort(simox_ctx* c) {
+    if (!c->have_ids) return SIMOX_E_STATE;
+    const int n = c->n;
+    cudaMemsetAsync(c->cell_count, 0, sizeof(int) * c->ncell, c->stream);
+    if (n > 0) {
+        Launch L(c, "cell_bin");
+        bin_atoms_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(
+            n, c->x, make_double3(c->hbox[0], c->hbox[1], c->hbox[2]), make_double3(c->lc[0], c->lc[1], c->lc[2]),
+            make_int3(c->nc[0], c->nc[1], c->nc[2]), c->cell_of, c->cell_count, c->status);
+    }
+    {
+        Launch L(c, "cell_scan");
+        scan_cells_kernel<<<1, 1024, 0, c->stream>>>(c->cell_count, c->cell_start, c->cell_fill, c->ncell, c->npt_max,
+                                                     c->status);
+    }
+    if (n > 0) {
+        Launch L(c, "cell_scatter");
+        scatter_atoms_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, c->cell_of, c->cell_fill, c->sorted);
+    }
+    {
+        Launch L(c, "cell_order");
+        cell_rank_sort_kernel<<<c->ncell, 128, sizeof(int) * c->npt_max, c->stream>>>(c->cell_start, c->sorted,
+                                                                                      c->npt_max);
+    }
+    int st = check_launch(c);
+    if (st) return st;
+    c->cells_valid = true;
+    c->gathered = false;
+    c->list_valid = false;
+    return SIMOX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// gather original-order state into cell order
+__global__ void gather_sorted_kernel(int n, const int* __restrict__ sorted, const double* __restrict__ x,
+                                     const double* __restrict__ q, const int* __restrict__ id,
+                                     double4* __restrict__ xq, int* __restrict__ ts) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int o = sorted[k];
+    xq[k] = make_double4(x[3 * o], x[3 * o + 1], x[3 * o + 2], q[o]);
+    ts[k] = id[o] - 1;
+}
+
+int gather_sorted(simox_ctx* c) {
+    if (!c->cells_valid) return SIMOX_E_STATE;
+    if (c->n > 0) {
+        Launch L(c, "gather_sorted");
+        gather_sorted_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->n, c->sorted, c->x, c->q, c->id, c->xq_s,
+                                                                        c->t_s);
+    }
+    c->gathered = true;
+    return SIMOX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// neighbour list
+struct LBParams {
+    double3 box, origin, lc;
+    int3 nc;
+    double rcut2;
+    float bx, by, bz, ibx, iby, ibz, r2lo, r2hi;
+    int cap, npt_max;
+};
+
+// reference r2 (force.f90:51-53): rx = dx - box*DNINT(dx/box), no FMA
+__device__ __forceinline__ double exact_r2(double4 a, double4 b, double3 box) {
+    double dx = __dsub_rn(a.x, b.x), dy = __dsub_rn(a.y, b.y), dz = __dsub_rn(a.z, b.z);
+    dx = __dsub_rn(dx, __dmul_rn(box.x, round(__ddiv_rn(dx, box.x))));
+    dy = __dsub_rn(dy, __dmul_rn(box.y, round(__ddiv_rn(dy, box.y))));
+    dz = __dsub_rn(dz, __dmul_rn(box.z, round(__ddiv_rn(dz, box.z))));
+    return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+}
+
+template <bool FAST>
+__global__ void __launch_bounds__(LB_THREADS)
+    build_list_kernel(const int* __restrict__ cell_start, const int* __restrict__ entries,
+                      const double4* __restrict__ xq, unsigned* __restrict__ nbr, int* __restrict__ nn, LBParams P,
+                      int* __restrict__ status, int* __restrict__ nn_max, unsigned long long* __restrict__ nn_tot) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    float4* cpos = reinterpret_cast<float4*>(smem);
+    unsigned* ctag = reinterpret_cast<unsigned*>(cpos + LB_TILE);
+    int* cnt = reinterpret_cast<int*>(ctag + LB_TILE);
+    __shared__ int es0[kEntries], edir[kEntries], epre[kEntries + 1];
+
+    const int cc = blockIdx.x;
+    const int h0 = cell_start[cc], nh = cell_start[cc + 1] - h0;
+    if (nh <= 0) return;
+    const int tid = threadIdx.x;
+    if (nh > P.npt_max) {   // over-full cell: CELL_SORT already flagged it; touch nothing
+        if (tid == 0) atomicOr(status, ST_CELL_OVERFLOW);
+        return;
+    }
+    if (tid < kEntries) {
+        int ent = entries[cc * kEntries + tid];
+        int ce = ent & 0x0fffffff;
+        es0[tid] = cell_start[ce];
+        epre[tid + 1] = cell_start[ce + 1] - cell_start[ce];
+        edir[tid] = ent >> 28;
+    }
+    for (int k = tid; k < nh; k += blockDim.x) cnt[k] = 0;
+    __syncthreads();
+    if (tid == 0) {
+        epre[0] = 0;
+        for (int e = 0; e < kEntries; e++) epre[e + 1] += epre[e];
+    }
+    __syncthreads();
+    const int T = epre[kEntries];
+    const int cz = cc / (P.nc.x * P.nc.y), cy = (cc / P.nc.x) % P.nc.y, cx = cc % P.nc.x;
+    const double cen_x = P.origin.x + (cx + 0.5) * P.lc.x;
+    const double cen_y = P.origin.y + (cy + 0.5) * P.lc.y;
+    const double cen_z = P.origin.z + (cz + 0.5) * P.lc.z;
+
+    for (int t0 = 0; t0 < T; t0 += LB_TILE) {
+        const int tn = min(LB_TILE, T - t0);
+        __syncthreads();
+        for (int k = tid; k < tn; k += blockDim.x) {
+            int g = t0 + k, e = 0;
+            while (epre[e + 1] <= g) e++;
+            int j = es0[e] + (g - epre[e]);
+            double4 p = xq[j];
+            cpos[k] = make_float4((float)(p.x - cen_x), (float)(p.y - cen_y), (float)(p.z - cen_z), 0.f);
+            ctag[k] = (unsigned)j | ((unsigned)edir[e] << 30);
+        }
+        __syncthreads();
+        for (int hl = tid; hl < nh; hl += blockDim.x) {
+            const int h = h0 + hl;
+            const double4 xh = xq[h];
+            const float hx = (float)(xh.x - cen_x), hy = (float)(xh.y - cen_y), hz = (float)(xh.z - cen_z);
+            int my = cnt[hl];
+            unsigned* row = nbr + (size_t)h * P.cap;
+            for (int k = 0; k < tn; k++) {
+                const unsigned tag = ctag[k];
+                const int j = (int)(tag & 0x3fffffffu);
+                if (j == h) continue;
+                bool acc;
+                if (FAST) {
+                    const float4 cp = cpos[k];
+                    float dx = hx - cp.x, dy = hy - cp.y, dz = hz - cp.z;
+                    dx -= P.bx * rintf(dx * P.ibx);
+                    dy -= P.by * rintf(dy * P.iby);
+                    dz -= P.bz * rintf(dz * P.ibz);
+                    const float r2 = dx * dx + dy * dy + dz * dz;
+                    if (r2 < P.r2lo) acc = true;
+                    else if (r2 > P.r2hi) acc = false;
+                    else acc = exact_r2(xh, xq[j], P.box) < P.rcut2;
+                } else {
+                    acc = exact_r2(xh, xq[j], P.box) < P.rcut2;
+                }
+                if (acc) {
+                    const unsigned dir = tag >> 30;
+                    const unsigned isa = dir == 0 ? (unsigned)(h < j) : (unsigned)(dir == 1);
+                    if (my < P.cap) row[my] = (unsigned)j | (isa << 31);
+                    my++;
+                }
+            }
+            cnt[hl] = my;
+        }
+    }
+    __syncthreads();
+    int lmax = 0;
+    unsigned long long ltot = 0;
+    for (int hl = tid; hl < nh; hl += blockDim.x) {
+        int m = cnt[hl];
+        nn[h0 + hl] = min(m, P.cap);
+        if (m > P.cap) atomicOr(status, ST_NBR_OVERFLOW);
+        lmax = max(lmax, m);
+        ltot += (unsigned long long)m;
+    }
+    atomicMax(nn_max, lmax);
+    atomicAdd(nn_tot, ltot);
+}
+
+int build_list(simox_ctx* c) {
+    if (!c->gathered) {
+        int st = gather_sorted(c);
+        if (st) return st;
+    }
+    cudaMemsetAsync(c->nn_max, 0, sizeof(int), c->stream);
+    cudaMemsetAsync(c->nn_tot, 0, sizeof(unsigned long long), c->stream);
+    LBParams P;
+    P.box = make_double3(c->box[0], c->box[1], c->box[2]);
+    P.origin = make_double3(-c->hbox[0], -c->hbox[1], -c->hbox[2]);
+    P.lc = make_double3(c->lc[0], c->lc[1], c->lc[2]);
+    P.nc = make_int3(c->nc[0], c->nc[1], c->nc[2]);
+    P.rcut2 = c->rcut2;
+    P.bx = (float)c->box[0]; P.by = (float)c->box[1]; P.bz = (float)c->box[2];
+    P.ibx = (float)(1.0 / c->box[0]); P.iby = (float)(1.0 / c->box[1]); P.ibz = (float)(1.0 / c->box[2]);
+    P.r2lo = (float)(c->rcut2 * (1.0 - 4.0e-5));
+    P.r2hi = (float)(c->rcut2 * (1.0 + 4.0e-5));
+    P.cap = c->nnb_cap;
+    P.npt_max = c->npt_max;
+    size_t smem = LB_TILE * (sizeof(float4) + sizeof(unsigned)) + sizeof(int) * c->npt_max;
+    {
+        Launch L(c, "neighbor_list");
+        if (c->fast_cells)
+            build_list_kernel<true><<<c->ncell, LB_THREADS, smem, c->stream>>>(
+                c->cell_start, c->entries, c->xq_s, c->nbr, c->nn, P, c->status, c->nn_max, c->nn_tot);
+        else
+            build_list_kernel<false><<<c->ncell, LB_THREADS, smem, c->stream>>>(
+                c->cell_start, c->entries, c->xq_s, c->nbr, c->nn, P, c->status, c->nn_max, c->nn_tot);
+    }
+    int st = check_launch(c);
+    if (st) return st;
+    c->list_valid = true;
+    return SIMOX_OK;
+}
+
+int ensure_list(simox_ctx* c) {
+    if (!c->cells_valid) return SIMOX_E_STATE;
+    if (!c->gathered) {
+        int st = gather_sorted(c);
+        if (st) return st;
+        c->list_valid = false;
+    }
+    if (!c->list_valid) return build_list(c);
+    return SIMOX_OK;
+}
+
+int list_prepare(simox_ctx* c) {
+    const int bytes = (int)(LB_TILE * (sizeof(float4) + sizeof(unsigned)) + sizeof(int) * c->npt_max);
+    cudaError_t e1 = cudaFuncSetAttribute(build_list_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaError_t e2 = cudaFuncSetAttribute(build_list_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e1 != cudaSuccess || e2 != cudaSuccess) return SIMOX_E_ARG;
+    return SIMOX_OK;
+}
+
+}  // namespace sx

@@ -1,0 +1,523 @@
+// pme.cu -- PME_SELF (force.f90:467-517), PME (force.f90:364-464) and the
+// potential gather of PHI_MESH (ctip.f90:336-396).
+//
+// The reference spreads charges with order-4 centred B-splines into a
+// complex K1xK2xK3 grid, runs two full complex FFTs (FFTE ZFFT3D, +1 with the
+// 1/N scale, then -1), multiplies by psi * prod 1/|b|^2 in between, and
+// gathers forces from the real part.  Because the charge grid is real and the
+// kernel is even, the same result is one real-to-complex transform, the
+// multiply on the half spectrum (with 1/N folded in) and one
+// complex-to-real transform (cuFFT D2Z/Z2D or R2C/C2R).  The energy
+// Epme = N sum_x Q(x) Qfin(x) is evaluated on the half spectrum as
+// sum_k G(k)|Q^(k)|^2 (Parseval), fused into the multiply.
+//
+// Spline order p is a template parameter: p = 4 uses the reference's cubic
+// polynomials (force.f90:389-400) term for term, other even orders the
+// cardinal B-spline recursion.  Stencil point n of coordinate u is
+// INT(u) - p/2 + 1 + n wrapped by MOD (force.f90:404).  The FP64 path rounds
+// the spread weight product to single precision before the multiply by q,
+// as force.f90:406 / ctip.f90:359 do with a default-kind CMPLX().
+#include "simox_internal.cuh"
+
+#include <cmath>
+#include <type_traits>
+#include <vector>
+
+namespace sx {
+
+// ---------------------------------------------------------------------------
+// B-spline weights
+template <int P>
+__device__ __forceinline__ void bspline_w(double u, double* w, double* dw) {
+    if constexpr (P == 4) {
+        double z = trunc(u) - u + 1.0;
+        w[0] = z * z * z / 6.0;
+        dw[0] = -3.0 * (z * z) / 6.0;
+        z = z + 1.0;
+        w[1] = (-3.0 * (z * z * z) + 12.0 * (z * z) - 12.0 * z + 4.0) / 6.0;
+        dw[1] = (9.0 * (z * z) - 24.0 * z + 12.0) / 6.0;
+        z = z + 1.0;
+        w[2] = (3.0 * (z * z * z) - 24.0 * (z * z) + 60.0 * z - 44.0) / 6.0;
+        dw[2] = (-9.0 * (z * z) + 48.0 * z - 60.0) / 6.0;
+        z = z + 1.0;
+        w[3] = (-(z * z * z) + 12.0 * (z * z) - 48.0 * z + 64.0) / 6.0;
+        dw[3] = (3.0 * (z * z) - 24.0 * z + 48.0) / 6.0;
+    } else {
+        const double fr = u - trunc(u);
+        double M[P];
+#pragma unroll
+        for (int k = 0; k < P; k++) M[k] = 0.0;
+        M[0] = fr;
+        M[1] = 1.0 - fr;
+        double dA[P];
+#pragma unroll
+        for (int n = 3; n <= P; n++) {
+            if (n == P) {
+#pragma unroll
+                for (int k = 0; k < P; k++) dA[k] = (k < P - 1 ? M[k] : 0.0) - (k >= 1 ? M[k - 1] : 0.0);
+            }
+            const double div = 1.0 / (double)(n - 1);
+#pragma unroll
+            for (int k = n - 1; k >= 0; k--) {
+                const double xk = fr + k;
+                const double a1 = k < n - 1 ? M[k] : 0.0;
+                const double a0 = k >= 1 ? M[k - 1] : 0.0;
+                M[k] = (xk * a1 + ((double)n - xk) * a0) * div;
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < P; s++) { w[s] = M[P - 1 - s]; dw[s] = dA[P - 1 - s]; }
+    }
+}
+
+struct PmeParams {
+    int3 K;
+    double3 box;
+    double3 kx;      // K/L
+    double cst;      // kc N / (V pi)
+    int n;
+};
+
+__device__ __forceinline__ int wrapi(int v, int K) {
+    v %= K;
+    return v < 0 ? v + K : v;
+}
+
+// spread: grid[x + K1(y + K2 z)] += q * W (cell-sorted atoms)
+template <typename R, int P>
+__global__ void __launch_bounds__(128)
+    spread_kernel(PmeParams S, const double4* __restrict__ xq, const double* __restrict__ qalt,
+                  R* __restrict__ grid, int round_weights) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= S.n) return;
+    const double4 a = xq[k];
+    const double q = qalt ? qalt[k] : a.w;
+    if (q == 0.0) return;
+    double wx[P], wy[P], wz[P], d[P];
+    const double ux = (double)S.K.x * (a.x + S.box.x * 0.5) / S.box.x;
+    const double uy = (double)S.K.y * (a.y + S.box.y * 0.5) / S.box.y;
+    const double uz = (double)S.K.z * (a.z + S.box.z * 0.5) / S.box.z;
+    bspline_w<P>(ux, wx, d);
+    bspline_w<P>(uy, wy, d);
+    bspline_w<P>(uz, wz, d);
+    const int bx = __double2int_rz(ux) - P / 2 + 1;
+    const int by = __double2int_rz(uy) - P / 2 + 1;
+    const int bz = __double2int_rz(uz) - P / 2 + 1;
+    int ix[P];
+#pragma unroll
+    for (int s = 0; s < P; s++) ix[s] = wrapi(bx + s, S.K.x);
+#pragma unroll
+    for (int c = 0; c < P; c++) {
+        const size_t gz = (size_t)wrapi(bz + c, S.K.z) * S.K.y;
+#pragma unroll
+        for (int b = 0; b < P; b++) {
+            const size_t gyz = (gz + wrapi(by + b, S.K.y)) * S.K.x;
+#pragma unroll
+            for (int aa = 0; aa < P; aa++) {
+                double w = wx[aa] * wy[b] * wz[c];
+                if (round_weights) w = (double)(float)w;   // CMPLX() default kind, force.f90:406
+                atomicAdd(grid + gyz + ix[aa], (R)(q * w));
+            }
+        }
+    }
+}
+
+// half-spectrum multiply by G/N and energy sum_k G |Q^|^2 (Hermitian weights)
+template <typename R>
+__global__ void __launch_bounds__(256)
+    influence_kernel(size_t nhalf, int kx_half, int K1,
+                     typename std::conditional<sizeof(R) == 8, double2, float2>::type* __restrict__ cg,
+                     const R* __restrict__ infl, double Ngrid, double* __restrict__ acc, int eflag) {
+    __shared__ double red[256 / 32];
+    double e = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nhalf; i += (size_t)gridDim.x * blockDim.x) {
+        const int kx = (int)(i % kx_half);
+        auto c = cg[i];
+        const R g = infl[i];
+        if (eflag) {
+            const double wgt = (kx == 0 || (2 * kx == K1)) ? 1.0 : 2.0;
+            e += wgt * (double)g * ((double)c.x * (double)c.x + (double)c.y * (double)c.y);
+        }
+        c.x *= g;
+        c.y *= g;
+        cg[i] = c;
+    }
+    if (eflag) block_add<256>(e * Ngrid, acc, A_EREC, red);
+}
+
+// gather forces: f[o] += -cst q sum (dW_x W_y W_z kx, ...) Qfin  (force.f90:439-456)
+template <typename R, int P>
+__global__ void __launch_bounds__(128)
+    gather_force_kernel(PmeParams S, const double4* __restrict__ xq, const R* __restrict__ grid,
+                        const int* __restrict__ sorted, double* __restrict__ f, double* __restrict__ acc) {
+    __shared__ double red[128 / 32];
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    double fo[3] = {0.0, 0.0, 0.0};
+    if (k < S.n) {
+        const double4 a = xq[k];
+        double wx[P], wy[P], wz[P], dx[P], dy[P], dz[P];
+        const double ux = (double)S.K.x * (a.x + S.box.x * 0.5) / S.box.x;
+        const double uy = (double)S.K.y * (a.y + S.box.y * 0.5) / S.box.y;
+        const double uz = (double)S.K.z * (a.z + S.box.z * 0.5) / S.box.z;
+        bspline_w<P>(ux, wx, dx);
+        bspline_w<P>(uy, wy, dy);
+        bspline_w<P>(uz, wz, dz);
+        const int bx = __double2int_rz(ux) - P / 2 + 1;
+        const int by = __double2int_rz(uy) - P / 2 + 1;
+        const int bz = __double2int_rz(uz) - P / 2 + 1;
+        int ix[P];
+#pragma unroll
+        for (int s = 0; s < P; s++) ix[s] = wrapi(bx + s, S.K.x);
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+#pragma unroll
+        for (int c = 0; c < P; c++) {
+            const size_t gz = (size_t)wrapi(bz + c, S.K.z) * S.K.y;
+#pragma unroll
+            for (int b = 0; b < P; b++) {
+                const size_t gyz = (gz + wrapi(by + b, S.K.y)) * S.K.x;
+                R tx = 0, tw = 0;
+#pragma unroll
+                for (int aa = 0; aa < P; aa++) {
+                    const R g = grid[gyz + ix[aa]];
+                    tx += (R)dx[aa] * g;
+                    tw += (R)wx[aa] * g;
+                }
+                sx += (double)tx * wy[b] * wz[c];
+                sy += (double)tw * dy[b] * wz[c];
+                sz += (double)tw * wy[b] * dz[c];
+            }
+        }
+        const double pre = -S.cst * a.w;
+        fo[0] = pre * sx * S.kx.x;
+        fo[1] = pre * sy * S.kx.y;
+        fo[2] = pre * sz * S.kx.z;
+        const int o = sorted[k];
+        f[3 * o] += fo[0];
+        f[3 * o + 1] += fo[1];
+        f[3 * o + 2] += fo[2];
+    }
+    block_add<128>(fo[0], acc, A_FSUM0, red);
+    block_add<128>(fo[1], acc, A_FSUM1, red);
+    block_add<128>(fo[2], acc, A_FSUM2, red);
+}
+
+// gather potential: phi[k] = scale * sum W Qfin  (ctip.f90:381-393)
+template <typename R, int P>
+__global__ void __launch_bounds__(128)
+    gather_pot_kernel(PmeParams S, const double4* __restrict__ xq, const R* __restrict__ grid,
+                      double* __restrict__ phi, double scale) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= S.n) return;
+    const double4 a = xq[k];
+    double wx[P], wy[P], wz[P], d[P];
+    const double ux = (double)S.K.x * (a.x + S.box.x * 0.5) / S.box.x;
+    const double uy = (double)S.K.y * (a.y + S.box.y * 0.5) / S.box.y;
+    const double uz = (double)S.K.z * (a.z + S.box.z * 0.5) / S.box.z;
+    bspline_w<P>(ux, wx, d);
+    bspline_w<P>(uy, wy, d);
+    bspline_w<P>(uz, wz, d);
+    const int bx = __double2int_rz(ux) - P / 2 + 1;
+    const int by = __double2int_rz(uy) - P / 2 + 1;
+    const int bz = __double2int_rz(uz) - P / 2 + 1;
+    int ix[P];
+#pragma unroll
+    for (int s = 0; s < P; s++) ix[s] = wrapi(bx + s, S.K.x);
+    double sum = 0.0;
+#pragma unroll
+    for (int c = 0; c < P; c++) {
+        const size_t gz = (size_t)wrapi(bz + c, S.K.z) * S.K.y;
+#pragma unroll
+        for (int b = 0; b < P; b++) {
+            const size_t gyz = (gz + wrapi(by + b, S.K.y)) * S.K.x;
+            R tw = 0;
+#pragma unroll
+            for (int aa = 0; aa < P; aa++) tw += (R)wx[aa] * grid[gyz + ix[aa]];
+            sum += (double)tw * wy[b] * wz[c];
+        }
+    }
+    phi[k] = scale * sum;
+}
+
+// psi(m) = exp(-pi^2 m2/a^2)/m2, m = 0 -> 0   (force.f90:500-514)
+__global__ void psi_kernel(int3 K, double3 box, double a2, double* __restrict__ psi) {
+    const size_t N = (size_t)K.x * K.y * K.z;
+    for (size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x; g < N; g += (size_t)gridDim.x * blockDim.x) {
+        int i = (int)(g % K.x), j = (int)((g / K.x) % K.y), k = (int)(g / ((size_t)K.x * K.y));
+        int ix = (i + K.x / 2) % K.x - K.x / 2;
+        int iy = (j + K.y / 2) % K.y - K.y / 2;
+        int iz = (k + K.z / 2) % K.z - K.z / 2;
+        int m = ix * ix + iy * iy + iz * iz;
+        double v = 0.0;
+        if (m != 0) {
+            double m2 = (double)(ix * ix) / (box.x * box.x) + (double)(iy * iy) / (box.y * box.y) +
+                        (double)(iz * iz) / (box.z * box.z);
+            v = exp(-m2 * (SX_PI * SX_PI) / a2) / m2;
+        }
+        psi[g] = v;
+    }
+}
+
+template <typename R>
+__global__ void infl_build_kernel(int3 K, int kxh, const double* __restrict__ psi, const double* __restrict__ bm,
+                                  double invN, R* __restrict__ infl) {
+    const size_t N = (size_t)kxh * K.y * K.z;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+        int kx = (int)(i % kxh), ky = (int)((i / kxh) % K.y), kz = (int)(i / ((size_t)kxh * K.y));
+        double p = psi[kx + (size_t)K.x * (ky + (size_t)K.y * kz)];
+        infl[i] = (R)(p * bm[kx] * bm[K.x + ky] * bm[K.x + K.y + kz] * invN);
+    }
+}
+
+// self energy (force.f90:486-498)
+__global__ void self_energy_kernel(int n, const int* __restrict__ id, const double* __restrict__ q,
+                                   const double* __restrict__ chi, const double* __restrict__ J,
+                                   const double* __restrict__ qmin, const double* __restrict__ qmax,
+                                   double* __restrict__ acc) {
+    __shared__ double red[256 / 32];
+    double q2 = 0.0, es = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double qi = q[i];
+        int s = id[i] - 1;
+        q2 -= qi * qi;
+        es += chi[s] * qi + 0.5 * J[s] * (qi * qi);
+        double dq = qi - qmin[s];
+        if (dq < 0.0) es += 2.0 * SX_WPEN * (dq * dq);
+        dq = qi - qmax[s];
+        if (dq > 0.0) es += 2.0 * SX_WPEN * (dq * dq);
+    }
+    block_add<256>(q2, acc, A_Q2SUM, red);
+    block_add<256>(es, acc, A_ESUM, red);
+}
+
+// ---------------------------------------------------------------------------
+// host side
+static double bmod_inv_host(int p, int k, int K) {
+    double th = 2.0 * SX_PI * (double)k / (double)K;
+    if (p == 4) {
+        double z = 4.0 + 2.0 * cos(th);
+        return 36.0 / (z * z);     // 36 / (4 + 2cos)^2 of force.f90:415-420
+    }
+    // centred B-spline values beta(t) = M_p(t + p/2) at integer t
+    std::vector<double> M(p + 1, 0.0), Mn(p + 1, 0.0);
+    M[0] = 0.0; M[1] = 1.0;                 // M_2 at 0, 1 (fr = 0)
+    for (int n = 3; n <= p; n++) {
+        for (int kk = 0; kk < n; kk++) {
+            double a1 = kk < n - 1 ? M[kk] : 0.0, a0 = kk >= 1 ? M[kk - 1] : 0.0;
+            Mn[kk] = (kk * a1 + (n - kk) * a0) / (double)(n - 1);
+        }
+        for (int kk = 0; kk < n; kk++) M[kk] = Mn[kk];
+    }
+    double b = 0.0;                          // M[kk] = M_p(kk)
+    for (int kk = 1; kk < p; kk++) b += M[kk] * cos(th * (kk - p / 2));
+    return 1.0 / (b * b);
+}
+
+int pme_free(simox_ctx* c) {
+    if (c->plans) {
+        cufftDestroy(c->plan_r2c);
+        cufftDestroy(c->plan_c2r);
+        c->plans = false;
+    }
+    cudaFree(c->grid); cudaFree(c->cgrid); cudaFree(c->infl); cudaFree(c->psi); cudaFree(c->bmod);
+    c->grid = c->cgrid = c->infl = nullptr;
+    c->psi = c->bmod = nullptr;
+    return SIMOX_OK;
+}
+
+int pme_setup(simox_ctx* c) {
+    const int* K = c->fft;
+    c->ngrid = (size_t)K[0] * K[1] * K[2];
+    c->nhalf = (size_t)(K[0] / 2 + 1) * K[1] * K[2];
+    const bool dbl = c->precision == SIMOX_FP64;
+    const size_t rs = dbl ? sizeof(double) : sizeof(float);
+    if (cudaMalloc(&c->grid, c->ngrid * rs) != cudaSuccess) return SIMOX_E_NOMEM;
+    if (cudaMalloc(&c->cgrid, c->nhalf * 2 * rs) != cudaSuccess) return SIMOX_E_NOMEM;
+    if (cudaMalloc(&c->infl, c->nhalf * rs) != cudaSuccess) return SIMOX_E_NOMEM;
+    if (cudaMalloc(&c->psi, c->ngrid * sizeof(double)) != cudaSuccess) return SIMOX_E_NOMEM;
+    if (cudaMalloc(&c->bmod, (K[0] + K[1] + K[2]) * sizeof(double)) != cudaSuccess) return SIMOX_E_NOMEM;
+    // cuFFT plans: dims slowest-first (K3, K2, K1); K1 is the contiguous x axis
+    if (cufftPlan3d(&c->plan_r2c, K[2], K[1], K[0], dbl ? CUFFT_D2Z : CUFFT_R2C) != CUFFT_SUCCESS) return SIMOX_E_FFT_SIZE;
+    if (cufftPlan3d(&c->plan_c2r, K[2], K[1], K[0], dbl ? CUFFT_Z2D : CUFFT_C2R) != CUFFT_SUCCESS) {
+        cufftDestroy(c->plan_r2c);
+        return SIMOX_E_FFT_SIZE;
+    }
+    cufftSetStream(c->plan_r2c, c->stream);
+    cufftSetStream(c->plan_c2r, c->stream);
+    c->plans = true;
+    std::vector<double> bm(K[0] + K[1] + K[2]);
+    int o = 0;
+    for (int d = 0; d < 3; d++)
+        for (int k = 0; k < K[d]; k++) bm[o++] = bmod_inv_host(c->order, k, K[d]);
+    if (cudaMemcpyAsync(c->bmod, bm.data(), bm.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream) !=
+        cudaSuccess)
+        return SIMOX_E_CUDA;
+    return cuda_status(cudaStreamSynchronize(c->stream));
+}
+
+// PME_SELF: psi table, influence function, self energy into acc
+int pme_self(simox_ctx* c) {
+    int3 K = make_int3(c->fft[0], c->fft[1], c->fft[2]);
+    double3 box = make_double3(c->box[0], c->box[1], c->box[2]);
+    {
+        Launch L(c, "pme_psi");
+        psi_kernel<<<num_sms(c) * 4, 256, 0, c->stream>>>(K, box, c->a * c->a, c->psi);
+    }
+    {
+        Launch L(c, "pme_influence_build");
+        const double invN = 1.0 / (double)c->ngrid;
+        if (c->precision == SIMOX_FP64)
+            infl_build_kernel<double><<<num_sms(c) * 4, 256, 0, c->stream>>>(K, K.x / 2 + 1, c->psi, c->bmod, invN,
+                                                                             (double*)c->infl);
+        else
+            infl_build_kernel<float><<<num_sms(c) * 4, 256, 0, c->stream>>>(K, K.x / 2 + 1, c->psi, c->bmod, invN,
+                                                                            (float*)c->infl);
+    }
+    c->psi_valid = true;
+    if (c->n > 0) {
+        // species parameter columns in device scratch (acc tail not used): small uploads
+        double h[4][5];
+        for (int s = 0; s < 5; s++) {
+            h[0][s] = c->pot.param[s].chi; h[1][s] = c->pot.param[s].J;
+            h[2][s] = c->pot.param[s].qmin; h[3][s] = c->pot.param[s].qmax;
+        }
+        double* d = c->line;   // line-search scratch is free outside CTIP
+        cudaMemcpyAsync(d, h, sizeof(h), cudaMemcpyHostToDevice, c->stream);
+        Launch L(c, "pme_self_energy");
+        self_energy_kernel<<<num_sms(c), 256, 0, c->stream>>>(c->n, c->id, c->q, d, d + 5, d + 10, d + 15, c->acc);
+    }
+    return check_launch(c);
+}
+
+template <typename R, int P>
+static void run_spread(simox_ctx* c, const PmeParams& S, const double* qalt) {
+    cudaMemsetAsync(c->grid, 0, c->ngrid * sizeof(R), c->stream);
+    Launch L(c, "pme_spread");
+    spread_kernel<R, P><<<(S.n + 127) / 128, 128, 0, c->stream>>>(S, c->xq_s, qalt, (R*)c->grid,
+                                                                  c->precision == SIMOX_FP64 ? 1 : 0);
+}
+
+static int run_convolution(simox_ctx* c, bool eflag) {
+    cufftResult r;
+    {
+        Launch L(c, "pme_fft_r2c");
+        if (c->precision == SIMOX_FP64)
+            r = cufftExecD2Z(c->plan_r2c, (cufftDoubleReal*)c->grid, (cufftDoubleComplex*)c->cgrid);
+        else
+            r = cufftExecR2C(c->plan_r2c, (cufftReal*)c->grid, (cufftComplex*)c->cgrid);
+    }
+    if (r != CUFFT_SUCCESS) return SIMOX_E_CUDA;
+    {
+        Launch L(c, "pme_influence");
+        int kxh = c->fft[0] / 2 + 1;
+        int g = num_sms(c) * 4;
+        if (c->precision == SIMOX_FP64)
+            influence_kernel<double><<<g, 256, 0, c->stream>>>(c->nhalf, kxh, c->fft[0], (double2*)c->cgrid,
+                                                               (const double*)c->infl, (double)c->ngrid, c->acc,
+                                                               eflag ? 1 : 0);
+        else
+            influence_kernel<float><<<g, 256, 0, c->stream>>>(c->nhalf, kxh, c->fft[0], (float2*)c->cgrid,
+                                                              (const float*)c->infl, (double)c->ngrid, c->acc,
+                                                              eflag ? 1 : 0);
+    }
+    {
+        Launch L(c, "pme_fft_c2r");
+        if (c->precision == SIMOX_FP64)
+            r = cufftExecZ2D(c->plan_c2r, (cufftDoubleComplex*)c->cgrid, (cufftDoubleReal*)c->grid);
+        else
+            r = cufftExecC2R(c->plan_c2r, (cufftComplex*)c->cgrid, (cufftReal*)c->grid);
+    }
+    if (r != CUFFT_SUCCESS) return SIMOX_E_CUDA;
+    return SIMOX_OK;
+}
+
+static PmeParams pme_params(const simox_ctx* c) {
+    PmeParams S;
+    S.K = make_int3(c->fft[0], c->fft[1], c->fft[2]);
+    S.box = make_double3(c->box[0], c->box[1], c->box[2]);
+    S.kx = make_double3(c->fft[0] / c->box[0], c->fft[1] / c->box[1], c->fft[2] / c->box[2]);
+    double V = c->box[0] * c->box[1] * c->box[2];
+    S.cst = SX_KC * (double)c->fft[0] * (double)c->fft[1] * (double)c->fft[2] / V / SX_PI;
+    S.n = c->n;
+    return S;
+}
+
+template <typename R, int P>
+static int pme_forces_t(simox_ctx* c) {
+    PmeParams S = pme_params(c);
+    run_spread<R, P>(c, S, nullptr);
+    int st = run_convolution(c, true);
+    if (st) return st;
+    Launch L(c, "pme_gather_force");
+    gather_force_kernel<R, P><<<(S.n + 127) / 128, 128, 0, c->stream>>>(S, c->xq_s, (const R*)c->grid, c->sorted,
+                                                                        c->f, c->acc);
+    return SIMOX_OK;
+}
+
+template <typename R, int P>
+static int pme_pot_t(simox_ctx* c, const double* qalt, double* phi, double scale) {
+    PmeParams S = pme_params(c);
+    run_spread<R, P>(c, S, qalt);
+    int st = run_convolution(c, false);
+    if (st) return st;
+    Launch L(c, "pme_gather_pot");
+    gather_pot_kernel<R, P><<<(S.n + 127) / 128, 128, 0, c->stream>>>(S, c->xq_s, (const R*)c->grid, phi, scale);
+    return SIMOX_OK;
+}
+
+// mean-force removal (force.f90:457-460)
+__global__ void subtract_mean_kernel(int n, double* __restrict__ f, const double* __restrict__ acc) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    // Fsum(:) = Fsum(:)/DBLE(Npt_all); ff = ff - Fsum   (force.f90:457-459)
+    f[3 * i] = __dsub_rn(f[3 * i], __ddiv_rn(acc[A_FSUM0], (double)n));
+    f[3 * i + 1] = __dsub_rn(f[3 * i + 1], __ddiv_rn(acc[A_FSUM1], (double)n));
+    f[3 * i + 2] = __dsub_rn(f[3 * i + 2], __ddiv_rn(acc[A_FSUM2], (double)n));
+}
+
+int pme_finalize_forces(simox_ctx* c) {
+    if (c->n == 0) return SIMOX_OK;
+    Launch L(c, "pme_mean_force");
+    subtract_mean_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->n, c->f, c->acc);
+    return check_launch(c);
+}
+
+int pme_forces(simox_ctx* c, bool finalize) {
+    if (!c->psi_valid) return SIMOX_E_STATE;
+    if (!c->gathered) {
+        int st = gather_sorted(c);
+        if (st) return st;
+    }
+    if (c->n == 0) return SIMOX_OK;
+    cudaMemsetAsync(c->acc + A_FSUM0, 0, 3 * sizeof(double), c->stream);
+    int st;
+    const bool dbl = c->precision == SIMOX_FP64;
+    switch (c->order) {
+        case 4: st = dbl ? pme_forces_t<double, 4>(c) : pme_forces_t<float, 4>(c); break;
+        case 6: st = dbl ? pme_forces_t<double, 6>(c) : pme_forces_t<float, 6>(c); break;
+        case 8: st = dbl ? pme_forces_t<double, 8>(c) : pme_forces_t<float, 8>(c); break;
+        default: return SIMOX_E_ARG;
+    }
+    if (st) return st;
+    if (finalize) {
+        st = pme_finalize_forces(c);
+        if (st) return st;
+    }
+    return check_launch(c);
+}
+
+int pme_potential(simox_ctx* c, const double* qalt, double* phi, double scale) {
+    if (!c->psi_valid) return SIMOX_E_STATE;
+    if (c->n == 0) return SIMOX_OK;
+    const bool dbl = c->precision == SIMOX_FP64;
+    int st;
+    switch (c->order) {
+        case 4: st = dbl ? pme_pot_t<double, 4>(c, qalt, phi, scale) : pme_pot_t<float, 4>(c, qalt, phi, scale); break;
+        case 6: st = dbl ? pme_pot_t<double, 6>(c, qalt, phi, scale) : pme_pot_t<float, 6>(c, qalt, phi, scale); break;
+        case 8: st = dbl ? pme_pot_t<double, 8>(c, qalt, phi, scale) : pme_pot_t<float, 8>(c, qalt, phi, scale); break;
+        default: return SIMOX_E_ARG;
+    }
+    if (st) return st;
+    return check_launch(c);
+}
+
+}  // namespace sx

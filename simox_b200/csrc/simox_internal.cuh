@@ -1,0 +1,256 @@
+// simox_internal.cuh -- device context, pair-parameter tables and helpers of
+// the B200 force / charge path.  Internal to libsimox_b200.so.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <cstdint>
+#include <cstddef>
+#include <string>
+#include <vector>
+
+#include "simox_gpu.h"
+
+#define SX_KC     14.399644154020082   // datafmt.f90:23
+#define SX_TFM    10.180505306645389   // datafmt.f90:24
+#define SX_PI     3.1415926535897931   // datafmt.f90:25
+#define SX_SQRTPI 1.7724538509055159   // datafmt.f90:26
+#define SX_WPEN   20.0                 // datafmt.f90:28 (w)
+
+namespace sx {
+
+constexpr int kSpecies = 4;           // Al, Ni, Fe, O on the device tables (H is rejected)
+constexpr int kMaxOrder = 8;
+constexpr int kEntries = 27;          // self + 13 forward + 13 reverse stencil cells
+constexpr unsigned kIsA = 0x80000000u;  // list entry bit: this atom is the reference's "i"
+constexpr unsigned kIdxMask = 0x7fffffffu;
+
+// Device status bits (OR-ed by kernels, read by the host after a call).
+enum : int {
+    ST_CELL_OVERFLOW = 1, ST_NBR_OVERFLOW = 2, ST_UNKNOWN_PAIR = 4, ST_UNKNOWN_ELEMENT = 8,
+    ST_POSITION = 16, ST_UNSUPPORTED = 32, ST_LINE_NOBRACKET = 64   // Brent: 100 steps without convergence
+};
+
+// Slots of the FP64 accumulator array (energies and reductions).
+enum : int {
+    A_EPAIR = 0, A_EDIR, A_ECTIP, A_EGROUP, A_EREC, A_FSUM0, A_FSUM1, A_FSUM2,
+    A_MV2, A_MV2S0, A_MV2S1 = A_MV2S0 + 1, A_MV2S4 = A_MV2S0 + 4, A_NS0, A_NS4 = A_NS0 + 4,
+    // CTIP
+    A_GSUM, A_PSUM, A_PMAX, A_GP, A_PAP, A_QSUM, A_Q2SUM, A_ESUM, A_NACT,
+    A_LINE0,                    // 32 line-search samples
+    A_COUNT = A_LINE0 + 32
+};
+
+// Uniform pair table: entry [X][Y] holds everything atom X needs about a
+// partner Y.  All EAM forms of eam.f90 used on the Al/Ni/Fe-O path are sums of
+// Zhou terms  g(r) = exp(-c (r/re - 1)) / (1 + (r/re - lam)^20).
+template <typename R>
+struct PairTab {
+    // density at X contributed by Y (force.f90:84-85 with eam.f90 fj)
+    R d_fe, d_inv_re, d_c, d_lam;
+    // density at Y contributed by X
+    R e_fe, e_inv_re, e_c, e_lam;
+    // pair potential phi = A gA - B gB
+    R p_inv_re, p_A, p_alpha, p_kappa, p_B, p_beta, p_lambda;
+    // CTIP (force.f90:101-140): xi, Z of X and Y; fifj = -(eX PX(r) + eY PY(r)),
+    // dfifj/dr = eX QX(r) + eY QY(r) with P = c0 + c1 r + c2 r^2 + c3 r^3 + cm1/r
+    // and Q = d0 + d1 r + d2 r^2 + dm1/r + dm2/r^2; eS = exp(-2 xi_S r).
+    R xi_x, xi_y, Z_x, Z_y;
+    R Px[5], Py[5], Qx[5], Qy[5];
+    // CTIP solver coefficients (ctip.f90:85-110): fifj_s = -(eX SX(r) + eY SY(r))/r
+    // with S = s0 + s1 r + s2 r^2 + s3 r^3 (as-written CTIP_SOLVER form).
+    R Sx[4], Sy[4];
+    int valid;          // 0: the pair form is not on the GPU path
+    int pad_;
+};
+
+struct Profile {
+    std::vector<std::string> names;
+    std::vector<double> ms;
+    std::vector<long long> launches;
+};
+
+}  // namespace sx
+
+struct simox_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    simox_setup setup{};
+    simox_potential pot{};
+    int n = 0, cap = 0;
+    int precision = SIMOX_FP64;
+    int flags = 0;
+    double box[3]{}, inv_box[3]{}, hbox[3]{};
+    double rcut = 0, rcut2 = 0, a = 0, dr_rdf = 0;
+    int nc[3]{}, ncell = 0;
+    double lc[3]{};
+    bool fast_cells = false;
+    int fft[3]{}, order = 4;
+    size_t ngrid = 0, nhalf = 0;
+    int npt_max = SIMOX_NPT_MAX, nnb_cap = 1024;
+
+    // species present
+    bool has_h = false;
+
+    // original-order state
+    int* id = nullptr;          // species 1..5
+    double* x = nullptr;        // [cap][3]
+    double* v = nullptr;
+    double* f = nullptr;
+    double* q = nullptr;
+    double* xm = nullptr;       // per-atom mass (from species)
+
+    // cells
+    int* cell_of = nullptr;     // [cap]
+    int* cell_count = nullptr;  // [ncell]
+    int* cell_start = nullptr;  // [ncell+1]
+    int* cell_fill = nullptr;   // [ncell]
+    int* sorted = nullptr;      // [cap] original index of sorted slot
+    int* pair13 = nullptr;      // [ncell*13] 1-based (reference layout)
+    int* entries = nullptr;     // [ncell*27] cell | dir<<28
+    std::vector<int> h_pair13;
+
+    // sorted copies
+    double4* xq_s = nullptr;    // x, y, z, q
+    int* t_s = nullptr;         // species 0..4
+
+    // neighbour list
+    int* nn = nullptr;
+    unsigned* nbr = nullptr;    // [cap*nnb_cap]
+    int* nn_max = nullptr;      // device max
+    unsigned long long* nn_tot = nullptr;
+
+    // EAM
+    double* rho_s = nullptr;
+    double* dF_s = nullptr;
+
+    // pair tables
+    sx::PairTab<double>* tab_d = nullptr;
+    sx::PairTab<float>* tab_f = nullptr;
+
+    // PME
+    cufftHandle plan_r2c = 0, plan_c2r = 0;
+    bool plans = false;
+    void* grid = nullptr;       // real grid (double or float)
+    void* cgrid = nullptr;      // half-spectrum complex grid
+    void* infl = nullptr;       // G/N on the half spectrum (double or float)
+    double* psi = nullptr;      // full-grid psi (reference layout)
+    double* bmod = nullptr;     // per-dimension 1/|b|^2, K1+K2+K3
+
+    // CTIP
+    double* c_const = nullptr;  // chi + sum Z asym (sorted)
+    double* g = nullptr;        // -dU/dq (sorted)
+    double* pv = nullptr;       // direction (sorted)
+    double* Ap = nullptr;       // A p (sorted)
+    double* qs = nullptr;       // charges (sorted, FP64)
+    double* jp = nullptr;       // J' per sorted atom
+    int* act = nullptr;         // active-set indices
+    double* line = nullptr;     // line search scalars (bracket, alpha, ...)
+
+    // reductions / status
+    double* acc = nullptr;      // [A_COUNT]
+    double* h_acc = nullptr;    // pinned mirror
+    int* status = nullptr;
+    int* h_status = nullptr;    // pinned
+    int* rdf = nullptr;         // [SIMOX_RDF_LEN]
+
+    // validity
+    bool have_ids = false, cells_valid = false, gathered = false, list_valid = false, psi_valid = false;
+    bool eam_valid = false;
+
+    // timing / counters
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    bool profiling = false;
+    sx::Profile prof;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
+    long long launches = 0;
+    double eself = 0.0;         // sys%Eself of the last PME_SELF or CTIP_SOLVER
+    int last_max_nnb = 0;
+    long long last_tot_nnb = 0;
+};
+
+// ---------------------------------------------------------------------------
+// host-side helpers shared between translation units
+namespace sx {
+
+int cuda_status(cudaError_t e);
+int check_launch(simox_ctx* c);
+int read_status(simox_ctx* c);          // sync + convert device status bits
+int profile_id(simox_ctx* c, const char* name);
+void prof_begin(simox_ctx* c, int id, cudaEvent_t* a, cudaEvent_t* b);
+void prof_end(simox_ctx* c, int id, cudaEvent_t a, cudaEvent_t b);
+void prof_collect(simox_ctx* c);
+int num_sms(simox_ctx* c);
+
+// RAII-like launch bracket for per-family timing
+struct Launch {
+    simox_ctx* c; int id; cudaEvent_t a = nullptr, b = nullptr;
+    Launch(simox_ctx* c_, const char* name) : c(c_), id(-1) {
+        c->launches++;
+        if (c->profiling) { id = profile_id(c, name); prof_begin(c, id, &a, &b); }
+    }
+    ~Launch() { if (id >= 0) prof_end(c, id, a, b); }
+};
+
+// cells.cu
+int build_cell_tables(simox_ctx* c);
+int cell_sort(simox_ctx* c);
+int gather_sorted(simox_ctx* c);
+int build_list(simox_ctx* c);
+int ensure_list(simox_ctx* c);
+// pair.cu
+int build_pair_tables(simox_ctx* c);
+int eam_density(simox_ctx* c, bool eflag);
+int pair_forces(simox_ctx* c, bool eflag, bool rdf);
+// pme.cu
+int pme_setup(simox_ctx* c);
+int pme_free(simox_ctx* c);
+int pme_self(simox_ctx* c);
+int pme_forces(simox_ctx* c, bool finalize);
+int pme_potential(simox_ctx* c, const double* charges_sorted, double* phi_out, double scale);
+int pme_finalize_forces(simox_ctx* c);
+// ctip.cu
+int ctip_solve(simox_ctx* c, int max_cg, simox_ctip_report* rep);
+int ctip_alloc(simox_ctx* c);
+// integrate.cu
+int vv1(simox_ctx* c, double dt, bool reflect);
+int vv2(simox_ctx* c, double dt, bool subtract_mean);
+int nvt2_berend(simox_ctx* c, double dt, double T_given, bool subtract_mean);
+int update_masses(simox_ctx* c);
+// md
+int md_run(simox_ctx* c, const simox_md_opts* o, int first, int nsteps, simox_energies* e, int* rdf);
+
+// device helpers -------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float warp_sumf(float v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Block-wide sum of one double into acc[slot] (one atomic per block).
+template <int NT>
+__device__ __forceinline__ void block_add(double v, double* acc, int slot, double* sm) {
+    v = warp_sum(v);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sm[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        double t = l < NT / 32 ? sm[l] : 0.0;
+        t = warp_sum(t);
+        if (l == 0 && t != 0.0) atomicAdd(acc + slot, t);
+    }
+}
+
+// DNINT: round half away from zero (vverlet.f90:92, force.f90:52)
+__device__ __forceinline__ double dnint(double x) { return round(x); }
+
+}  // namespace sx

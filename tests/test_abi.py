@@ -1,0 +1,61 @@
+"""C-ABI library checks that need no GPU: it loads, exports every entry
+point include/simox_gpu.h declares, and its host-only helpers agree with the
+oracle."""
+import os
+import re
+
+import numpy as np
+
+from simox_b200 import _abi
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "simox_gpu.h")
+
+
+def declared_symbols():
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(simox_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_header_declarations_listed():
+    assert declared_symbols() == sorted(_abi.EXPORTED)
+
+
+def test_library_exports_every_symbol(simox_lib):
+    for name in declared_symbols():
+        assert hasattr(simox_lib, name), name
+
+
+def test_status_strings_match(simox_lib):
+    for code in range(0, -17, -1):
+        assert simox_lib.simox_status_string(code).decode() == _abi.status_text(code)
+
+
+def test_default_potential_equals_oracle(simox_lib):
+    from simox_b200 import api
+    from oracle import oracle as O
+    assert _abi.potential_to_bytes(api.default_potential()) == _abi.potential_to_bytes(O.potential_setup())
+
+
+def test_create_without_gpu_reports_status(simox_lib):
+    """No GPU here: create must return a status, not crash or fall back."""
+    import ctypes as C
+    from simox_b200.api import _vp
+    s = _abi.Setup()
+    s.n_atoms = 2
+    s.box[:] = [30.0, 30.0, 30.0]
+    s.fft[:] = [16, 16, 16]
+    s.pme_order = 4
+    s.rcut = 10.0
+    ctx = _vp()
+    st = simox_lib.simox_create(C.byref(s), None, C.byref(ctx))
+    try:
+        import torch
+        has = torch.cuda.is_available()
+    except Exception:
+        has = False
+    if not has:
+        assert st == _abi.SIMOX_E_NO_DEVICE
+    else:
+        assert st == 0
+        simox_lib.simox_destroy(ctx)

@@ -1,0 +1,229 @@
+"""GPU parity: libsimox_b200.so (through the C ABI) against the FP64 oracle.
+
+Bars (written in each test):
+  * cell lists, neighbour membership, RDF histogram (FP64 path): bit-exact;
+  * FP64 path forces / energies / rho / F': relative 1e-9;
+  * mixed path forces: ||dF||/||F|| <= 1e-5 (the FP32 pair + PME bar);
+  * CTIP charges: |dq| <= 1e-6 e with the same CG iteration count;
+  * integrator kernels given identical forces: bit-exact.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from simox_b200 import _abi, systems as S
+from tests.helpers import gpu_context, oracle_system, rel_err, small_cases
+
+pytestmark = pytest.mark.gpu
+
+CASES = small_cases()
+IDS = [c[0] for c in CASES]
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _lib(simox_lib):
+    return simox_lib
+
+
+@pytest.mark.parametrize("name,s", CASES, ids=IDS)
+def test_cell_sort_bit_exact(name, s):
+    o = oracle_system(s)
+    npt_o, link_o = o.cell_sort()
+    with gpu_context(s) as g:
+        nc, pair = g.cell_hierarchy()
+        assert np.array_equal(nc, o.nc)
+        assert np.array_equal(pair, o.pair)          # CELL_HIERARCHY
+        g.cell_sort()
+        npt, link = g.get_cells(link_stride=link_o.shape[1])
+    assert np.array_equal(npt, npt_o)
+    for c in range(len(npt)):
+        assert np.array_equal(link[c, : npt[c]], link_o[c, : npt_o[c]]), c
+
+
+def test_cell_sort_boundaries_bit_exact():
+    """Atoms placed exactly on cell faces and at +-L/2 bin like INT/MOD do."""
+    s = S.small_alo(seed=11, n=400, box=(30.0, 33.0, 36.3), fft=(24, 24, 24))
+    nc, lc, _ = O.cell_grid(s.box, s.rcut)
+    x = s.x.copy()
+    k = 0
+    for d in range(3):
+        for m in range(int(nc[d]) + 1):
+            x[k, d] = -s.box[d] / 2 + m * lc[d]
+            k += 1
+    x[k] = -s.box / 2
+    x[k + 1] = np.nextafter(s.box / 2, 0)
+    s.x = x
+    o = oracle_system(s)
+    npt_o, link_o = o.cell_sort()
+    with gpu_context(s) as g:
+        g.cell_sort()
+        npt, link = g.get_cells(link_stride=link_o.shape[1])
+    assert np.array_equal(npt, npt_o)
+    for c in range(len(npt)):
+        assert np.array_equal(link[c, : npt[c]], link_o[c, : npt_o[c]])
+
+
+@pytest.mark.parametrize("name,s", CASES, ids=IDS)
+def test_force_fp64(name, s):
+    o = oracle_system(s)
+    o.cell_sort()
+    f_o, e_o, rho_o, dF_o, rdf_o = o.force(rdf=True)
+    rdf = np.zeros(_abi.RDF_LEN, np.int32)
+    with gpu_context(s) as g:
+        g.cell_sort()
+        e = g.force(rdf=rdf)
+        st = g.get_state()
+        rho, dF = g.get_eam()
+    fmax = np.abs(f_o).max()
+    assert np.abs(st["f"] - f_o).max() <= 1e-9 * fmax
+    for k in ("Epair", "Edir", "Ectip", "Egroup"):
+        assert abs(e[k] - e_o[k]) <= 1e-9 * max(1.0, abs(e_o[k])), (k, e[k], e_o[k])
+    assert np.abs(rho - rho_o).max() <= 1e-10 * np.abs(rho_o).max()
+    assert np.abs(dF - dF_o).max() <= 1e-9 * max(1.0, np.abs(dF_o).max())
+    assert np.array_equal(rdf, rdf_o)                 # bit-exact histogram
+
+
+@pytest.mark.parametrize("name,s", CASES, ids=IDS)
+def test_pme_self_and_pme_fp64(name, s):
+    o = oracle_system(s)
+    es_o = o.pme_self()
+    f_o, erec_o = o.pme()
+    with gpu_context(s) as g:
+        es = g.pme_self()
+        psi = g.get_psi()
+        g.cell_sort()
+        g.set_state(f=np.zeros((s.n, 3)))
+        erec = g.pme()
+        f = g.get_state()["f"]
+    assert abs(es - es_o) <= 1e-11 * abs(es_o)
+    assert np.abs(psi - o.psi).max() <= 1e-14 * np.abs(o.psi).max()
+    assert abs(erec - erec_o) <= 1e-10 * abs(erec_o)
+    assert np.abs(f - f_o).max() <= 1e-9 * np.abs(f_o).max()
+
+
+@pytest.mark.parametrize("name,s", CASES[:2], ids=IDS[:2])
+def test_ctip_fp64(name, s):
+    o = oracle_system(s)
+    o.pme_self()
+    o.cell_sort()
+    es_o, ncg_o, _, err_o = o.ctip()
+    with gpu_context(s) as g:
+        g.pme_self()
+        g.cell_sort()
+        es, rep = g.ctip_solver()
+        q = g.get_state()["q"]
+    assert rep["n_cg"] == ncg_o, (rep, ncg_o)
+    assert np.abs(q - o.q).max() <= 1e-6
+    assert abs(rep["q_sum"] - s.q.sum()) <= 1e-9 * max(1.0, np.abs(s.q).sum())   # projection keeps the total
+    assert abs(es - es_o) <= 1e-6 * abs(es_o)
+
+
+@pytest.mark.parametrize("name,s", CASES[:2], ids=IDS[:2])
+def test_force_mixed(name, s):
+    o = oracle_system(s)
+    o.cell_sort()
+    o.pme_self()
+    f_o, e_o, *_ = o.force()
+    f_o, erec_o = o.pme(f_o)
+    with gpu_context(s, precision="mixed") as g:
+        g.pme_self()
+        g.cell_sort()
+        e = g.force()
+        erec = g.pme()
+        f = g.get_state()["f"]
+    assert rel_err(f, f_o) <= 1e-5, rel_err(f, f_o)
+    etot_o = sum(e_o.values()) + erec_o
+    etot = sum(e.values()) + erec
+    assert abs(etot - etot_o) / s.n <= 1e-6, (etot, etot_o)
+
+
+def test_integrators_bit_exact():
+    s = S.small_alo(seed=5, n=300, box=(30.5, 31.0, 32.0), fft=(16, 16, 16))
+    rng = np.random.default_rng(0)
+    f = rng.normal(0, 1.0, (s.n, 3))
+    dt = 1.0 / S.TFM
+    o = oracle_system(s)
+    with gpu_context(s) as g:
+        g.set_state(f=f)
+        # VV_NVE1
+        v1 = o.vv_nve1(s.v, f, dt)
+        g.vv_nve1(dt)
+        st = g.get_state()
+        assert np.array_equal(st["x"], o.x) and np.array_equal(st["v"], v1)
+        # VV_NVE2
+        v2, mv2_o = o.vv_nve2(v1, f, dt)
+        mv2 = g.vv_nve2(dt)
+        assert np.array_equal(g.get_state()["v"], v2)
+        assert abs(mv2 - mv2_o) <= 1e-12 * mv2_o
+        # VV_NVT2_BEREND
+        v3, mv3_o = o.vv_nvt2_berend(v2, f, dt, 600.0 * S.KB)
+        mv3 = g.vv_nvt2_berend(dt, 600.0 * S.KB)
+        assert np.allclose(g.get_state()["v"], v3, rtol=1e-14, atol=0)
+        assert abs(mv3 - mv3_o) <= 1e-12 * mv3_o
+        # VV_NVE1_REFLECT
+        v4 = o.vv_nve1(v3, f, dt, reflect=True)
+        g.set_state(v=v3)
+        g.vv_nve1(dt, reflect=True)
+        st = g.get_state()
+        assert np.array_equal(st["x"], o.x) and np.array_equal(st["v"], v4)
+
+
+def test_md_steps_fp64_vs_oracle():
+    """Three steps of the regular loop (VV1, CELL_SORT, FORCE, PME, VV2)."""
+    s = S.small_alo(seed=12, n=500, box=(31.0, 32.0, 33.0), fft=(24, 24, 24), order=4)
+    dt = 1.0 / S.TFM
+    o = oracle_system(s)
+    o.pme_self()
+    o.cell_sort()
+    f, *_ = o.force()
+    f, _ = o.pme(f)
+    v = s.v.copy()
+    with gpu_context(s) as g:
+        g.pme_self()
+        g.cell_sort()
+        g.force()
+        g.pme()
+        for step in range(1, 4):
+            v = o.vv_nve1(v, f, dt)
+            o.cell_sort()
+            f, e_o, *_ = o.force()
+            f, erec_o = o.pme(f)
+            v, mv2_o = o.vv_nve2(v, f, dt)
+        e = g.md_run(3, dt, first_step=1, freq_new=0, freq_sort=1)
+        st = g.get_state()
+    assert np.abs(st["x"] - o.x).max() <= 1e-10
+    assert np.abs(st["v"] - v).max() <= 1e-9 * np.abs(v).max()
+    assert abs(e["mv2"] - mv2_o) <= 1e-9 * mv2_o
+    assert abs(e["Erec"] - erec_o) <= 1e-8 * abs(erec_o)
+
+
+def test_status_codes():
+    """Limit breaches come back as the reference's STOP texts, not faults."""
+    from simox_b200.api import SimoxError
+    s = S.small_alo(seed=4, n=600, box=(31.0, 32.0, 33.0), fft=(24, 24, 32))
+    # per-cell capacity of 5 -> "=== Cell particle limit crashed !!! ==="
+    with gpu_context(s, npt_max=5) as g:
+        with pytest.raises(SimoxError) as ei:
+            g.cell_sort()
+        assert ei.value.code == _abi.SIMOX_E_CELL_OVERFLOW
+    # neighbour capacity 8 -> "=== neighbor particle limit crashed !!! ==="
+    with gpu_context(s, nnb_max=8) as g:
+        g.cell_sort()
+        with pytest.raises(SimoxError) as ei:
+            g.force()
+        assert ei.value.code == _abi.SIMOX_E_NBR_OVERFLOW
+    # a hydrogen atom -> "=== Unknown particle pair ==="
+    s2 = s.copy()
+    s2.ids[0] = 5
+    with gpu_context(s2) as g:
+        g.cell_sort()
+        with pytest.raises(SimoxError) as ei:
+            g.force()
+        assert ei.value.code in (_abi.SIMOX_E_UNKNOWN_PAIR, _abi.SIMOX_E_UNKNOWN_ELEMENT)
+    # a NaN coordinate is reported, not binned
+    s3 = s.copy()
+    s3.x[3, 1] = np.nan
+    with gpu_context(s3) as g:
+        with pytest.raises(SimoxError) as ei:
+            g.cell_sort()
+        assert ei.value.code == _abi.SIMOX_E_POSITION
