@@ -1,0 +1,429 @@
+#!/usr/bin/env python
+"""Benchmark: atom-steps/s of SIMOX's per-step force and charge path on B200.
+
+Workload (the 128k bulk-oxide configuration): alpha-Al2O3 corundum supercell
+of 20x14x8 orthohexagonal cells, 128,000 atoms after 4.8 % random vacancies
+(Al:O = 2:3), PME 128^3 with order-6 B-splines, Rcut 10 A, NVT Berendsen at
+600 K, dt = 1 fs, cell sort every step.  Charges are equilibrated by
+CTIP_SOLVER at step 1 (TAG_SET with freq_new larger than the run, inside the
+warm-up); the timed steps are VV_NVE1, CELL_SORT, FORCE, PME and
+VV_NVT2_BEREND of main.f90:41-61 with energies and the RDF accumulated every
+step, as the reference does.  Synthetic seeded input (no dataset exists).
+
+One step = one pass of that loop over all 128,000 atoms.  ``value`` is the
+mixed-precision path (FP32 pair and PME terms, FP64 sums) with device-resident
+inputs; ``fp64`` reports the all-FP64 path on the same input.  ``e2e`` goes
+through the C ABI with host buffers: per step simox_set_state from pinned host
+memory, one step, simox_get_state back (x, v, f, q both ways).
+
+Multi-GPU: replicas only (one independent system per rank, weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "atom-steps/s @128k Al/O: mixed vs FP64 on B200 (force err≤1e-5), CPU ref"
+UNIT = "atom-steps/s"
+WORKLOAD = "corundum Al2O3 128000 atoms, PME 128^3 order 6, Rcut 10 A, NVT Berendsen 600 K, dt 1 fs"
+FREQ_NEW = 1000000          # CTIP at step 1 only (warm-up)
+
+
+def dist_info():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def init_dist(world, backend):
+    if world <= 1:
+        return None
+    import torch.distributed as dist
+    from datetime import timedelta
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group(backend=backend, timeout=timedelta(seconds=300))
+    return dist
+
+
+def reduce_max(dist, v, device=None):
+    """Max of a float over ranks (identity for one rank)."""
+    if dist is None:
+        return float(v)
+    import torch
+    t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist, device=None):
+    if dist is None:
+        return
+    if device is not None and str(device).startswith("cuda"):
+        dist.barrier(device_ids=[int(str(device).split(":")[1])])
+    else:
+        dist.barrier()
+
+
+# --------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index=0):
+        self.proc = None
+        self.idx = gpu_index
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if p[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "of measured"
+    except Exception:
+        return 6650.0, "of fallback"
+
+
+def profile_traffic(kernel):
+    """DRAM bytes per launch of ``kernel`` from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_corundum128k.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+# Algorithmic bytes per launch of each kernel family (unique bytes a launch
+# must move: per-atom state in and out plus its neighbour-list row).  n atoms,
+# nnb mean neighbours, K grid points, p spline order.
+def algorithmic_bytes(name, n, nnb, K, prec):
+    r = 8 if prec == "fp64" else 4
+    if name == "pair_force":      # xq 32, type 4, count 4, F' 8, list 4*nnb in; force 24 out
+        return n * (32 + 4 + 4 + 8 + 4 * nnb + 24)
+    if name == "eam_density":     # xq 32, type 4, count 4, list 4*nnb in; rho, F' 16 out
+        return n * (32 + 4 + 4 + 4 * nnb + 16)
+    if name == "neighbor_list":   # positions 32 in, list 4*nnb + count 4 out
+        return n * (32 + 4 * nnb + 4)
+    if name == "pme_spread":      # xq 32 in, grid K r out
+        return n * 32 + K * r
+    if name == "pme_gather_force":
+        return n * (32 + 4 + 48) + K * r
+    if name in ("pme_fft_r2c", "pme_fft_c2r"):
+        return 2 * K * r * 2
+    return None
+
+
+# --------------------------------------------------------------------------
+def build_system(seed=2):
+    from simox_b200 import systems as S
+    return S.corundum(seed=seed)
+
+
+def equilibrated_context(s, precision, device=0):
+    """Context with PME_SELF, CELL_SORT, initial FORCE/PME and the step-1
+    CTIP solve done (the first warm-up step)."""
+    from simox_b200 import api
+    g = api.from_system(s, precision=precision, device=device)
+    g.pme_self()
+    g.cell_sort()
+    g.force()
+    g.pme()
+    return g
+
+
+def run_md(g, s, first, nsteps, rdf):
+    from simox_b200 import systems as S
+    return g.md_run(nsteps, 1.0 / S.TFM, first_step=first, thermostat=True, T_given=600.0 * S.KB,
+                    freq_new=FREQ_NEW, freq_sort=1, rdf=rdf)
+
+
+def time_device(g, s, steps, warmup, dist, device):
+    """W warm-up steps (step 1 runs CTIP), then K steps between events."""
+    from simox_b200 import _abi
+    rdf = np.zeros(_abi.RDF_LEN, np.int32)
+    t0 = time.perf_counter()
+    run_md(g, s, 1, warmup, rdf)
+    g.sync()
+    warm_s = time.perf_counter() - t0
+    barrier(dist, device)
+    g.sync()
+    l0 = g.launch_count()
+    g.timer_begin()
+    e = run_md(g, s, warmup + 1, steps, rdf)
+    ms = g.timer_end()
+    g.sync()
+    launches = g.launch_count() - l0
+    barrier(dist, device)
+    return ms, e, launches, warm_s
+
+
+def time_e2e(g, s, steps, first):
+    """Through the C ABI with host buffers: set_state (pinned host -> device),
+    one step, get_state (device -> pinned host), every step."""
+    import torch
+    n = s.n
+    pin = lambda shape: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+    x, v, f, q = pin((n, 3)), pin((n, 3)), pin((n, 3)), pin((n,))
+    st = g.get_state()
+    x[:], v[:], f[:], q[:] = st["x"], st["v"], st["f"], st["q"]
+    from simox_b200 import api
+    L = api.lib()
+    ctx = g._ctx
+    dp = api._dp
+    xs, vs, fs, qs = (a.ctypes.data_as(dp) for a in (x, v, f, q))
+    from simox_b200 import _abi
+    rdf = np.zeros(_abi.RDF_LEN, np.int32)
+    g.sync()
+    t0 = time.perf_counter()
+    for k in range(steps):
+        rc = L.simox_set_state(ctx, n, None, xs, vs, fs, qs)
+        if rc:
+            raise RuntimeError(f"set_state {rc}")
+        run_md(g, s, first + k, 1, rdf)
+        rc = L.simox_get_state(ctx, n, None, xs, vs, fs, qs)
+        if rc:
+            raise RuntimeError(f"get_state {rc}")
+    dt = time.perf_counter() - t0
+    nbytes = n * (3 + 3 + 3 + 1) * 8
+    return dt, nbytes
+
+
+def profile_steps(g, s, steps, first):
+    g.profile(True)
+    g.profile_reset()
+    run_md(g, s, first, steps, None)
+    prof = g.profile_read()
+    g.profile(False)
+    return prof
+
+
+def cpu_baseline_sample(s, timeout_s=120.0):
+    """The oracle (FP64 C restatement, one thread) on one full MD step of the
+    same system: VV_NVE1, CELL_SORT, FORCE, PME, VV_NVT2_BEREND."""
+    from oracle import oracle as O
+    from simox_b200 import systems as S
+    o = O.System(s.ids, s.x, s.q, s.box, s.rcut, s.fft, order=s.order, nnb_max=640)
+    o.pme_self()
+    o.cell_sort()
+    f, *_ = o.force()
+    f, _ = o.pme(f)
+    dt = 1.0 / S.TFM
+    t0 = time.perf_counter()
+    v = o.vv_nve1(s.v, f, dt)
+    o.cell_sort()
+    f, *_ = o.force()
+    f, _ = o.pme(f)
+    v, _ = o.vv_nvt2_berend(v, f, dt, 600.0 * S.KB)
+    el = time.perf_counter() - t0
+    return el
+
+
+def run_reference(args):
+    """--impl reference: the reference's path on host cores.  The Fortran
+    reference cannot be compiled here (no Fortran compiler), so this times
+    the oracle port of it (FP64, single thread, as the serial reference)."""
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return 0
+    s = build_system()
+    from oracle import oracle as O
+    from simox_b200 import systems as S
+    o = O.System(s.ids, s.x, s.q, s.box, s.rcut, s.fft, order=s.order, nnb_max=640)
+    o.pme_self()
+    o.cell_sort()
+    f, *_ = o.force()
+    f, _ = o.pme(f)
+    dt = 1.0 / S.TFM
+    v = s.v.copy()
+    nsteps = max(1, min(args.steps, 3))
+    warm = 1 if args.warmup > 0 else 0
+
+    def step(v, f):
+        v = o.vv_nve1(v, f, dt)
+        o.cell_sort()
+        f, *_ = o.force(rdf=True)
+        f, _ = o.pme(f)
+        v, _ = o.vv_nvt2_berend(v, f, dt, 600.0 * S.KB)
+        return v, f
+
+    for _ in range(warm):
+        v, f = step(v, f)
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        v, f = step(v, f)
+    el = time.perf_counter() - t0
+    val = s.n * nsteps / el
+    sample = (f"{nsteps} timed step(s) after {warm} warm-up of the full 128,000-atom step "
+              f"(VV_NVE1, CELL_SORT, FORCE, PME, VV_NVT2_BEREND) on 1 host thread; "
+              f"oracle port of the Fortran (no Fortran compiler on this image)")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": nsteps, "warmup": warm, "ms_per_step": el / nsteps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_atoms": s.n},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-fp64", action="store_true", help="skip the all-FP64 comparison run")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--ncu", action="store_true",
+                    help="profiling run: set-up, then --steps MD steps of the workload (charges as "
+                         "generated, no CTIP, no comparison runs); prints nothing else")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="precision of --ncu")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    if args.ncu:
+        from simox_b200 import build
+        build.build()
+        s = build_system()
+        g = equilibrated_context(s, args.precision)
+        run_md(g, s, 2, args.steps, None)
+        g.sync()
+        g.close()
+        return 0
+    args.warmup = max(args.warmup, 3)
+
+    rank, world, local = dist_info()
+    import torch
+    device = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    dist = init_dist(world, "nccl")
+
+    from simox_b200 import build
+    build.build()
+    s = build_system(seed=2 + rank)
+
+    # mixed path (the headline)
+    g = equilibrated_context(s, "mixed", device=local)
+    clocks = ClockSampler(local)
+    ms, e, launches, warm_s = time_device(g, s, args.steps, args.warmup, dist, device)
+    clk = clocks.stop()
+    ms_max = reduce_max(dist, ms, device)
+    value = world * s.n * args.steps / (ms_max / 1e3)
+    mx_nnb, tot_nnb = g.neighbor_stats()
+    nnb = tot_nnb / s.n
+
+    # e2e through the C ABI with host buffers
+    e2e_s, nbytes = time_e2e(g, s, max(3, args.steps // 2), args.warmup + args.steps + 1)
+    e2e_s = reduce_max(dist, e2e_s, device)
+    e2e_val = world * s.n * max(3, args.steps // 2) / e2e_s
+
+    # per-kernel profile (separate pass; event-bracketed launches)
+    prof = profile_steps(g, s, min(args.steps, 5), args.warmup + args.steps + 100)
+    g.close()
+    dom = max((k for k in prof if algorithmic_bytes(k, 1, 1, 1, "mixed") is not None),
+              key=lambda k: prof[k][0])
+    K = int(np.prod(s.fft))
+    dom_ms = prof[dom][0] / max(prof[dom][1], 1)
+    dom_bytes = algorithmic_bytes(dom, s.n, nnb, K, "mixed")
+    peak, peak_kind = measured_peaks()
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    traffic = profile_traffic(dom)
+
+    # all-FP64 path, same input
+    fp64 = None
+    if not args.no_fp64:
+        g64 = equilibrated_context(s, "fp64", device=local)
+        ms64, _, _, _ = time_device(g64, s, args.steps, args.warmup, dist, device)
+        g64.close()
+        ms64 = reduce_max(dist, ms64, device)
+        fp64 = {"value": world * s.n * args.steps / (ms64 / 1e3), "unit": UNIT, "ms_per_step": ms64 / args.steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        el = cpu_baseline_sample(s)
+        cpu = {"value": s.n / el, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": "one full 128,000-atom step (VV_NVE1, CELL_SORT, FORCE, PME, VV_NVT2_BEREND) "
+                         "of the oracle port on 1 host thread"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n_atoms": s.n, "per_rank_replicas": 1,
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "precision": "mixed: FP32 pair/PME terms, FP64 sums, energies, CG",
+                       "charges": "CTIP at step 1 (warm-up), freq_new > run length",
+                       "l2": "inputs larger than L2 (neighbour list %.0f MB rebuilt every step)" % (tot_nnb * 4 / 1e6),
+                       "mean_neighbours": round(nnb, 1), "max_neighbours": mx_nnb},
+            "fp64": fp64,
+            "mixed_over_fp64": (value / fp64["value"]) if fp64 else None,
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
+            "gpu_launches": launches,
+            "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                         "avg_launch_ms": dom_ms, "algorithmic_bytes_per_launch": dom_bytes},
+            "kernels_ms_per_step": {k: round(v[0] / max(min(args.steps, 5), 1), 4) for k, v in
+                                    sorted(prof.items(), key=lambda kv: -kv[1][0])},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "energies_last_step": e,
+            "warmup_seconds": warm_s,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
