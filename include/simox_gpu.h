@@ -59,6 +59,8 @@ extern "C" {
 #define SIMOX_E_NO_DEVICE      -15  /* no CUDA device / library built without one */
 #define SIMOX_E_UNSUPPORTED    -16  /* hetero-metal pair forms (METAL_HETERO, AL_NI,
                                        eam.f90:38-168) are not on the GPU path */
+#define SIMOX_E_SCRATCH_LIMIT  -17  /* simox_cell_sort_noalloc: more than 65,536 cells
+                                       or a link stride above 4,096 */
 
 /* ---- precision modes --------------------------------------------------- */
 #define SIMOX_FP64   0   /* every term in FP64 (the FP64 GPU oracle path) */
@@ -227,6 +229,32 @@ int simox_launch_count(simox_ctx* ctx, long long* n);
 int simox_sync(simox_ctx* ctx);
 /* Neighbour statistics of the last list build: max and total list length. */
 int simox_neighbor_stats(simox_ctx* ctx, int* max_nnb, long long* total_nnb);
+
+/* ---- allocation-free cell binning ---------------------------------------
+ * No counterpart in the reference.  For callers that cannot let a library
+ * allocate device memory -- programs whose GPU memory belongs to another
+ * allocator (a framework's caching pool, or an arena reserved at start-up),
+ * or per-step loops where cudaMalloc/cudaFree would synchronise the device.
+ * Bins n atoms exactly as simox_cell_sort does (same cell membership and
+ * in-cell order) without a context and without allocating: the only scratch
+ * is a fixed device array of 65,536 cell counters inside the library, which
+ * each GPU that loads the library keeps until the process exits.
+ *   x_dev       device pointer, positions [n][3] FP64 (centred box coords)
+ *   box, rcut   host values; Ncell = INT(box/rcut) as in READ_INPUT
+ *   npt_dev     device pointer, Ncell1*Ncell2*Ncell3 ints: atoms per cell
+ *   link_dev    device pointer, Ncell*link_stride ints: 1-based atom ids,
+ *               ascending within each cell (cell(c)%link layout)
+ *   link_stride per-cell row length, 1..4,096 (500 in the reference)
+ *   stream      cudaStream_t as void* (NULL: the legacy default stream)
+ * Returns SIMOX_E_SCRATCH_LIMIT beyond 65,536 cells or a stride above 4,096,
+ * SIMOX_E_CELL_OVERFLOW when a cell holds more than link_stride atoms.
+ * The call synchronises the stream.  The first call on a device looks up the
+ * scratch array's device address with that device current; make that first
+ * call before any stream capture.  All calls share the one scratch array, so
+ * calls whose work overlaps on the GPU (other threads, other streams) race:
+ * serialise them. */
+int simox_cell_sort_noalloc(const double* x_dev, int n, const double* box, double rcut,
+                            int* npt_dev, int* link_dev, int link_stride, void* stream);
 
 #ifdef __cplusplus
 }

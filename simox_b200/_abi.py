@@ -31,6 +31,7 @@ SIMOX_E_FFT_SIZE = -13
 SIMOX_E_STATE = -14
 SIMOX_E_NO_DEVICE = -15
 SIMOX_E_UNSUPPORTED = -16
+SIMOX_E_SCRATCH_LIMIT = -17
 
 SIMOX_FP64 = 0
 SIMOX_MIXED = 1
@@ -57,6 +58,7 @@ _STATUS = {
     SIMOX_E_STATE: "call order violated",
     SIMOX_E_NO_DEVICE: "no CUDA device",
     SIMOX_E_UNSUPPORTED: "hetero-metal pair form not implemented on the GPU path",
+    SIMOX_E_SCRATCH_LIMIT: "size beyond the fixed scratch of simox_cell_sort_noalloc (65536 cells, stride 4096)",
 }
 
 
@@ -125,5 +127,5 @@ EXPORTED = [
     "simox_vv_nve1", "simox_vv_nve1_reflect", "simox_vv_nve2", "simox_vv_nvt2_berend",
     "simox_md_run", "simox_timer_begin", "simox_timer_end", "simox_profile_enable",
     "simox_profile_read", "simox_profile_reset", "simox_launch_count", "simox_sync",
-    "simox_neighbor_stats",
+    "simox_neighbor_stats", "simox_cell_sort_noalloc",
 ]

@@ -76,6 +76,7 @@ def lib():
         "simox_launch_count": [_vp, C.POINTER(C.c_longlong)],
         "simox_sync": [_vp],
         "simox_neighbor_stats": [_vp, _ip, C.POINTER(C.c_longlong)],
+        "simox_cell_sort_noalloc": [_vp, C.c_int, _dp, C.c_double, _vp, _vp, C.c_int, _vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

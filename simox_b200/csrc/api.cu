@@ -236,6 +236,7 @@ extern "C" const char* simox_status_string(int s) {
         case SIMOX_E_STATE: return "call order violated";
         case SIMOX_E_NO_DEVICE: return "no CUDA device";
         case SIMOX_E_UNSUPPORTED: return "hetero-metal pair form not implemented on the GPU path";
+        case SIMOX_E_SCRATCH_LIMIT: return "size beyond the fixed scratch of simox_cell_sort_noalloc (65536 cells, stride 4096)";
         default: return "unknown status";
     }
 }
