@@ -135,6 +135,8 @@ typedef struct {
     int    reflect;      /* 1 = VV_NVE1_REFLECT (oxidation mode top wall)         */
     int    charge_every_step; /* 1 = CTIP on every step (driver flag)             */
     int    accumulate_rdf;    /* 1 = accumulate the RDF histogram in FORCE        */
+    int    freq_stat;         /* energies (FP64) on steps with MOD(step, freq_stat)
+                                 == 0 (TAG_SET's status rule); <= 0: every step  */
 } simox_md_opts;
 
 typedef struct simox_ctx simox_ctx;
@@ -189,6 +191,9 @@ int simox_get_psi(simox_ctx* ctx, double* psi);
 int simox_ctip_solve(simox_ctx* ctx, int max_cg, simox_energies* e, simox_ctip_report* rep);
 /* FORCE (force.f90:3-361): EAM density, embedding, pair, Ewald real-space and
  * CTIP short-range forces; overwrites forces; sets Epair, Edir, Ectip, Egroup.
+ * e: NULL to skip the energies.  Energies are always evaluated with FP64 pair
+ * terms (in the mixed precision mode a call with e != NULL runs the FP64 pair
+ * kernels), forces of a call with e == NULL use the context's precision.
  * rdf: NULL, or a host histogram of SIMOX_RDF_LEN ints that is incremented. */
 int simox_force(simox_ctx* ctx, simox_energies* e, int* rdf);
 /* PME (force.f90:364-464): reciprocal-space forces added to the forces, the
@@ -207,7 +212,8 @@ int simox_vv_nvt2_berend(simox_ctx* ctx, double dt, double T_given, double* mv2)
 /* ---- device-resident main loop (main.f90:40-84) -------------------------
  * Runs steps first_step .. first_step+nsteps-1 of the reference loop on the
  * device: VV1, CELL_SORT, CTIP_SOLVER (TAG_SET rule), FORCE, PME, VV2/NVT.
- * last: energies of the final step (may be NULL). rdf: as simox_force. */
+ * last: energies of the last energy step of the run (may be NULL); mv2 is the
+ * final step's.  rdf: as simox_force, accumulated every step. */
 int simox_md_run(simox_ctx* ctx, const simox_md_opts* opts, int first_step,
                  int nsteps, simox_energies* last, int* rdf);
 

@@ -111,7 +111,7 @@ class CtipReport(C.Structure):
 class MdOpts(C.Structure):
     _fields_ = [("dt", C.c_double), ("thermostat", C.c_int), ("T_given", C.c_double),
                 ("freq_new", C.c_int), ("freq_sort", C.c_int), ("reflect", C.c_int),
-                ("charge_every_step", C.c_int), ("accumulate_rdf", C.c_int)]
+                ("charge_every_step", C.c_int), ("accumulate_rdf", C.c_int), ("freq_stat", C.c_int)]
 
 
 def potential_to_bytes(p: Potential) -> bytes:

@@ -230,20 +230,25 @@ class Simox:
             raise SimoxError(st, "CTIP_SOLVER")
         return e.Eself, dict(n_cg=r.n_cg, n_line=r.n_line, error=r.error, q_sum=r.q_sum)
 
-    def force(self, rdf: np.ndarray | None = None):
-        """FORCE: overwrites forces; returns dict(Epair, Edir, Ectip, Egroup).
-        ``rdf`` (int32, SIMOX_RDF_LEN) is incremented like pair%rdf."""
+    def force(self, rdf: np.ndarray | None = None, energies: bool = True):
+        """FORCE: overwrites forces; returns dict(Epair, Edir, Ectip, Egroup)
+        (None with ``energies=False``: forces only, in the context's precision;
+        energies are FP64 in both modes).  ``rdf`` (int32, SIMOX_RDF_LEN) is
+        incremented like pair%rdf."""
         e = Energies()
         if rdf is not None:
             assert rdf.dtype == np.int32 and rdf.size == _abi.RDF_LEN and rdf.flags.c_contiguous
-        _check(lib().simox_force(self._ctx, C.byref(e), _i(rdf)), "FORCE")
+        _check(lib().simox_force(self._ctx, C.byref(e) if energies else None, _i(rdf)), "FORCE")
+        if not energies:
+            return None
         return dict(Epair=e.Epair, Edir=e.Edir, Ectip=e.Ectip, Egroup=e.Egroup)
 
-    def pme(self) -> float:
-        """PME: adds reciprocal forces, removes the mean; returns Erec."""
+    def pme(self, energies: bool = True):
+        """PME: adds reciprocal forces, removes the mean; returns Erec (None
+        with ``energies=False``)."""
         e = Energies()
-        _check(lib().simox_pme(self._ctx, C.byref(e)), "PME")
-        return e.Erec
+        _check(lib().simox_pme(self._ctx, C.byref(e) if energies else None), "PME")
+        return e.Erec if energies else None
 
     def get_eam(self):
         rho = np.zeros(self.n)
@@ -269,8 +274,11 @@ class Simox:
     # -- main loop ----------------------------------------------------------
     def md_run(self, nsteps: int, dt: float, first_step: int = 1, thermostat: bool = False,
                T_given: float = 0.0, freq_new: int = 0, freq_sort: int = 1, reflect: bool = False,
-               charge_every_step: bool = False, rdf: np.ndarray | None = None):
-        """Steps first_step..first_step+nsteps-1 of main.f90:40-84 on the device."""
+               charge_every_step: bool = False, rdf: np.ndarray | None = None, freq_stat: int = 0):
+        """Steps first_step..first_step+nsteps-1 of main.f90:40-84 on the device.
+        Energies (FP64) are evaluated on steps with MOD(step, freq_stat) == 0,
+        TAG_SET's status rule (every step with freq_stat <= 0); the returned
+        energies are those of the last such step, mv2 that of the final step."""
         o = MdOpts()
         o.dt = float(dt)
         o.thermostat = 1 if thermostat else 0
@@ -280,6 +288,7 @@ class Simox:
         o.reflect = 1 if reflect else 0
         o.charge_every_step = 1 if charge_every_step else 0
         o.accumulate_rdf = 1 if rdf is not None else 0
+        o.freq_stat = int(freq_stat)
         e = Energies()
         _check(lib().simox_md_run(self._ctx, C.byref(o), int(first_step), int(nsteps), C.byref(e), _i(rdf)),
                "md_run")

@@ -101,7 +101,8 @@ int md_run(simox_ctx* c, const simox_md_opts* o, int first, int nsteps, simox_en
     for (int step = first; step < first + nsteps; step++) {
         const bool new_charge = o->freq_new > 0 && (o->charge_every_step || step % o->freq_new == 1);
         const bool sort = o->freq_sort > 0 && step % o->freq_sort == 0;
-        cudaMemsetAsync(c->acc, 0, sizeof(double) * (A_EREC + 1), c->stream);
+        const bool estep = o->freq_stat <= 0 || step % o->freq_stat == 0;   // TAG_SET status rule
+        if (estep) cudaMemsetAsync(c->acc, 0, sizeof(double) * (A_EREC + 1), c->stream);
         if ((st = vv1(c, o->dt, o->reflect != 0))) return st;
         if (sort && (st = cell_sort(c))) return st;
         if (new_charge) {
@@ -109,9 +110,9 @@ int md_run(simox_ctx* c, const simox_md_opts* o, int first, int nsteps, simox_en
             if ((st = ctip_solve(c, 0, &rep))) return st;
         }
         if ((st = ensure_list(c))) return st;
-        if ((st = eam_density(c, true))) return st;
-        if ((st = pair_forces(c, true, want_rdf))) return st;
-        if ((st = pme_forces(c, false))) return st;
+        if ((st = eam_density(c, estep))) return st;
+        if ((st = pair_forces(c, estep, want_rdf))) return st;
+        if ((st = pme_forces(c, false, estep))) return st;
         if (o->thermostat) st = nvt2_berend(c, o->dt, o->T_given, true);
         else st = vv2(c, o->dt, true);
         if (st) return st;
@@ -251,7 +252,7 @@ static void free_ctx(simox_ctx* c) {
     pme_free(c);
     void* bufs[] = {c->id, c->x, c->v, c->f, c->q, c->xm, c->cell_of, c->cell_count, c->cell_start, c->cell_fill,
                     c->sorted, c->pair13, c->entries, c->xq_s, c->t_s, c->nn, c->nbr, c->nn_max, c->nn_tot,
-                    c->rho_s, c->dF_s, c->tab_d, c->tab_f, c->c_const, c->g, c->pv, c->Ap, c->qs, c->jp,
+                    c->rho_s, c->dF_s, c->dF_f, c->tab_d, c->tab_f, c->c_const, c->g, c->pv, c->Ap, c->qs, c->jp,
                     c->act, c->line, c->acc, c->status, c->rdf};
     for (void* p : bufs)
         if (p) cudaFree(p);
@@ -317,7 +318,11 @@ extern "C" int simox_create(const simox_setup* s, const simox_potential* pot, si
         delete c;
         return SIMOX_E_CELL_TOO_SMALL;
     }
-    c->fast_cells = c->nc[0] >= 3 && c->nc[1] >= 3 && c->nc[2] >= 3;
+    // the FP32 staged-offset list build needs, per axis, Ncell >= 3 and
+    // L/2 > Rcut + Lcell/2 (so a home atom's offset difference is the minimum image)
+    c->fast_cells = true;
+    for (int d = 0; d < 3; d++)
+        if (c->nc[d] < 3 || !(0.5 * c->box[d] - c->rcut - 0.5 * c->lc[d] > 0.01)) c->fast_cells = false;
     c->ncell = c->nc[0] * c->nc[1] * c->nc[2];
 
     int st = SIMOX_OK;
@@ -327,9 +332,9 @@ extern "C" int simox_create(const simox_setup* s, const simox_potential* pot, si
               dalloc(&c->q, N) && dalloc(&c->cell_of, N) && dalloc(&c->cell_count, c->ncell) &&
               dalloc(&c->cell_start, c->ncell + 1) && dalloc(&c->cell_fill, c->ncell) && dalloc(&c->sorted, N) &&
               dalloc(&c->pair13, (size_t)c->ncell * 13) && dalloc(&c->entries, (size_t)c->ncell * kEntries) &&
-              dalloc(&c->xq_s, N) && dalloc(&c->t_s, N) && dalloc(&c->nn, N) &&
+              dalloc(&c->xq_s, N) && dalloc(&c->t_s, N) && dalloc(&c->nn, 2 * N) &&
               dalloc(&c->nbr, N * (size_t)c->nnb_cap) && dalloc(&c->nn_max, 1) && dalloc(&c->nn_tot, 1) &&
-              dalloc(&c->rho_s, N) && dalloc(&c->dF_s, N) && dalloc(&c->tab_d, kSpecies * kSpecies) &&
+              dalloc(&c->rho_s, N) && dalloc(&c->dF_s, N) && dalloc(&c->dF_f, N) && dalloc(&c->tab_d, kSpecies * kSpecies) &&
               dalloc(&c->tab_f, kSpecies * kSpecies) && dalloc(&c->line, 64) && dalloc(&c->acc, A_COUNT) &&
               dalloc(&c->status, 1) && dalloc(&c->rdf, SIMOX_RDF_LEN);
     if (!ok) { free_ctx(c); return SIMOX_E_NOMEM; }
@@ -478,10 +483,11 @@ extern "C" int simox_force(simox_ctx* c, simox_energies* e, int* rdf) {
     if (!c) return SIMOX_E_ARG;
     cudaSetDevice(c->device);
     if (!c->cells_valid) return SIMOX_E_STATE;
+    const bool eflag = e != nullptr;
     cudaMemsetAsync(c->acc, 0, sizeof(double) * (A_EGROUP + 1), c->stream);
     if (rdf) cudaMemsetAsync(c->rdf, 0, sizeof(int) * SIMOX_RDF_LEN, c->stream);
     int st;
-    if ((st = ensure_list(c)) || (st = eam_density(c, true)) || (st = pair_forces(c, true, rdf != nullptr))) return st;
+    if ((st = ensure_list(c)) || (st = eam_density(c, eflag)) || (st = pair_forces(c, eflag, rdf != nullptr))) return st;
     if ((st = read_status(c))) return st;
     cudaMemcpyAsync(c->h_acc, c->acc, sizeof(double) * A_COUNT, cudaMemcpyDeviceToHost, c->stream);
     std::vector<int> h;
@@ -506,7 +512,7 @@ extern "C" int simox_pme(simox_ctx* c, simox_energies* e) {
     cudaSetDevice(c->device);
     if (!c->cells_valid) return SIMOX_E_STATE;
     cudaMemsetAsync(c->acc + A_EREC, 0, sizeof(double), c->stream);
-    int st = pme_forces(c, true);
+    int st = pme_forces(c, true, e != nullptr);
     if (st) return st;
     cudaMemcpyAsync(c->h_acc, c->acc, sizeof(double) * A_COUNT, cudaMemcpyDeviceToHost, c->stream);
     if ((st = cuda_status(cudaStreamSynchronize(c->stream)))) return st;

@@ -14,7 +14,8 @@
 // home atom and tests every staged candidate with an FP32 distance.  Pairs
 // within a relative band of 4e-5 around Rcut^2 are re-tested with the
 // reference's exact FP64 expression (dx - L*DNINT(dx/L), r2 summed without
-// FMA), so list membership equals the reference's r2 < Rcut2 test.
+// FMA), so list membership equals the reference's r2 < Rcut2 test.  Rows are
+// grouped by partner species (metals from the front, oxygen from the back).
 #include "simox_internal.cuh"
 
 #include <algorithm>
@@ -23,7 +24,7 @@
 namespace sx {
 
 constexpr int LB_THREADS = 128;
-constexpr int LB_TILE = 2048;
+constexpr int LB_TILE = 1024;
 
 // ---------------------------------------------------------------------------
 // CELL_HIERARCHY cellsort.f90:3-36 (host): 13-cell half stencil, 1-based ids
@@ -208,11 +209,17 @@ int gather_sorted(simox_ctx* c) {
 
 // ---------------------------------------------------------------------------
 // neighbour list
+//
+// Rows are grouped by partner species: metal partners fill a row from the
+// front, oxygen partners from the back (row[cap-1], row[cap-2], ...), and
+// nn[i] = (n_metal, n_oxygen).  A warp looping over one group therefore sees
+// one partner species, so the pair kernels run species-specialised code
+// without divergence.
 struct LBParams {
-    double3 box, origin, lc;
+    double3 box, ibox, origin, lc;
     int3 nc;
     double rcut2;
-    float bx, by, bz, ibx, iby, ibz, r2lo, r2hi;
+    float r2lo, r2hi, hlx, hly, hlz;
     int cap, npt_max;
 };
 
@@ -225,15 +232,33 @@ __device__ __forceinline__ double exact_r2(double4 a, double4 b, double3 box) {
     return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
 }
 
+__device__ __forceinline__ void list_append(unsigned* row, int2& my, int cap, unsigned j, unsigned isa, int sp) {
+    const int used = my.x + my.y;
+    if (sp == 3) {
+        if (used < cap) row[cap - 1 - my.y] = j | (isa << 31);
+        my.y++;
+    } else {
+        if (used < cap) row[my.x] = j | (isa << 31);
+        my.x++;
+    }
+}
+
+// FAST (every Ncell >= 3 and L/2 > Rcut + Lcell/2): candidates are staged as
+// FP32 offsets from the home-cell centre, already minimum-imaged with respect
+// to that centre; for a home atom inside its cell that offset difference is
+// the pair's minimum image, so the inner loop is three subtractions and a
+// squared norm.  Pairs within 4e-5 of Rcut^2, home atoms outside their cell
+// and the generic (multi-image) path use the reference's exact FP64 r2.
 template <bool FAST>
 __global__ void __launch_bounds__(LB_THREADS)
     build_list_kernel(const int* __restrict__ cell_start, const int* __restrict__ entries,
-                      const double4* __restrict__ xq, unsigned* __restrict__ nbr, int* __restrict__ nn, LBParams P,
-                      int* __restrict__ status, int* __restrict__ nn_max, unsigned long long* __restrict__ nn_tot) {
+                      const double4* __restrict__ xq, const int* __restrict__ ts, unsigned* __restrict__ nbr,
+                      int2* __restrict__ nn, LBParams P, int* __restrict__ status, int* __restrict__ nn_max,
+                      unsigned long long* __restrict__ nn_tot) {
     extern __shared__ __align__(16) unsigned char smem[];
     float4* cpos = reinterpret_cast<float4*>(smem);
     unsigned* ctag = reinterpret_cast<unsigned*>(cpos + LB_TILE);
-    int* cnt = reinterpret_cast<int*>(ctag + LB_TILE);
+    int2* cnt = reinterpret_cast<int2*>(ctag + LB_TILE);
     __shared__ int es0[kEntries], edir[kEntries], epre[kEntries + 1];
 
     const int cc = blockIdx.x;
@@ -251,7 +276,7 @@ __global__ void __launch_bounds__(LB_THREADS)
         epre[tid + 1] = cell_start[ce + 1] - cell_start[ce];
         edir[tid] = ent >> 28;
     }
-    for (int k = tid; k < nh; k += blockDim.x) cnt[k] = 0;
+    for (int k = tid; k < nh; k += blockDim.x) cnt[k] = make_int2(0, 0);
     __syncthreads();
     if (tid == 0) {
         epre[0] = 0;
@@ -270,9 +295,13 @@ __global__ void __launch_bounds__(LB_THREADS)
         for (int k = tid; k < tn; k += blockDim.x) {
             int g = t0 + k, e = 0;
             while (epre[e + 1] <= g) e++;
-            int j = es0[e] + (g - epre[e]);
-            double4 p = xq[j];
-            cpos[k] = make_float4((float)(p.x - cen_x), (float)(p.y - cen_y), (float)(p.z - cen_z), 0.f);
+            const int j = es0[e] + (g - epre[e]);
+            const double4 p = xq[j];
+            double rx = p.x - cen_x, ry = p.y - cen_y, rz = p.z - cen_z;
+            rx -= P.box.x * rint(rx * P.ibox.x);
+            ry -= P.box.y * rint(ry * P.ibox.y);
+            rz -= P.box.z * rint(rz * P.ibox.z);
+            cpos[k] = make_float4((float)rx, (float)ry, (float)rz, __int_as_float(ts[j]));
             ctag[k] = (unsigned)j | ((unsigned)edir[e] << 30);
         }
         __syncthreads();
@@ -280,31 +309,37 @@ __global__ void __launch_bounds__(LB_THREADS)
             const int h = h0 + hl;
             const double4 xh = xq[h];
             const float hx = (float)(xh.x - cen_x), hy = (float)(xh.y - cen_y), hz = (float)(xh.z - cen_z);
-            int my = cnt[hl];
+            int2 my = cnt[hl];
             unsigned* row = nbr + (size_t)h * P.cap;
-            for (int k = 0; k < tn; k++) {
-                const unsigned tag = ctag[k];
-                const int j = (int)(tag & 0x3fffffffu);
-                if (j == h) continue;
-                bool acc;
-                if (FAST) {
+            const bool inside = FAST && fabsf(hx) <= P.hlx && fabsf(hy) <= P.hly && fabsf(hz) <= P.hlz;
+            if (inside) {
+#pragma unroll 4
+                for (int k = 0; k < tn; k++) {
                     const float4 cp = cpos[k];
-                    float dx = hx - cp.x, dy = hy - cp.y, dz = hz - cp.z;
-                    dx -= P.bx * rintf(dx * P.ibx);
-                    dy -= P.by * rintf(dy * P.iby);
-                    dz -= P.bz * rintf(dz * P.ibz);
+                    const float dx = hx - cp.x, dy = hy - cp.y, dz = hz - cp.z;
                     const float r2 = dx * dx + dy * dy + dz * dz;
-                    if (r2 < P.r2lo) acc = true;
-                    else if (r2 > P.r2hi) acc = false;
-                    else acc = exact_r2(xh, xq[j], P.box) < P.rcut2;
-                } else {
-                    acc = exact_r2(xh, xq[j], P.box) < P.rcut2;
+                    if (r2 < P.r2hi) {
+                        const unsigned tag = ctag[k];
+                        const int j = (int)(tag & 0x3fffffffu);
+                        bool acc = r2 < P.r2lo;
+                        if (!acc) acc = exact_r2(xh, xq[j], P.box) < P.rcut2;
+                        if (acc && j != h) {
+                            const unsigned dir = tag >> 30;
+                            const unsigned isa = dir == 0 ? (unsigned)(h < j) : (unsigned)(dir == 1);
+                            list_append(row, my, P.cap, (unsigned)j, isa, __float_as_int(cp.w));
+                        }
+                    }
                 }
-                if (acc) {
-                    const unsigned dir = tag >> 30;
-                    const unsigned isa = dir == 0 ? (unsigned)(h < j) : (unsigned)(dir == 1);
-                    if (my < P.cap) row[my] = (unsigned)j | (isa << 31);
-                    my++;
+            } else {
+                for (int k = 0; k < tn; k++) {
+                    const unsigned tag = ctag[k];
+                    const int j = (int)(tag & 0x3fffffffu);
+                    if (j == h) continue;
+                    if (exact_r2(xh, xq[j], P.box) < P.rcut2) {
+                        const unsigned dir = tag >> 30;
+                        const unsigned isa = dir == 0 ? (unsigned)(h < j) : (unsigned)(dir == 1);
+                        list_append(row, my, P.cap, (unsigned)j, isa, __float_as_int(cpos[k].w));
+                    }
                 }
             }
             cnt[hl] = my;
@@ -314,11 +349,16 @@ __global__ void __launch_bounds__(LB_THREADS)
     int lmax = 0;
     unsigned long long ltot = 0;
     for (int hl = tid; hl < nh; hl += blockDim.x) {
-        int m = cnt[hl];
-        nn[h0 + hl] = min(m, P.cap);
-        if (m > P.cap) atomicOr(status, ST_NBR_OVERFLOW);
-        lmax = max(lmax, m);
-        ltot += (unsigned long long)m;
+        const int2 m = cnt[hl];
+        const int tot = m.x + m.y;
+        if (tot > P.cap) {
+            atomicOr(status, ST_NBR_OVERFLOW);
+            nn[h0 + hl] = make_int2(0, 0);
+        } else {
+            nn[h0 + hl] = m;
+        }
+        lmax = max(lmax, tot);
+        ltot += (unsigned long long)tot;
     }
     atomicMax(nn_max, lmax);
     atomicAdd(nn_tot, ltot);
@@ -333,25 +373,29 @@ int build_list(simox_ctx* c) {
     cudaMemsetAsync(c->nn_tot, 0, sizeof(unsigned long long), c->stream);
     LBParams P;
     P.box = make_double3(c->box[0], c->box[1], c->box[2]);
+    P.ibox = make_double3(c->inv_box[0], c->inv_box[1], c->inv_box[2]);
     P.origin = make_double3(-c->hbox[0], -c->hbox[1], -c->hbox[2]);
     P.lc = make_double3(c->lc[0], c->lc[1], c->lc[2]);
     P.nc = make_int3(c->nc[0], c->nc[1], c->nc[2]);
     P.rcut2 = c->rcut2;
-    P.bx = (float)c->box[0]; P.by = (float)c->box[1]; P.bz = (float)c->box[2];
-    P.ibx = (float)(1.0 / c->box[0]); P.iby = (float)(1.0 / c->box[1]); P.ibz = (float)(1.0 / c->box[2]);
     P.r2lo = (float)(c->rcut2 * (1.0 - 4.0e-5));
     P.r2hi = (float)(c->rcut2 * (1.0 + 4.0e-5));
+    P.hlx = (float)(0.5 * c->lc[0] + 1.0e-3);
+    P.hly = (float)(0.5 * c->lc[1] + 1.0e-3);
+    P.hlz = (float)(0.5 * c->lc[2] + 1.0e-3);
     P.cap = c->nnb_cap;
     P.npt_max = c->npt_max;
-    size_t smem = LB_TILE * (sizeof(float4) + sizeof(unsigned)) + sizeof(int) * c->npt_max;
+    size_t smem = LB_TILE * (sizeof(float4) + sizeof(unsigned)) + sizeof(int2) * c->npt_max;
     {
         Launch L(c, "neighbor_list");
         if (c->fast_cells)
             build_list_kernel<true><<<c->ncell, LB_THREADS, smem, c->stream>>>(
-                c->cell_start, c->entries, c->xq_s, c->nbr, c->nn, P, c->status, c->nn_max, c->nn_tot);
+                c->cell_start, c->entries, c->xq_s, c->t_s, c->nbr, reinterpret_cast<int2*>(c->nn), P, c->status,
+                c->nn_max, c->nn_tot);
         else
             build_list_kernel<false><<<c->ncell, LB_THREADS, smem, c->stream>>>(
-                c->cell_start, c->entries, c->xq_s, c->nbr, c->nn, P, c->status, c->nn_max, c->nn_tot);
+                c->cell_start, c->entries, c->xq_s, c->t_s, c->nbr, reinterpret_cast<int2*>(c->nn), P, c->status,
+                c->nn_max, c->nn_tot);
     }
     int st = check_launch(c);
     if (st) return st;
@@ -371,7 +415,7 @@ int ensure_list(simox_ctx* c) {
 }
 
 int list_prepare(simox_ctx* c) {
-    const int bytes = (int)(LB_TILE * (sizeof(float4) + sizeof(unsigned)) + sizeof(int) * c->npt_max);
+    const int bytes = (int)(LB_TILE * (sizeof(float4) + sizeof(unsigned)) + sizeof(int2) * c->npt_max);
     cudaError_t e1 = cudaFuncSetAttribute(build_list_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     cudaError_t e2 = cudaFuncSetAttribute(build_list_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e1 != cudaSuccess || e2 != cudaSuccess) return SIMOX_E_ARG;

@@ -44,10 +44,17 @@ struct CtipParams {
 
 template <typename R> __device__ __forceinline__ R cexp(R x);
 template <> __device__ __forceinline__ double cexp<double>(double x) { return exp(x); }
-template <> __device__ __forceinline__ float cexp<float>(float x) { return expf(x); }
+template <> __device__ __forceinline__ float cexp<float>(float x) { return __expf(x); }
 template <typename R> __device__ __forceinline__ R cerfc(R x);
 template <> __device__ __forceinline__ double cerfc<double>(double x) { return erfc(x); }
-template <> __device__ __forceinline__ float cerfc<float>(float x) { return erfcf(x); }
+// Numerical Recipes "erfcc" (Chebyshev fit, fractional error < 1.2e-7, x >= 0)
+template <> __device__ __forceinline__ float cerfc<float>(float z) {
+    const float t = __fdividef(1.0f, 1.0f + 0.5f * z);
+    const float p = -1.26551223f + t * (1.00002368f + t * (0.37409196f + t * (0.09678418f +
+                    t * (-0.18628806f + t * (0.27886807f + t * (-1.13520398f + t * (1.48851587f +
+                    t * (-0.82215223f + t * 0.17087277f))))))));
+    return t * __expf(p - z * z);
+}
 
 __device__ __forceinline__ double pen_d(double q, double lo, double hi) {
     // 2w*(dqmin + dqmax) with dqmin = min(0, q-qmin), dqmax = max(0, q-qmax)  ctip.f90:317-322
@@ -57,53 +64,77 @@ __device__ __forceinline__ double pen_d(double q, double lo, double hi) {
     return 2.0 * SX_WPEN * (a + b);
 }
 
+// One group of X's row: sr += sum_Y sym_XY v_Y; cz += sum_Y Z_Y asym_XY.
+// SAME: the partner has X's species (one Slater exponential).
+template <typename R, bool WITH_C, bool SAME>
+__device__ __forceinline__ void ctip_group(const CtipParams& P, const PairTab<R>* st, const unsigned* row, int g,
+                                           int mg, int lane, const double4& xa, int sX, int sY_fixed,
+                                           const double4* __restrict__ xq, const int* __restrict__ ts,
+                                           const double* __restrict__ vin, double& sr, double& cz) {
+    const R a = (R)P.a, kc = (R)P.kc;
+    const int nm = g == 2 ? sY_fixed : 0;   // group 2: the whole row, sY_fixed = number of metal partners
+    if (g == 2) sY_fixed = -1;
+    for (int k = lane; k < mg; k += 32) {
+        const int slot = g == 0 ? k : (g == 1 ? P.cap - 1 - k : (k < nm ? k : P.cap - 1 - (k - nm)));
+        const int Y = (int)(row[slot] & kIdxMask);
+        const double4 xb = xq[Y];
+        const int sY = sY_fixed >= 0 ? sY_fixed : ts[Y];
+        if (sY >= kSpecies || (SAME && sY != sX)) continue;   // flagged by the force pass
+        double dx = __dsub_rn(xa.x, xb.x), dy = __dsub_rn(xa.y, xb.y), dz = __dsub_rn(xa.z, xb.z);
+        dx = __dsub_rn(dx, __dmul_rn(P.box.x, rint(dx * P.ibox.x)));
+        dy = __dsub_rn(dy, __dmul_rn(P.box.y, rint(dy * P.ibox.y)));
+        dz = __dsub_rn(dz, __dmul_rn(P.box.z, rint(dz * P.ibox.z)));
+        const double r2d = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+        R r, ir;
+        if (sizeof(R) == 8) { r = (R)sqrt(r2d); ir = R(1) / r; }
+        else { ir = (R)rsqrtf((float)r2d); r = (R)r2d * ir; }
+        const PairTab<R>& T = st[sX * kSpecies + sY];
+        const R eX = cexp<R>(R(-2) * T.xi_x * r);
+        // fifj (ctip.f90:91-100) = -(eX SX(r) + eY SY(r))/r
+        R num = eX * (T.Sx[0] + r * (T.Sx[1] + r * (T.Sx[2] + r * T.Sx[3])));
+        if (!SAME) num += cexp<R>(R(-2) * T.xi_y * r) * (T.Sy[0] + r * T.Sy[1]);
+        const R fifj = -num * ir;
+        const R sym = kc * (fifj + cerfc<R>(a * r) * ir);            // ctip.f90:108
+        sr += (double)sym * vin[Y];
+        if (WITH_C) {
+            const R afbX = -eX * (T.xi_x + ir);                         // ctip.f90:86,96
+            cz += (double)(T.Z_y * kc * (afbX - fifj));                 // ctip.f90:106 x XJZ(j,3)
+        }
+    }
+}
+
 // Pair pass over the list: out[X] = sum_Y sym_XY v_Y ; optional cconst[X] = chi_X + sum_Y Z_Y asym_XY
 template <typename R, bool WITH_C>
 __global__ void __launch_bounds__(CT_THREADS)
     ctip_pair_kernel(CtipParams P, const PairTab<R>* __restrict__ tab, const double4* __restrict__ xq,
-                     const int* __restrict__ ts, const int* __restrict__ nn, const unsigned* __restrict__ nbr,
+                     const int* __restrict__ ts, const int2* __restrict__ nn, const unsigned* __restrict__ nbr,
                      const double* __restrict__ vin, double* __restrict__ out, double* __restrict__ cconst,
                      CtipSpecies S) {
     __shared__ PairTab<R> st[kSpecies * kSpecies];
     for (int k = threadIdx.x; k < kSpecies * kSpecies; k += blockDim.x) st[k] = tab[k];
     __syncthreads();
     const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
-    const R a = (R)P.a, kc = (R)P.kc;
     for (int X = blockIdx.x * wpb + (threadIdx.x >> 5); X < P.n; X += gridDim.x * wpb) {
         const double4 xa = xq[X];
-        const int sX = min(ts[X], kSpecies - 1);
-        const int m = nn[X];
+        const int sX = ts[X];
+        const int2 m = nn[X];
         const unsigned* row = nbr + (size_t)X * P.cap;
         double sr = 0.0, cz = 0.0;
-        for (int k = lane; k < m; k += 32) {
-            const int Y = (int)(row[k] & kIdxMask);
-            const double4 xb = xq[Y];
-            const int sY = min(ts[Y], kSpecies - 1);
-            double dx = __dsub_rn(xa.x, xb.x), dy = __dsub_rn(xa.y, xb.y), dz = __dsub_rn(xa.z, xb.z);
-            dx = __dsub_rn(dx, __dmul_rn(P.box.x, rint(dx * P.ibox.x)));
-            dy = __dsub_rn(dy, __dmul_rn(P.box.y, rint(dy * P.ibox.y)));
-            dz = __dsub_rn(dz, __dmul_rn(P.box.z, rint(dz * P.ibox.z)));
-            const R r = sqrt((R)__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
-            const R ir = R(1) / r;
-            const PairTab<R>& T = st[sX * kSpecies + sY];
-            const R eX = cexp<R>(R(-2) * T.xi_x * r);
-            const R eY = cexp<R>(R(-2) * T.xi_y * r);
-            // fifj (ctip.f90:91-100) = -(eX SX(r) + eY SY(r))/r
-            const R SXv = T.Sx[0] + r * (T.Sx[1] + r * (T.Sx[2] + r * T.Sx[3]));
-            const R SYv = T.Sy[0] + r * (T.Sy[1] + r * (T.Sy[2] + r * T.Sy[3]));
-            const R fifj = -(eX * SXv + eY * SYv) * ir;
-            const R sym = kc * (fifj + cerfc<R>(a * r) * ir);            // ctip.f90:108
-            sr += (double)sym * vin[Y];
-            if (WITH_C) {
-                const R afbX = -eX * (T.xi_x + ir);                         // ctip.f90:86,96
-                cz += (double)(T.Z_y * kc * (afbX - fifj));                 // ctip.f90:106 x XJZ(j,3)
-            }
+        if (sX >= kSpecies) {
+        } else if (sizeof(R) == 8) {   // FP64: one table-driven body (I-cache)
+            ctip_group<R, WITH_C, false>(P, st, row, 2, m.x + m.y, lane, xa, sX, m.x, xq, ts, vin, sr, cz);
+        } else if (sX < 3) {
+            ctip_group<R, WITH_C, true>(P, st, row, 0, m.x, lane, xa, sX, -1, xq, ts, vin, sr, cz);
+            ctip_group<R, WITH_C, false>(P, st, row, 1, m.y, lane, xa, sX, 3, xq, ts, vin, sr, cz);
+        } else {
+            ctip_group<R, WITH_C, false>(P, st, row, 0, m.x, lane, xa, sX, -1, xq, ts, vin, sr, cz);
+            ctip_group<R, WITH_C, true>(P, st, row, 1, m.y, lane, xa, sX, 3, xq, ts, vin, sr, cz);
         }
         sr = warp_sum(sr);
         if (WITH_C) cz = warp_sum(cz);
         if (lane == 0) {
             out[X] = sr;
-            if (WITH_C) cconst[X] = S.chi[min(ts[X], 4)] + cz;
+            if (WITH_C) cconst[X] = S.chi[min(sX, 4)] + cz;
         }
     }
 }
@@ -361,10 +392,10 @@ static void launch_ctip_pair(simox_ctx* c, const PairTab<R>* tab, const double* 
     int g = std::min((c->n + wpb - 1) / wpb, num_sms(c) * 8);
     if (g < 1) g = 1;
     if (cconst)
-        ctip_pair_kernel<R, true><<<g, CT_THREADS, 0, c->stream>>>(P, tab, c->xq_s, c->t_s, c->nn, c->nbr, vin, out,
+        ctip_pair_kernel<R, true><<<g, CT_THREADS, 0, c->stream>>>(P, tab, c->xq_s, c->t_s, reinterpret_cast<const int2*>(c->nn), c->nbr, vin, out,
                                                                    cconst, S);
     else
-        ctip_pair_kernel<R, false><<<g, CT_THREADS, 0, c->stream>>>(P, tab, c->xq_s, c->t_s, c->nn, c->nbr, vin, out,
+        ctip_pair_kernel<R, false><<<g, CT_THREADS, 0, c->stream>>>(P, tab, c->xq_s, c->t_s, reinterpret_cast<const int2*>(c->nn), c->nbr, vin, out,
                                                                     nullptr, S);
 }
 

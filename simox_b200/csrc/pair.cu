@@ -9,10 +9,14 @@
 //
 // One warp owns one atom (lanes stride over its neighbour row, then a warp
 // reduction), so every force is written once and no float atomics are used.
+// Rows are grouped by partner species, and each group runs code specialised
+// for its species pair: Al-Al needs two Zhou terms and one CTIP exponential,
+// O-O three and one, Al-O four and two (the uniform form needs four and two).
 // Precision: R = double (FP64 path) or float (mixed path: per-pair terms in
 // FP32 from an FP64 separation; per-atom sums, energies in FP64).
 #include "simox_internal.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -93,16 +97,33 @@ int build_pair_tables(simox_ctx* c) {
 }
 
 // ---------------------------------------------------------------------------
-// device math in R
+// device math in R.  FP64: CUDA's exp / erfc / IEEE division.  FP32 (mixed
+// path): the SFU exponential (ex2.approx on x*log2(e)), an approximate
+// reciprocal, and erfc from the Chebyshev fit of Numerical Recipes (Press et
+// al., "erfcc", fractional error < 1.2e-7 for all x >= 0), which shares the
+// SFU exponential; tests/test_gpu_parity.py bounds the resulting force error.
 template <typename R> __device__ __forceinline__ R dexp(R x);
 template <> __device__ __forceinline__ double dexp<double>(double x) { return exp(x); }
-template <> __device__ __forceinline__ float dexp<float>(float x) { return expf(x); }
-template <typename R> __device__ __forceinline__ R derfc(R x);
-template <> __device__ __forceinline__ double derfc<double>(double x) { return erfc(x); }
-template <> __device__ __forceinline__ float derfc<float>(float x) { return erfcf(x); }
+template <> __device__ __forceinline__ float dexp<float>(float x) { return __expf(x); }
 template <typename R> __device__ __forceinline__ R drcp(R x);
 template <> __device__ __forceinline__ double drcp<double>(double x) { return 1.0 / x; }
 template <> __device__ __forceinline__ float drcp<float>(float x) { return __fdividef(1.0f, x); }
+
+// erfc(z) and exp(-z^2) for z >= 0
+template <typename R> __device__ __forceinline__ void erfc_exp(R z, R& erfcv, R& ez2);
+template <> __device__ __forceinline__ void erfc_exp<double>(double z, double& erfcv, double& ez2) {
+    erfcv = erfc(z);
+    ez2 = exp(-z * z);
+}
+template <> __device__ __forceinline__ void erfc_exp<float>(float z, float& erfcv, float& ez2) {
+    const float t = __fdividef(1.0f, 1.0f + 0.5f * z);
+    const float p = -1.26551223f + t * (1.00002368f + t * (0.37409196f + t * (0.09678418f +
+                    t * (-0.18628806f + t * (0.27886807f + t * (-1.13520398f + t * (1.48851587f +
+                    t * (-0.82215223f + t * 0.17087277f))))))));
+    const float z2 = z * z;
+    erfcv = t * __expf(p - z2);
+    ez2 = __expf(-z2);
+}
 
 // Zhou term g = exp(-c(r/re - 1)) / (1 + (r/re - lam)^20) and dg/dr (eam.f90:16-23)
 template <typename R>
@@ -178,14 +199,20 @@ __device__ __forceinline__ void min_image(double4 a, double4 b, const PairParams
     dz = __dsub_rn(dz, __dmul_rn(P.box.z, rint(dz * P.ibox.z)));
 }
 
+// list slot k of group g in a row (metals from the front, oxygen from the
+// back); group 2 walks the whole row, nm = number of metal partners
+__device__ __forceinline__ int row_slot(int g, int k, int cap, int nm = 0) {
+    return g == 0 ? k : (g == 1 ? cap - 1 - k : (k < nm ? k : cap - 1 - (k - nm)));
+}
+
 constexpr int PK_THREADS = 256;
 
 // pass 1 -------------------------------------------------------------------
 template <typename R>
 __global__ void __launch_bounds__(PK_THREADS)
     density_kernel(PairParams P, const PairTab<R>* __restrict__ tab, const double4* __restrict__ xq,
-                   const int* __restrict__ ts, const int* __restrict__ nn, const unsigned* __restrict__ nbr,
-                   EmbedParams E, double* __restrict__ rho_s, double* __restrict__ dF_s,
+                   const int* __restrict__ ts, const int2* __restrict__ nn, const unsigned* __restrict__ nbr,
+                   EmbedParams E, double* __restrict__ rho_s, double* __restrict__ dF_s, float* __restrict__ dF_f,
                    double* __restrict__ acc, int* __restrict__ status, int eflag) {
     __shared__ PairTab<R> st[kSpecies * kSpecies];
     __shared__ double red[PK_THREADS / 32];
@@ -198,21 +225,36 @@ __global__ void __launch_bounds__(PK_THREADS)
     for (int X = blockIdx.x * wpb + (threadIdx.x >> 5); X < P.n; X += gridDim.x * wpb) {
         const double4 xa = xq[X];
         const int sX = ts[X];
-        const int m = nn[X];
+        const int2 m = nn[X];
         const unsigned* row = nbr + (size_t)X * P.cap;
         double rho = 0.0;
-        for (int k = lane; k < m; k += 32) {
-            const int Y = (int)(row[k] & kIdxMask);
-            const double4 xb = xq[Y];
-            const int sY = ts[Y];
-            if (sX >= kSpecies || sY >= kSpecies) { bad |= ST_UNKNOWN_PAIR; continue; }
-            double dx, dy, dz;
-            min_image(xa, xb, P, dx, dy, dz);
-            const R r2 = (R)__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-            const R r = sqrt(r2);
-            const PairTab<R>& T = st[sX * kSpecies + sY];
-            if (!T.valid) bad |= ST_UNSUPPORTED;
-            rho += (double)(T.d_fe * zhou_val<R>(r, T.d_inv_re, T.d_c, T.d_lam));
+        if (sX < kSpecies) {
+#pragma unroll 1
+            for (int g = 0; g < 2; g++) {
+                const int mg = g == 0 ? m.x : m.y;
+                // partner species of the group: oxygen (3) for g = 1; metals for g = 0
+                unsigned ent_n = lane < mg ? row[row_slot(g, lane, P.cap)] : 0u;
+                double4 xb_n = lane < mg ? xq[ent_n & kIdxMask] : make_double4(0, 0, 0, 0);
+                for (int k = lane; k < mg; k += 32) {
+                    const int Y = (int)(ent_n & kIdxMask);
+                    const double4 xb = xb_n;
+                    if (k + 32 < mg) {
+                        ent_n = row[row_slot(g, k + 32, P.cap)];
+                        xb_n = xq[ent_n & kIdxMask];
+                    }
+                    const int sY = g == 1 ? 3 : ts[Y];
+                    if (sY >= kSpecies) { bad |= ST_UNKNOWN_PAIR; continue; }
+                    double dx, dy, dz;
+                    min_image(xa, xb, P, dx, dy, dz);
+                    const R r2 = (R)__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+                    const R r = sqrt(r2);
+                    const PairTab<R>& T = st[sX * kSpecies + sY];
+                    if (!T.valid) bad |= ST_UNSUPPORTED;
+                    rho += (double)(T.d_fe * zhou_val<R>(r, T.d_inv_re, T.d_c, T.d_lam));
+                }
+            }
+        } else if (m.x + m.y > 0) {
+            bad |= ST_UNKNOWN_PAIR;
         }
         rho = warp_sum(rho);
         if (lane == 0) {
@@ -220,6 +262,7 @@ __global__ void __launch_bounds__(PK_THREADS)
             if (embed(E, sX, rho, F, dF)) bad |= ST_UNKNOWN_ELEMENT;
             rho_s[X] = rho;
             dF_s[X] = dF;
+            dF_f[X] = (float)dF;
             egroup += F;
         }
     }
@@ -227,15 +270,143 @@ __global__ void __launch_bounds__(PK_THREADS)
     if (eflag) block_add<PK_THREADS>(egroup, acc, A_EGROUP, red);
 }
 
+// One pair's scalar force f/r on X (force.f90:81-98, 135-138), specialised on
+//   SAME : the partner has X's species (one density function, one CTIP exponential)
+//   MHOMO: same-species metals, whose pair B-term is the density shape (METAL_HOMO)
+template <typename R, bool SAME, bool MHOMO, bool EFLAG>
+__device__ __forceinline__ R pair_fs(const PairTab<R>& T, R r, R ir, R qa, R qb, R dFX, R dFY, R a,
+                                     R two_a_sqrtpi, R kc, R& erfcv, double& ep, double& ed, double& ec) {
+    const R ir2 = ir * ir;
+    R fs;
+    if (MHOMO) {
+        R g, dg, gA, dgA;
+        zhou<R>(r, T.d_inv_re, T.d_c, T.d_lam, g, dg);          // ftn, eam.f90:21-23
+        zhou<R>(r, T.p_inv_re, T.p_alpha, T.p_kappa, gA, dgA);  // eam.f90:29-31
+        fs = -(T.p_A * dgA - T.p_B * dg + (dFX + dFY) * T.d_fe * dg) * ir;
+        if (EFLAG) ep += (double)(T.p_A * gA - T.p_B * g);
+    } else {
+        R gD, dgD, gA, dgA, gB, dgB, dgE;
+        zhou<R>(r, T.d_inv_re, T.d_c, T.d_lam, gD, dgD);
+        if (SAME) {
+            dgE = dgD;
+        } else {
+            R gE;
+            zhou<R>(r, T.e_inv_re, T.e_c, T.e_lam, gE, dgE);
+        }
+        zhou<R>(r, T.p_inv_re, T.p_alpha, T.p_kappa, gA, dgA);
+        zhou<R>(r, T.p_inv_re, T.p_beta, T.p_lambda, gB, dgB);
+        fs = -(T.p_A * dgA - T.p_B * dgB + dFX * T.d_fe * dgD + dFY * T.e_fe * dgE) * ir;
+        if (EFLAG) ep += (double)(T.p_A * gA - T.p_B * gB);
+    }
+    // Ewald real space (force.f90:94-98)
+    R ea;
+    erfc_exp<R>(a * r, erfcv, ea);
+    fs += kc * qa * qb * (two_a_sqrtpi * r * ea + erfcv) * ir2 * ir;
+    // CTIP (force.f90:101-140)
+    const R eX = dexp<R>(R(-2) * T.xi_x * r);
+    const R eY = SAME ? eX : dexp<R>(R(-2) * T.xi_y * r);
+    const R djfi = eX * (R(2) * T.xi_x * T.xi_x + (R(1) + R(2) * T.xi_x * r) * ir2);
+    const R difj = SAME ? djfi : eY * (R(2) * T.xi_y * T.xi_y + (R(1) + R(2) * T.xi_y * r) * ir2);
+    const R QX = T.Qx[0] + r * (T.Qx[1] + r * T.Qx[2]) + ir * (T.Qx[3] + ir * T.Qx[4]);
+    R dfifj = eX * QX;
+    if (!SAME) dfifj += eY * (T.Qy[0] + ir * (T.Qy[3] + ir * T.Qy[4]));
+    const R ZX = T.Z_x, ZY = T.Z_y;
+    fs += kc * ((qa * ZY + qb * ZX - qa * qb) * dfifj - qa * ZY * djfi - qb * ZX * difj) * ir;
+    if (EFLAG) {
+        ed += (double)(qa * qb * erfcv * ir);
+        const R jfi = -eX * (T.xi_x + ir);
+        const R ifj = SAME ? jfi : -eY * (T.xi_y + ir);
+        R fifj = -eX * (T.Px[0] + r * (T.Px[1] + r * (T.Px[2] + r * T.Px[3])) + T.Px[4] * ir);
+        if (!SAME) fifj -= eY * (T.Py[0] + T.Py[4] * ir);
+        ec += (double)(qa * ZY * (jfi - fifj) + qb * ZX * (ifj - fifj) + qa * qb * fifj);
+    }
+    return fs;
+}
+
+// One group of X's row with a fixed specialisation.
+// F' of a partner: the FP32 copy on the mixed path, FP64 otherwise
+template <typename R> __device__ __forceinline__ R dFY_of(const double* dF, const float* dFf, int Y);
+template <> __device__ __forceinline__ double dFY_of<double>(const double* dF, const float*, int Y) { return dF[Y]; }
+template <> __device__ __forceinline__ float dFY_of<float>(const double*, const float* dFf, int Y) { return dFf[Y]; }
+
+template <typename R, bool SAME, bool MHOMO, bool EFLAG, bool RDF>
+__device__ __forceinline__ void force_group(const PairParams& P, const PairTab<R>* st, const unsigned* row, int g,
+                                            int mg, int lane, const double4& xa, int sX, int sY_fixed, R qa, R dFX,
+                                            const double4* __restrict__ xq, const int* __restrict__ ts,
+                                            const double* __restrict__ dF_s, const float* __restrict__ dF_f,
+                                            double& fx, double& fy, double& fz,
+                                            double& ep, double& ed, double& ec, int* hist, int& bad) {
+    constexpr int NB = SIMOX_NRDF + 2;
+    const R a = (R)P.a;
+    const R two_a_sqrtpi = (R)(2.0 * P.a / SX_SQRTPI);
+    const R kc = (R)P.kc;
+    const int nm = g == 2 ? sY_fixed : 0;
+    if (g == 2) sY_fixed = -1;
+    // software pipeline: the next iteration's list entry, position and F' are
+    // loaded before this iteration's arithmetic
+    unsigned ent_n = 0;
+    double4 xb_n = make_double4(0, 0, 0, 0);
+    R dFY_n = 0;
+    if (lane < mg) {
+        ent_n = row[row_slot(g, lane, P.cap, nm)];
+        xb_n = xq[ent_n & kIdxMask];
+        dFY_n = dFY_of<R>(dF_s, dF_f, (int)(ent_n & kIdxMask));
+    }
+    for (int k = lane; k < mg; k += 32) {
+        const unsigned ent = ent_n;
+        const int Y = (int)(ent & kIdxMask);
+        const double4 xb = xb_n;
+        const R dFY = dFY_n;
+        if (k + 32 < mg) {
+            ent_n = row[row_slot(g, k + 32, P.cap, nm)];
+            xb_n = xq[ent_n & kIdxMask];
+            dFY_n = dFY_of<R>(dF_s, dF_f, (int)(ent_n & kIdxMask));
+        }
+        const int sY = sY_fixed >= 0 ? sY_fixed : ts[Y];
+        if (sY >= kSpecies) { bad |= ST_UNKNOWN_PAIR; continue; }
+        if (MHOMO && sY != sX) { bad |= ST_UNSUPPORTED; continue; }
+        double dx, dy, dz;
+        min_image(xa, xb, P, dx, dy, dz);
+        const double r2d = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+        R r, ir;
+        if (sizeof(R) == 8) { r = (R)sqrt(r2d); ir = R(1) / r; }
+        else { ir = (R)rsqrtf((float)r2d); r = (R)r2d * ir; }
+        const PairTab<R>& T = st[sX * kSpecies + sY];
+        R erfcv;
+        const R fs = pair_fs<R, SAME, MHOMO, EFLAG>(T, r, ir, qa, (R)xb.w, dFX, dFY, a, two_a_sqrtpi, kc, erfcv, ep,
+                                                    ed, ec);
+        // f_X += rx * fs, accumulated in FP64 on the FP64 separation
+        const double fsd = (double)fs;
+        fx = fma(fsd, dx, fx);
+        fy = fma(fsd, dy, fy);
+        fz = fma(fsd, dz, fz);
+        if (RDF && (ent & kIsA)) {
+            int bin;
+            if (sizeof(R) == 8) bin = __double2int_rz(__ddiv_rn(__dsqrt_rn(r2d), P.dr_rdf));  // INT(r/dr)
+            else bin = (int)((float)r * (float)(1.0 / P.dr_rdf));
+            bin = min(max(bin, 0), NB - 1);
+            atomicAdd(&hist[(sX + kSpecies * sY) * NB + bin], 2);
+        }
+    }
+}
+
 // pass 2 -------------------------------------------------------------------
+// Block shape: FP32 uses 256-thread CTAs, 3 per SM (<= 85 registers); the
+// FP64 variant needs ~150 registers, so 128-thread CTAs pack 3 per SM.
+template <typename R> struct ForceShape {
+    static constexpr int threads = sizeof(R) == 4 ? 256 : 128;
+    static constexpr int blocks = sizeof(R) == 4 ? 3 : 4;
+};
+
 template <typename R, bool EFLAG, bool RDF>
-__global__ void __launch_bounds__(PK_THREADS)
+__global__ void __launch_bounds__(ForceShape<R>::threads, ForceShape<R>::blocks)
     force_kernel(PairParams P, const PairTab<R>* __restrict__ tab, const double4* __restrict__ xq,
-                 const int* __restrict__ ts, const int* __restrict__ nn, const unsigned* __restrict__ nbr,
-                 const double* __restrict__ dF_s, const int* __restrict__ sorted, double* __restrict__ f,
-                 double* __restrict__ acc, int* __restrict__ rdf, int* __restrict__ status) {
+                 const int* __restrict__ ts, const int2* __restrict__ nn, const unsigned* __restrict__ nbr,
+                 const double* __restrict__ dF_s, const float* __restrict__ dF_f, const int* __restrict__ sorted,
+                 double* __restrict__ f, double* __restrict__ acc, int* __restrict__ rdf, int* __restrict__ status) {
+    constexpr int NT = ForceShape<R>::threads;
     __shared__ PairTab<R> st[kSpecies * kSpecies];
-    __shared__ double red[PK_THREADS / 32];
+    __shared__ double red[NT / 32];
     constexpr int NB = SIMOX_NRDF + 2;
     __shared__ int hist[RDF ? kSpecies * kSpecies * NB : 1];
     for (int k = threadIdx.x; k < kSpecies * kSpecies; k += blockDim.x) st[k] = tab[k];
@@ -244,9 +415,6 @@ __global__ void __launch_bounds__(PK_THREADS)
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int wpb = blockDim.x >> 5;
-    const R a = (R)P.a;
-    const R two_a_sqrtpi = (R)(2.0 * P.a / SX_SQRTPI);
-    const R kc = (R)P.kc;
     double ep = 0.0, ed = 0.0, ec = 0.0;
     int bad = 0;
     for (int X = blockIdx.x * wpb + (threadIdx.x >> 5); X < P.n; X += gridDim.x * wpb) {
@@ -254,70 +422,26 @@ __global__ void __launch_bounds__(PK_THREADS)
         const int sX = ts[X];
         const R qa = (R)xa.w;
         const R dFX = (R)dF_s[X];
-        const int m = nn[X];
+        const int2 m = nn[X];
         const unsigned* row = nbr + (size_t)X * P.cap;
         double fx = 0.0, fy = 0.0, fz = 0.0;
-        for (int k = lane; k < m; k += 32) {
-            const unsigned ent = row[k];
-            const int Y = (int)(ent & kIdxMask);
-            const double4 xb = xq[Y];
-            const int sY = ts[Y];
-            if (sX >= kSpecies || sY >= kSpecies) { bad |= ST_UNKNOWN_PAIR; continue; }
-            double dx, dy, dz;
-            min_image(xa, xb, P, dx, dy, dz);
-            const double r2d = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-            const R rx = (R)dx, ry = (R)dy, rz = (R)dz;
-            const R r2 = (R)r2d;
-            const R r = sqrt(r2);
-            const R ir = drcp<R>(r);
-            const R ir2 = ir * ir;
-            const PairTab<R>& T = st[sX * kSpecies + sY];
-            const R qb = (R)xb.w;
-            const R dFY = (R)dF_s[Y];
-            // EAM (eam.f90 pair forms; force.f90:81-91, 349, 356)
-            R gD, dgD, gE, dgE, gA, dgA, gB, dgB;
-            zhou<R>(r, T.d_inv_re, T.d_c, T.d_lam, gD, dgD);
-            zhou<R>(r, T.e_inv_re, T.e_c, T.e_lam, gE, dgE);
-            zhou<R>(r, T.p_inv_re, T.p_alpha, T.p_kappa, gA, dgA);
-            zhou<R>(r, T.p_inv_re, T.p_beta, T.p_lambda, gB, dgB);
-            const R dphi = T.p_A * dgA - T.p_B * dgB;
-            R fs = -(dphi + dFX * T.d_fe * dgD + dFY * T.e_fe * dgE) * ir;
-            // Ewald real space (force.f90:94-98)
-            const R ar = a * r;
-            const R erfcv = derfc<R>(ar);
-            const R ea = dexp<R>(-ar * ar);
-            fs += kc * qa * qb * (two_a_sqrtpi * r * ea + erfcv) * ir2 * ir;
-            // CTIP (force.f90:101-140)
-            const R eX = dexp<R>(R(-2) * T.xi_x * r);
-            const R eY = dexp<R>(R(-2) * T.xi_y * r);
-            const R djfi = eX * (R(2) * T.xi_x * T.xi_x + (R(1) + R(2) * T.xi_x * r) * ir2);
-            const R difj = eY * (R(2) * T.xi_y * T.xi_y + (R(1) + R(2) * T.xi_y * r) * ir2);
-            const R QX = T.Qx[0] + r * (T.Qx[1] + r * T.Qx[2]) + ir * (T.Qx[3] + ir * T.Qx[4]);
-            const R QY = T.Qy[0] + r * (T.Qy[1] + r * T.Qy[2]) + ir * (T.Qy[3] + ir * T.Qy[4]);
-            const R dfifj = eX * QX + eY * QY;
-            const R ZX = T.Z_x, ZY = T.Z_y;
-            fs += kc * ((qa * ZY + qb * ZX - qa * qb) * dfifj - qa * ZY * djfi - qb * ZX * difj) * ir;
-            fx += (double)(rx * fs);
-            fy += (double)(ry * fs);
-            fz += (double)(rz * fs);
-            if (!T.valid) bad |= ST_UNSUPPORTED;
-            if (EFLAG) {
-                ep += (double)(T.p_A * gA - T.p_B * gB);
-                ed += (double)(qa * qb * erfcv * ir);
-                const R jfi = -eX * (T.xi_x + ir);
-                const R ifj = -eY * (T.xi_y + ir);
-                const R PX = T.Px[0] + r * (T.Px[1] + r * (T.Px[2] + r * T.Px[3])) + T.Px[4] * ir;
-                const R PY = T.Py[0] + r * (T.Py[1] + r * (T.Py[2] + r * T.Py[3])) + T.Py[4] * ir;
-                const R fifj = -(eX * PX + eY * PY);
-                ec += (double)(qa * ZY * (jfi - fifj) + qb * ZX * (ifj - fifj) + qa * qb * fifj);
-            }
-            if (RDF && (ent & kIsA)) {
-                int bin;
-                if (sizeof(R) == 8) bin = __double2int_rz(__ddiv_rn(__dsqrt_rn(r2d), P.dr_rdf));  // INT(r/dr)
-                else bin = (int)((float)r * (float)(1.0 / P.dr_rdf));
-                bin = min(max(bin, 0), NB - 1);
-                atomicAdd(&hist[(sX + kSpecies * sY) * NB + bin], 2);
-            }
+        if (sX >= kSpecies) {
+            if (m.x + m.y > 0) bad |= ST_UNKNOWN_PAIR;
+        } else if (sizeof(R) == 8) {
+            // FP64: one table-driven body over the whole row (the inlined FP64
+            // exp/erfc sequences make per-species copies overflow the I-cache)
+            force_group<R, false, false, EFLAG, RDF>(P, st, row, 2, m.x + m.y, lane, xa, sX, m.x, qa, dFX, xq, ts,
+                                                     dF_s, dF_f, fx, fy, fz, ep, ed, ec, hist, bad);
+        } else if (sX < 3) {   // metal X: metal partners (same species) then oxygen partners
+            force_group<R, true, true, EFLAG, RDF>(P, st, row, 0, m.x, lane, xa, sX, -1, qa, dFX, xq, ts, dF_s, dF_f, fx,
+                                                   fy, fz, ep, ed, ec, hist, bad);
+            force_group<R, false, false, EFLAG, RDF>(P, st, row, 1, m.y, lane, xa, sX, 3, qa, dFX, xq, ts, dF_s, dF_f,
+                                                     fx, fy, fz, ep, ed, ec, hist, bad);
+        } else {               // oxygen X: metal partners then oxygen partners
+            force_group<R, false, false, EFLAG, RDF>(P, st, row, 0, m.x, lane, xa, sX, -1, qa, dFX, xq, ts, dF_s, dF_f,
+                                                     fx, fy, fz, ep, ed, ec, hist, bad);
+            force_group<R, true, false, EFLAG, RDF>(P, st, row, 1, m.y, lane, xa, sX, 3, qa, dFX, xq, ts, dF_s, dF_f, fx,
+                                                    fy, fz, ep, ed, ec, hist, bad);
         }
         fx = warp_sum(fx);
         fy = warp_sum(fy);
@@ -331,9 +455,9 @@ __global__ void __launch_bounds__(PK_THREADS)
     }
     if (bad) atomicOr(status, bad);
     if (EFLAG) {
-        block_add<PK_THREADS>(0.5 * ep, acc, A_EPAIR, red);
-        block_add<PK_THREADS>(0.5 * ed, acc, A_EDIR, red);
-        block_add<PK_THREADS>(0.5 * ec, acc, A_ECTIP, red);
+        block_add<NT>(0.5 * ep, acc, A_EPAIR, red);
+        block_add<NT>(0.5 * ed, acc, A_EDIR, red);
+        block_add<NT>(0.5 * ec, acc, A_ECTIP, red);
     }
     if (RDF) {
         __syncthreads();
@@ -384,20 +508,26 @@ static int pair_grid(simox_ctx* c) {
     return need < lim ? (need > 0 ? need : 1) : lim;
 }
 
+// In the mixed mode the energies are FP64: a pass that must produce energies
+// runs the FP64 kernels (densities, embedding, forces and energies).
+static bool use_fp64(const simox_ctx* c, bool eflag) { return c->precision == SIMOX_FP64 || eflag; }
+
 int eam_density(simox_ctx* c, bool eflag) {
     int st = ensure_list(c);
     if (st) return st;
     if (c->n == 0) return SIMOX_OK;
     PairParams P = pair_params(c);
     EmbedParams E = embed_params(c->pot);
-    Launch L(c, "eam_density");
-    if (c->precision == SIMOX_MIXED)
-        density_kernel<float><<<pair_grid(c), PK_THREADS, 0, c->stream>>>(P, c->tab_f, c->xq_s, c->t_s, c->nn, c->nbr, E,
-                                                                         c->rho_s, c->dF_s, c->acc, c->status, eflag);
+    Launch L(c, use_fp64(c, eflag) ? "eam_density_fp64" : "eam_density");
+    if (!use_fp64(c, eflag))
+        density_kernel<float><<<pair_grid(c), PK_THREADS, 0, c->stream>>>(P, c->tab_f, c->xq_s, c->t_s,
+                                                                         reinterpret_cast<const int2*>(c->nn), c->nbr, E,
+                                                                         c->rho_s, c->dF_s, c->dF_f, c->acc, c->status, eflag);
     else
-        density_kernel<double><<<pair_grid(c), PK_THREADS, 0, c->stream>>>(P, c->tab_d, c->xq_s, c->t_s, c->nn, c->nbr,
-                                                                          E, c->rho_s, c->dF_s, c->acc, c->status,
-                                                                          eflag);
+        density_kernel<double><<<pair_grid(c), PK_THREADS, 0, c->stream>>>(P, c->tab_d, c->xq_s, c->t_s,
+                                                                          reinterpret_cast<const int2*>(c->nn), c->nbr,
+                                                                          E, c->rho_s, c->dF_s, c->dF_f, c->acc,
+                                                                          c->status, eflag);
     c->eam_valid = true;
     return check_launch(c);
 }
@@ -405,26 +535,29 @@ int eam_density(simox_ctx* c, bool eflag) {
 template <typename R>
 static void launch_force(simox_ctx* c, const PairTab<R>* tab, bool eflag, bool rdf) {
     PairParams P = pair_params(c);
-    int g = pair_grid(c);
+    constexpr int PK_THREADS = ForceShape<R>::threads;
+    const int wpb = PK_THREADS / 32;
+    int g = std::min((c->n + wpb - 1) / wpb, num_sms(c) * 3 * (256 / PK_THREADS) * 2);
+    if (g < 1) g = 1;
     if (eflag && rdf)
-        force_kernel<R, true, true><<<g, PK_THREADS, 0, c->stream>>>(P, tab, c->xq_s, c->t_s, c->nn, c->nbr, c->dF_s,
+        force_kernel<R, true, true><<<g, PK_THREADS, 0, c->stream>>>(P, tab, c->xq_s, c->t_s, reinterpret_cast<const int2*>(c->nn), c->nbr, c->dF_s, c->dF_f,
                                                                      c->sorted, c->f, c->acc, c->rdf, c->status);
     else if (eflag)
-        force_kernel<R, true, false><<<g, PK_THREADS, 0, c->stream>>>(P, tab, c->xq_s, c->t_s, c->nn, c->nbr, c->dF_s,
+        force_kernel<R, true, false><<<g, PK_THREADS, 0, c->stream>>>(P, tab, c->xq_s, c->t_s, reinterpret_cast<const int2*>(c->nn), c->nbr, c->dF_s, c->dF_f,
                                                                       c->sorted, c->f, c->acc, c->rdf, c->status);
     else if (rdf)
-        force_kernel<R, false, true><<<g, PK_THREADS, 0, c->stream>>>(P, tab, c->xq_s, c->t_s, c->nn, c->nbr, c->dF_s,
+        force_kernel<R, false, true><<<g, PK_THREADS, 0, c->stream>>>(P, tab, c->xq_s, c->t_s, reinterpret_cast<const int2*>(c->nn), c->nbr, c->dF_s, c->dF_f,
                                                                       c->sorted, c->f, c->acc, c->rdf, c->status);
     else
-        force_kernel<R, false, false><<<g, PK_THREADS, 0, c->stream>>>(P, tab, c->xq_s, c->t_s, c->nn, c->nbr, c->dF_s,
+        force_kernel<R, false, false><<<g, PK_THREADS, 0, c->stream>>>(P, tab, c->xq_s, c->t_s, reinterpret_cast<const int2*>(c->nn), c->nbr, c->dF_s, c->dF_f,
                                                                        c->sorted, c->f, c->acc, c->rdf, c->status);
 }
 
 int pair_forces(simox_ctx* c, bool eflag, bool rdf) {
     if (!c->eam_valid) return SIMOX_E_STATE;
     if (c->n == 0) return SIMOX_OK;
-    Launch L(c, "pair_force");
-    if (c->precision == SIMOX_MIXED) launch_force<float>(c, c->tab_f, eflag, rdf);
+    Launch L(c, use_fp64(c, eflag) ? "pair_force_fp64" : "pair_force");
+    if (!use_fp64(c, eflag)) launch_force<float>(c, c->tab_f, eflag, rdf);
     else launch_force<double>(c, c->tab_d, eflag, rdf);
     return check_launch(c);
 }

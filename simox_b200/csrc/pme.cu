@@ -312,15 +312,39 @@ static double bmod_inv_host(int p, int k, int K) {
     return 1.0 / (b * b);
 }
 
-int pme_free(simox_ctx* c) {
-    if (c->plans) {
-        cufftDestroy(c->plan_r2c);
-        cufftDestroy(c->plan_c2r);
-        c->plans = false;
+static void pme_res_free(PmeRes& R) {
+    if (R.ready) {
+        cufftDestroy(R.r2c);
+        cufftDestroy(R.c2r);
     }
-    cudaFree(c->grid); cudaFree(c->cgrid); cudaFree(c->infl); cudaFree(c->psi); cudaFree(c->bmod);
-    c->grid = c->cgrid = c->infl = nullptr;
+    cudaFree(R.grid); cudaFree(R.cgrid); cudaFree(R.infl);
+    R = PmeRes();
+}
+
+int pme_free(simox_ctx* c) {
+    pme_res_free(c->pme[0]);
+    pme_res_free(c->pme[1]);
+    cudaFree(c->psi); cudaFree(c->bmod);
     c->psi = c->bmod = nullptr;
+    return SIMOX_OK;
+}
+
+static int pme_res_init(simox_ctx* c, PmeRes& R, bool dbl) {
+    const int* K = c->fft;
+    const size_t rs = dbl ? sizeof(double) : sizeof(float);
+    R.dbl = dbl;
+    if (cudaMalloc(&R.grid, c->ngrid * rs) != cudaSuccess) return SIMOX_E_NOMEM;
+    if (cudaMalloc(&R.cgrid, c->nhalf * 2 * rs) != cudaSuccess) return SIMOX_E_NOMEM;
+    if (cudaMalloc(&R.infl, c->nhalf * rs) != cudaSuccess) return SIMOX_E_NOMEM;
+    // cuFFT plans: dims slowest-first (K3, K2, K1); K1 is the contiguous x axis
+    if (cufftPlan3d(&R.r2c, K[2], K[1], K[0], dbl ? CUFFT_D2Z : CUFFT_R2C) != CUFFT_SUCCESS) return SIMOX_E_FFT_SIZE;
+    if (cufftPlan3d(&R.c2r, K[2], K[1], K[0], dbl ? CUFFT_Z2D : CUFFT_C2R) != CUFFT_SUCCESS) {
+        cufftDestroy(R.r2c);
+        return SIMOX_E_FFT_SIZE;
+    }
+    cufftSetStream(R.r2c, c->stream);
+    cufftSetStream(R.c2r, c->stream);
+    R.ready = true;
     return SIMOX_OK;
 }
 
@@ -328,22 +352,11 @@ int pme_setup(simox_ctx* c) {
     const int* K = c->fft;
     c->ngrid = (size_t)K[0] * K[1] * K[2];
     c->nhalf = (size_t)(K[0] / 2 + 1) * K[1] * K[2];
-    const bool dbl = c->precision == SIMOX_FP64;
-    const size_t rs = dbl ? sizeof(double) : sizeof(float);
-    if (cudaMalloc(&c->grid, c->ngrid * rs) != cudaSuccess) return SIMOX_E_NOMEM;
-    if (cudaMalloc(&c->cgrid, c->nhalf * 2 * rs) != cudaSuccess) return SIMOX_E_NOMEM;
-    if (cudaMalloc(&c->infl, c->nhalf * rs) != cudaSuccess) return SIMOX_E_NOMEM;
+    int st = pme_res_init(c, c->pme[0], c->precision == SIMOX_FP64);
+    if (st) return st;
+    if (c->precision != SIMOX_FP64 && (st = pme_res_init(c, c->pme[1], true))) return st;
     if (cudaMalloc(&c->psi, c->ngrid * sizeof(double)) != cudaSuccess) return SIMOX_E_NOMEM;
     if (cudaMalloc(&c->bmod, (K[0] + K[1] + K[2]) * sizeof(double)) != cudaSuccess) return SIMOX_E_NOMEM;
-    // cuFFT plans: dims slowest-first (K3, K2, K1); K1 is the contiguous x axis
-    if (cufftPlan3d(&c->plan_r2c, K[2], K[1], K[0], dbl ? CUFFT_D2Z : CUFFT_R2C) != CUFFT_SUCCESS) return SIMOX_E_FFT_SIZE;
-    if (cufftPlan3d(&c->plan_c2r, K[2], K[1], K[0], dbl ? CUFFT_Z2D : CUFFT_C2R) != CUFFT_SUCCESS) {
-        cufftDestroy(c->plan_r2c);
-        return SIMOX_E_FFT_SIZE;
-    }
-    cufftSetStream(c->plan_r2c, c->stream);
-    cufftSetStream(c->plan_c2r, c->stream);
-    c->plans = true;
     std::vector<double> bm(K[0] + K[1] + K[2]);
     int o = 0;
     for (int d = 0; d < 3; d++)
@@ -354,7 +367,7 @@ int pme_setup(simox_ctx* c) {
     return cuda_status(cudaStreamSynchronize(c->stream));
 }
 
-// PME_SELF: psi table, influence function, self energy into acc
+// PME_SELF: psi table, influence function(s), self energy into acc
 int pme_self(simox_ctx* c) {
     int3 K = make_int3(c->fft[0], c->fft[1], c->fft[2]);
     double3 box = make_double3(c->box[0], c->box[1], c->box[2]);
@@ -362,15 +375,17 @@ int pme_self(simox_ctx* c) {
         Launch L(c, "pme_psi");
         psi_kernel<<<num_sms(c) * 4, 256, 0, c->stream>>>(K, box, c->a * c->a, c->psi);
     }
-    {
+    const double invN = 1.0 / (double)c->ngrid;
+    for (int k = 0; k < 2; k++) {
+        PmeRes& R = c->pme[k];
+        if (!R.ready) continue;
         Launch L(c, "pme_influence_build");
-        const double invN = 1.0 / (double)c->ngrid;
-        if (c->precision == SIMOX_FP64)
+        if (R.dbl)
             infl_build_kernel<double><<<num_sms(c) * 4, 256, 0, c->stream>>>(K, K.x / 2 + 1, c->psi, c->bmod, invN,
-                                                                             (double*)c->infl);
+                                                                             (double*)R.infl);
         else
             infl_build_kernel<float><<<num_sms(c) * 4, 256, 0, c->stream>>>(K, K.x / 2 + 1, c->psi, c->bmod, invN,
-                                                                            (float*)c->infl);
+                                                                            (float*)R.infl);
     }
     c->psi_valid = true;
     if (c->n > 0) {
@@ -389,42 +404,37 @@ int pme_self(simox_ctx* c) {
 }
 
 template <typename R, int P>
-static void run_spread(simox_ctx* c, const PmeParams& S, const double* qalt) {
-    cudaMemsetAsync(c->grid, 0, c->ngrid * sizeof(R), c->stream);
+static void run_spread(simox_ctx* c, PmeRes& Rs, const PmeParams& S, const double* qalt) {
+    cudaMemsetAsync(Rs.grid, 0, c->ngrid * sizeof(R), c->stream);
     Launch L(c, "pme_spread");
-    spread_kernel<R, P><<<(S.n + 127) / 128, 128, 0, c->stream>>>(S, c->xq_s, qalt, (R*)c->grid,
-                                                                  c->precision == SIMOX_FP64 ? 1 : 0);
+    spread_kernel<R, P><<<(S.n + 127) / 128, 128, 0, c->stream>>>(S, c->xq_s, qalt, (R*)Rs.grid, Rs.dbl ? 1 : 0);
 }
 
-static int run_convolution(simox_ctx* c, bool eflag) {
+static int run_convolution(simox_ctx* c, PmeRes& Rs, bool eflag) {
     cufftResult r;
     {
         Launch L(c, "pme_fft_r2c");
-        if (c->precision == SIMOX_FP64)
-            r = cufftExecD2Z(c->plan_r2c, (cufftDoubleReal*)c->grid, (cufftDoubleComplex*)c->cgrid);
-        else
-            r = cufftExecR2C(c->plan_r2c, (cufftReal*)c->grid, (cufftComplex*)c->cgrid);
+        if (Rs.dbl) r = cufftExecD2Z(Rs.r2c, (cufftDoubleReal*)Rs.grid, (cufftDoubleComplex*)Rs.cgrid);
+        else r = cufftExecR2C(Rs.r2c, (cufftReal*)Rs.grid, (cufftComplex*)Rs.cgrid);
     }
     if (r != CUFFT_SUCCESS) return SIMOX_E_CUDA;
     {
         Launch L(c, "pme_influence");
         int kxh = c->fft[0] / 2 + 1;
         int g = num_sms(c) * 4;
-        if (c->precision == SIMOX_FP64)
-            influence_kernel<double><<<g, 256, 0, c->stream>>>(c->nhalf, kxh, c->fft[0], (double2*)c->cgrid,
-                                                               (const double*)c->infl, (double)c->ngrid, c->acc,
+        if (Rs.dbl)
+            influence_kernel<double><<<g, 256, 0, c->stream>>>(c->nhalf, kxh, c->fft[0], (double2*)Rs.cgrid,
+                                                               (const double*)Rs.infl, (double)c->ngrid, c->acc,
                                                                eflag ? 1 : 0);
         else
-            influence_kernel<float><<<g, 256, 0, c->stream>>>(c->nhalf, kxh, c->fft[0], (float2*)c->cgrid,
-                                                              (const float*)c->infl, (double)c->ngrid, c->acc,
+            influence_kernel<float><<<g, 256, 0, c->stream>>>(c->nhalf, kxh, c->fft[0], (float2*)Rs.cgrid,
+                                                              (const float*)Rs.infl, (double)c->ngrid, c->acc,
                                                               eflag ? 1 : 0);
     }
     {
         Launch L(c, "pme_fft_c2r");
-        if (c->precision == SIMOX_FP64)
-            r = cufftExecZ2D(c->plan_c2r, (cufftDoubleComplex*)c->cgrid, (cufftDoubleReal*)c->grid);
-        else
-            r = cufftExecC2R(c->plan_c2r, (cufftComplex*)c->cgrid, (cufftReal*)c->grid);
+        if (Rs.dbl) r = cufftExecZ2D(Rs.c2r, (cufftDoubleComplex*)Rs.cgrid, (cufftDoubleReal*)Rs.grid);
+        else r = cufftExecC2R(Rs.c2r, (cufftComplex*)Rs.cgrid, (cufftReal*)Rs.grid);
     }
     if (r != CUFFT_SUCCESS) return SIMOX_E_CUDA;
     return SIMOX_OK;
@@ -442,25 +452,25 @@ static PmeParams pme_params(const simox_ctx* c) {
 }
 
 template <typename R, int P>
-static int pme_forces_t(simox_ctx* c) {
+static int pme_forces_t(simox_ctx* c, PmeRes& Rs, bool eflag) {
     PmeParams S = pme_params(c);
-    run_spread<R, P>(c, S, nullptr);
-    int st = run_convolution(c, true);
+    run_spread<R, P>(c, Rs, S, nullptr);
+    int st = run_convolution(c, Rs, eflag);
     if (st) return st;
     Launch L(c, "pme_gather_force");
-    gather_force_kernel<R, P><<<(S.n + 127) / 128, 128, 0, c->stream>>>(S, c->xq_s, (const R*)c->grid, c->sorted,
+    gather_force_kernel<R, P><<<(S.n + 127) / 128, 128, 0, c->stream>>>(S, c->xq_s, (const R*)Rs.grid, c->sorted,
                                                                         c->f, c->acc);
     return SIMOX_OK;
 }
 
 template <typename R, int P>
-static int pme_pot_t(simox_ctx* c, const double* qalt, double* phi, double scale) {
+static int pme_pot_t(simox_ctx* c, PmeRes& Rs, const double* qalt, double* phi, double scale) {
     PmeParams S = pme_params(c);
-    run_spread<R, P>(c, S, qalt);
-    int st = run_convolution(c, false);
+    run_spread<R, P>(c, Rs, S, qalt);
+    int st = run_convolution(c, Rs, false);
     if (st) return st;
     Launch L(c, "pme_gather_pot");
-    gather_pot_kernel<R, P><<<(S.n + 127) / 128, 128, 0, c->stream>>>(S, c->xq_s, (const R*)c->grid, phi, scale);
+    gather_pot_kernel<R, P><<<(S.n + 127) / 128, 128, 0, c->stream>>>(S, c->xq_s, (const R*)Rs.grid, phi, scale);
     return SIMOX_OK;
 }
 
@@ -481,7 +491,7 @@ int pme_finalize_forces(simox_ctx* c) {
     return check_launch(c);
 }
 
-int pme_forces(simox_ctx* c, bool finalize) {
+int pme_forces(simox_ctx* c, bool finalize, bool eflag) {
     if (!c->psi_valid) return SIMOX_E_STATE;
     if (!c->gathered) {
         int st = gather_sorted(c);
@@ -490,11 +500,13 @@ int pme_forces(simox_ctx* c, bool finalize) {
     if (c->n == 0) return SIMOX_OK;
     cudaMemsetAsync(c->acc + A_FSUM0, 0, 3 * sizeof(double), c->stream);
     int st;
-    const bool dbl = c->precision == SIMOX_FP64;
+    // energies are FP64: a mixed context uses its FP64 twin when they are requested
+    PmeRes& Rs = (eflag && c->pme[1].ready) ? c->pme[1] : c->pme[0];
+    const bool dbl = Rs.dbl;
     switch (c->order) {
-        case 4: st = dbl ? pme_forces_t<double, 4>(c) : pme_forces_t<float, 4>(c); break;
-        case 6: st = dbl ? pme_forces_t<double, 6>(c) : pme_forces_t<float, 6>(c); break;
-        case 8: st = dbl ? pme_forces_t<double, 8>(c) : pme_forces_t<float, 8>(c); break;
+        case 4: st = dbl ? pme_forces_t<double, 4>(c, Rs, eflag) : pme_forces_t<float, 4>(c, Rs, eflag); break;
+        case 6: st = dbl ? pme_forces_t<double, 6>(c, Rs, eflag) : pme_forces_t<float, 6>(c, Rs, eflag); break;
+        case 8: st = dbl ? pme_forces_t<double, 8>(c, Rs, eflag) : pme_forces_t<float, 8>(c, Rs, eflag); break;
         default: return SIMOX_E_ARG;
     }
     if (st) return st;
@@ -508,12 +520,13 @@ int pme_forces(simox_ctx* c, bool finalize) {
 int pme_potential(simox_ctx* c, const double* qalt, double* phi, double scale) {
     if (!c->psi_valid) return SIMOX_E_STATE;
     if (c->n == 0) return SIMOX_OK;
-    const bool dbl = c->precision == SIMOX_FP64;
+    PmeRes& Rs = c->pme[0];
+    const bool dbl = Rs.dbl;
     int st;
     switch (c->order) {
-        case 4: st = dbl ? pme_pot_t<double, 4>(c, qalt, phi, scale) : pme_pot_t<float, 4>(c, qalt, phi, scale); break;
-        case 6: st = dbl ? pme_pot_t<double, 6>(c, qalt, phi, scale) : pme_pot_t<float, 6>(c, qalt, phi, scale); break;
-        case 8: st = dbl ? pme_pot_t<double, 8>(c, qalt, phi, scale) : pme_pot_t<float, 8>(c, qalt, phi, scale); break;
+        case 4: st = dbl ? pme_pot_t<double, 4>(c, Rs, qalt, phi, scale) : pme_pot_t<float, 4>(c, Rs, qalt, phi, scale); break;
+        case 6: st = dbl ? pme_pot_t<double, 6>(c, Rs, qalt, phi, scale) : pme_pot_t<float, 6>(c, Rs, qalt, phi, scale); break;
+        case 8: st = dbl ? pme_pot_t<double, 8>(c, Rs, qalt, phi, scale) : pme_pot_t<float, 8>(c, Rs, qalt, phi, scale); break;
         default: return SIMOX_E_ARG;
     }
     if (st) return st;

@@ -64,6 +64,15 @@ struct PairTab {
     int pad_;
 };
 
+// Device resources of one PME precision (grid, half spectrum, G/N, plans).
+struct PmeRes {
+    bool dbl = false, ready = false;
+    void* grid = nullptr;       // real grid K1*K2*K3 (x fastest)
+    void* cgrid = nullptr;      // half-spectrum complex grid
+    void* infl = nullptr;       // G/N on the half spectrum
+    cufftHandle r2c = 0, c2r = 0;
+};
+
 struct Profile {
     std::vector<std::string> names;
     std::vector<double> ms;
@@ -115,25 +124,23 @@ struct simox_ctx {
     int* t_s = nullptr;         // species 0..4
 
     // neighbour list
-    int* nn = nullptr;
-    unsigned* nbr = nullptr;    // [cap*nnb_cap]
+    int* nn = nullptr;          // [cap] int2: (metal partners, oxygen partners)
+    unsigned* nbr = nullptr;    // [cap*nnb_cap]; metal partners from the front, oxygen from the back
     int* nn_max = nullptr;      // device max
     unsigned long long* nn_tot = nullptr;
 
     // EAM
     double* rho_s = nullptr;
     double* dF_s = nullptr;
+    float* dF_f = nullptr;      // FP32 copy of F' for the mixed pair kernel
 
     // pair tables
     sx::PairTab<double>* tab_d = nullptr;
     sx::PairTab<float>* tab_f = nullptr;
 
-    // PME
-    cufftHandle plan_r2c = 0, plan_c2r = 0;
-    bool plans = false;
-    void* grid = nullptr;       // real grid (double or float)
-    void* cgrid = nullptr;      // half-spectrum complex grid
-    void* infl = nullptr;       // G/N on the half spectrum (double or float)
+    // PME: pme[0] in the context's precision; pme[1] the FP64 twin that a
+    // mixed-precision context uses when energies are requested
+    sx::PmeRes pme[2];
     double* psi = nullptr;      // full-grid psi (reference layout)
     double* bmod = nullptr;     // per-dimension 1/|b|^2, K1+K2+K3
 
@@ -207,7 +214,7 @@ int pair_forces(simox_ctx* c, bool eflag, bool rdf);
 int pme_setup(simox_ctx* c);
 int pme_free(simox_ctx* c);
 int pme_self(simox_ctx* c);
-int pme_forces(simox_ctx* c, bool finalize);
+int pme_forces(simox_ctx* c, bool finalize, bool eflag);
 int pme_potential(simox_ctx* c, const double* charges_sorted, double* phi_out, double scale);
 int pme_finalize_forces(simox_ctx* c);
 // ctip.cu

@@ -120,6 +120,9 @@ def test_ctip_fp64(name, s):
 
 @pytest.mark.parametrize("name,s", CASES[:2], ids=IDS[:2])
 def test_force_mixed(name, s):
+    """Mixed path: FP32 pair and PME terms give forces within 1e-5 (relative
+    norm); energies, requested separately, are FP64 and within 1e-7 eV/atom
+    (the PME grid stays FP32)."""
     o = oracle_system(s)
     o.cell_sort()
     o.pme_self()
@@ -128,13 +131,15 @@ def test_force_mixed(name, s):
     with gpu_context(s, precision="mixed") as g:
         g.pme_self()
         g.cell_sort()
+        g.force(energies=False)
+        g.pme(energies=False)
+        f = g.get_state()["f"]
         e = g.force()
         erec = g.pme()
-        f = g.get_state()["f"]
     assert rel_err(f, f_o) <= 1e-5, rel_err(f, f_o)
     etot_o = sum(e_o.values()) + erec_o
     etot = sum(e.values()) + erec
-    assert abs(etot - etot_o) / s.n <= 1e-6, (etot, etot_o)
+    assert abs(etot - etot_o) / s.n <= 1e-7, (etot, etot_o)
 
 
 def test_integrators_bit_exact():
