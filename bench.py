@@ -145,9 +145,18 @@ def profile_traffic(kernel):
 
 # Algorithmic bytes per launch of each kernel family (unique bytes a launch
 # must move: per-atom state in and out plus its neighbour-list row).  n atoms,
-# nnb mean neighbours, K grid points, p spline order.
-def algorithmic_bytes(name, n, nnb, K, prec):
+# nnb mean neighbours, K grid points, p spline order.  The skin list's mean
+# row length is taken as nnb ((Rcut + skin) / Rcut)^3 (uniform density).
+SKIN = 1.0
+
+
+def algorithmic_bytes(name, n, nnb, K, prec, rcut=10.0):
     r = 8 if prec == "fp64" else 4
+    nnb_s = nnb * ((rcut + SKIN) / rcut) ** 3
+    if name == "neighbor_filter_density":
+        # xq 32, type 4, cell 4, index 4, skin count 8, skin row 4*nnb_s in;
+        # exact row 4*nnb, count 8, rho 8, F' 8 + 4 out
+        return n * (32 + 4 + 4 + 4 + 8 + 4 * nnb_s + 4 * nnb + 8 + 8 + 12)
     if name == "pair_force":      # xq 32, type 4, count 4, F' 8, list 4*nnb in; force 24 out
         return n * (32 + 4 + 4 + 8 + 4 * nnb + 24)
     if name == "eam_density":     # xq 32, type 4, count 4, list 4*nnb in; rho, F' 16 out
@@ -376,7 +385,7 @@ def main():
               key=lambda k: prof[k][0])
     K = int(np.prod(s.fft))
     dom_ms = prof[dom][0] / max(prof[dom][1], 1)
-    dom_bytes = algorithmic_bytes(dom, s.n, nnb, K, "mixed")
+    dom_bytes = algorithmic_bytes(dom, s.n, nnb, K, "mixed", s.rcut)
     peak, peak_kind = measured_peaks()
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
     traffic = profile_traffic(dom)

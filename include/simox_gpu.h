@@ -109,6 +109,8 @@ typedef struct {
     int    nnb_max;      /* per-atom neighbour capacity (0 = 1024)               */
     int    device;       /* CUDA device ordinal                                  */
     int    flags;        /* SIMOX_FLAG_*                                         */
+    double skin;         /* Verlet skin (A) of the internal pair list: 0 = 1.0,
+                            < 0 = rebuild from the reference cells every call  */
 } simox_setup;
 
 /* Energies of TYPE STAT (datafmt.f90:59-63), all FP64, eV. */

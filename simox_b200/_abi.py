@@ -94,7 +94,7 @@ class Setup(C.Structure):
         ("n_atoms", C.c_int), ("capacity", C.c_int), ("box", C.c_double * 3),
         ("fft", C.c_int * 3), ("pme_order", C.c_int), ("rcut", C.c_double),
         ("precision", C.c_int), ("npt_max", C.c_int), ("nnb_max", C.c_int),
-        ("device", C.c_int), ("flags", C.c_int)]
+        ("device", C.c_int), ("flags", C.c_int), ("skin", C.c_double)]
 
 
 class Energies(C.Structure):

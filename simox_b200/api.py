@@ -124,7 +124,7 @@ class Simox:
 
     def __init__(self, ids, x, box, fft, rcut=10.0, q=None, v=None, f=None, order=4,
                  precision="fp64", capacity=0, npt_max=0, nnb_max=0, device=0, flags=0,
-                 potential: Potential | None = None):
+                 potential: Potential | None = None, skin: float = 0.0):
         self._ctx = _vp()
         ids = np.ascontiguousarray(ids, dtype=np.int32)
         n = len(ids)
@@ -141,6 +141,7 @@ class Simox:
         s.nnb_max = int(nnb_max)
         s.device = int(device)
         s.flags = int(flags)
+        s.skin = float(skin)
         self.setup = s
         self.precision = precision
         self.potential = potential if potential is not None else default_potential()

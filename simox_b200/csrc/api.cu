@@ -250,9 +250,10 @@ static void free_ctx(simox_ctx* c) {
     if (!c) return;
     prof_collect(c);
     pme_free(c);
-    void* bufs[] = {c->id, c->x, c->v, c->f, c->q, c->xm, c->cell_of, c->cell_count, c->cell_start, c->cell_fill,
-                    c->sorted, c->pair13, c->entries, c->xq_s, c->t_s, c->nn, c->nbr, c->nn_max, c->nn_tot,
-                    c->rho_s, c->dF_s, c->dF_f, c->tab_d, c->tab_f, c->c_const, c->g, c->pv, c->Ap, c->qs, c->jp,
+    void* bufs[] = {c->id, c->x, c->v, c->f, c->q, c->xm, c->cell_of, c->cell_xyz, c->cell_count, c->cell_start, c->cell_fill,
+                    c->sorted, c->pair13, c->entries, c->xq_s, c->t_s, c->cx_s, c->nn, c->nbr, c->nn_max, c->nn_tot,
+                    c->cs_count, c->cs_start, c->cs_fill, c->cs_cell_of, c->cs_entries, c->perm, c->x0,
+                    c->skin_flag, c->nn_s, c->nbr_s, c->rho_s, c->dF_s, c->dF_f, c->tab_d, c->tab_f, c->c_const, c->g, c->pv, c->Ap, c->qs, c->jp,
                     c->act, c->line, c->acc, c->status, c->rdf};
     for (void* p : bufs)
         if (p) cudaFree(p);
@@ -299,6 +300,9 @@ extern "C" int simox_create(const simox_setup* s, const simox_potential* pot, si
     c->order = order;
     c->npt_max = s->npt_max > 0 ? s->npt_max : SIMOX_NPT_MAX;
     c->nnb_cap = (c->flags & SIMOX_FLAG_REFERENCE_LIMITS) ? SIMOX_NNB_MAX : (s->nnb_max > 0 ? s->nnb_max : 1024);
+    c->cap_s = 2 * c->nnb_cap;
+    c->npt_max_s = std::max(2 * c->npt_max, 1024);
+    c->skin = s->skin == 0.0 ? 1.0 : s->skin;
     for (int d = 0; d < 3; d++) {
         c->box[d] = s->box[d];
         c->inv_box[d] = 1.0 / s->box[d];
@@ -314,7 +318,8 @@ extern "C" int simox_create(const simox_setup* s, const simox_potential* pot, si
         c->nc[d] = (int)(c->box[d] / c->rcut);
         c->lc[d] = c->box[d] / (double)c->nc[d];
     }
-    if ((c->nc[0] < 3 && c->nc[1] < 3 && c->nc[2] < 3) || c->nc[0] < 2 || c->nc[1] < 2 || c->nc[2] < 2) {
+    if ((c->nc[0] < 3 && c->nc[1] < 3 && c->nc[2] < 3) || c->nc[0] < 2 || c->nc[1] < 2 || c->nc[2] < 2 ||
+        c->nc[0] > 1024 || c->nc[1] > 1024 || c->nc[2] > 1024) {
         delete c;
         return SIMOX_E_CELL_TOO_SMALL;
     }
@@ -329,10 +334,10 @@ extern "C" int simox_create(const simox_setup* s, const simox_potential* pot, si
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { free_ctx(c); return SIMOX_E_CUDA; }
     const size_t N = (size_t)c->cap;
     bool ok = dalloc(&c->id, N) && dalloc(&c->x, 3 * N) && dalloc(&c->v, 3 * N) && dalloc(&c->f, 3 * N) &&
-              dalloc(&c->q, N) && dalloc(&c->cell_of, N) && dalloc(&c->cell_count, c->ncell) &&
+              dalloc(&c->q, N) && dalloc(&c->cell_of, N) && dalloc(&c->cell_xyz, N) && dalloc(&c->cell_count, c->ncell) &&
               dalloc(&c->cell_start, c->ncell + 1) && dalloc(&c->cell_fill, c->ncell) && dalloc(&c->sorted, N) &&
               dalloc(&c->pair13, (size_t)c->ncell * 13) && dalloc(&c->entries, (size_t)c->ncell * kEntries) &&
-              dalloc(&c->xq_s, N) && dalloc(&c->t_s, N) && dalloc(&c->nn, 2 * N) &&
+              dalloc(&c->xq_s, N) && dalloc(&c->t_s, N) && dalloc(&c->cx_s, N) && dalloc(&c->nn, 2 * N) &&
               dalloc(&c->nbr, N * (size_t)c->nnb_cap) && dalloc(&c->nn_max, 1) && dalloc(&c->nn_tot, 1) &&
               dalloc(&c->rho_s, N) && dalloc(&c->dF_s, N) && dalloc(&c->dF_f, N) && dalloc(&c->tab_d, kSpecies * kSpecies) &&
               dalloc(&c->tab_f, kSpecies * kSpecies) && dalloc(&c->line, 64) && dalloc(&c->acc, A_COUNT) &&
@@ -350,7 +355,9 @@ extern "C" int simox_create(const simox_setup* s, const simox_potential* pot, si
     cudaMemsetAsync(c->q, 0, sizeof(double) * N, c->stream);
     cudaEventCreate(&c->t0);
     cudaEventCreate(&c->t1);
-    if ((st = build_cell_tables(c)) || (st = build_pair_tables(c)) || (st = pme_setup(c)) || (st = ctip_alloc(c))) {
+    c->pair_order = c->sorted;
+    if ((st = build_cell_tables(c)) || (st = setup_skin(c)) || (st = build_pair_tables(c)) || (st = pme_setup(c)) ||
+        (st = ctip_alloc(c))) {
         free_ctx(c);
         return st;
     }
@@ -384,6 +391,13 @@ extern "C" int simox_set_state(simox_ctx* c, int n, const int* id, const double*
         c->have_ids = true;
     }
     if (n != c->n) c->cells_valid = false;
+    if (n != c->n || id) c->skin_valid = false;
+    if (x) {
+        bool inb = true;
+        for (int i = 0; i < 3 * n && inb; i++) inb = std::fabs(x[i]) <= c->hbox[i % 3];
+        c->in_box = inb;
+        c->cells_fresh = false;
+    }
     c->n = n;
     if (x) cudaMemcpyAsync(c->x, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s);
     if (v) cudaMemcpyAsync(c->v, v, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s);
@@ -532,7 +546,7 @@ extern "C" int simox_get_eam(simox_ctx* c, double* rho, double* dFdrho) {
     std::vector<int> srt(std::max(n, 1));
     cudaMemcpyAsync(r.data(), c->rho_s, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream);
     cudaMemcpyAsync(d.data(), c->dF_s, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream);
-    cudaMemcpyAsync(srt.data(), c->sorted, sizeof(int) * n, cudaMemcpyDeviceToHost, c->stream);
+    cudaMemcpyAsync(srt.data(), c->pair_order, sizeof(int) * n, cudaMemcpyDeviceToHost, c->stream);
     int st = cuda_status(cudaStreamSynchronize(c->stream));
     if (st) return st;
     for (int k = 0; k < n; k++) {

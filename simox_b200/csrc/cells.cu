@@ -79,7 +79,8 @@ int build_cell_tables(simox_ctx* c) {
 // ---------------------------------------------------------------------------
 // CELL_SORT kernels
 __global__ void bin_atoms_kernel(int n, const double* __restrict__ x, double3 hbox, double3 lc, int3 nc,
-                                 int* __restrict__ cell_of, int* __restrict__ count, int* __restrict__ status) {
+                                 int* __restrict__ cell_of, int* __restrict__ cell_xyz, int* __restrict__ count,
+                                 int* __restrict__ status) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int id[3];
@@ -99,11 +100,15 @@ __global__ void bin_atoms_kernel(int n, const double* __restrict__ x, double3 hb
     if (bad) atomicOr(status, ST_POSITION);
     int cell = id[0] + id[1] * m[0] + id[2] * m[0] * m[1];
     cell_of[i] = cell;
+    cell_xyz[i] = id[0] | (id[1] << 10) | (id[2] << 20);   // Ncell <= 1024 per axis (checked at set-up)
     atomicAdd(count + cell, 1);
 }
 
+// cond: nullptr, or a device flag that must be non-zero for the kernel to run
+// (the skin-list rebuild is decided on the device, without a host round trip)
 __global__ void scan_cells_kernel(const int* __restrict__ count, int* __restrict__ start, int* __restrict__ fill,
-                                  int ncell, int npt_max, int* __restrict__ status) {
+                                  int ncell, int npt_max, int* __restrict__ status, const int* __restrict__ cond) {
+    if (cond && *cond == 0) return;
     __shared__ int sm[1024];
     __shared__ int carry;
     const int t = threadIdx.x;
@@ -130,7 +135,8 @@ __global__ void scan_cells_kernel(const int* __restrict__ count, int* __restrict
 }
 
 __global__ void scatter_atoms_kernel(int n, const int* __restrict__ cell_of, int* __restrict__ fill,
-                                     int* __restrict__ sorted) {
+                                     int* __restrict__ sorted, const int* __restrict__ cond) {
+    if (cond && *cond == 0) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int slot = atomicAdd(fill + cell_of[i], 1);
@@ -138,7 +144,9 @@ __global__ void scatter_atoms_kernel(int n, const int* __restrict__ cell_of, int
 }
 
 // Rank sort inside each cell: ascending original index (= CELL_SORT order).
-__global__ void cell_rank_sort_kernel(const int* __restrict__ start, int* __restrict__ sorted, int npt_max) {
+__global__ void cell_rank_sort_kernel(const int* __restrict__ start, int* __restrict__ sorted, int npt_max,
+                                      const int* __restrict__ cond) {
+    if (cond && *cond == 0) return;
     extern __shared__ int buf[];
     const int cc = blockIdx.x;
     const int s0 = start[cc], n = start[cc + 1] - s0;
@@ -160,25 +168,26 @@ int cell_sort(simox_ctx* c) {
         Launch L(c, "cell_bin");
         bin_atoms_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(
             n, c->x, make_double3(c->hbox[0], c->hbox[1], c->hbox[2]), make_double3(c->lc[0], c->lc[1], c->lc[2]),
-            make_int3(c->nc[0], c->nc[1], c->nc[2]), c->cell_of, c->cell_count, c->status);
+            make_int3(c->nc[0], c->nc[1], c->nc[2]), c->cell_of, c->cell_xyz, c->cell_count, c->status);
     }
     {
         Launch L(c, "cell_scan");
         scan_cells_kernel<<<1, 1024, 0, c->stream>>>(c->cell_count, c->cell_start, c->cell_fill, c->ncell, c->npt_max,
-                                                     c->status);
+                                                     c->status, nullptr);
     }
     if (n > 0) {
         Launch L(c, "cell_scatter");
-        scatter_atoms_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, c->cell_of, c->cell_fill, c->sorted);
+        scatter_atoms_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, c->cell_of, c->cell_fill, c->sorted, nullptr);
     }
     {
         Launch L(c, "cell_order");
         cell_rank_sort_kernel<<<c->ncell, 128, sizeof(int) * c->npt_max, c->stream>>>(c->cell_start, c->sorted,
-                                                                                      c->npt_max);
+                                                                                      c->npt_max, nullptr);
     }
     int st = check_launch(c);
     if (st) return st;
     c->cells_valid = true;
+    c->cells_fresh = true;
     c->gathered = false;
     c->list_valid = false;
     return SIMOX_OK;
@@ -188,22 +197,25 @@ int cell_sort(simox_ctx* c) {
 // gather original-order state into cell order
 __global__ void gather_sorted_kernel(int n, const int* __restrict__ sorted, const double* __restrict__ x,
                                      const double* __restrict__ q, const int* __restrict__ id,
-                                     double4* __restrict__ xq, int* __restrict__ ts) {
+                                     const int* __restrict__ cell_xyz, double4* __restrict__ xq,
+                                     int* __restrict__ ts, int* __restrict__ cx) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     int o = sorted[k];
     xq[k] = make_double4(x[3 * o], x[3 * o + 1], x[3 * o + 2], q[o]);
     ts[k] = id[o] - 1;
+    cx[k] = cell_xyz[o];
 }
 
 int gather_sorted(simox_ctx* c) {
     if (!c->cells_valid) return SIMOX_E_STATE;
     if (c->n > 0) {
         Launch L(c, "gather_sorted");
-        gather_sorted_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->n, c->sorted, c->x, c->q, c->id, c->xq_s,
-                                                                        c->t_s);
+        gather_sorted_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->n, c->pair_order, c->x, c->q, c->id,
+                                                                        c->cell_xyz, c->xq_s, c->t_s, c->cx_s);
     }
     c->gathered = true;
+    c->rho_ready = false;
     return SIMOX_OK;
 }
 
@@ -254,7 +266,8 @@ __global__ void __launch_bounds__(LB_THREADS)
     build_list_kernel(const int* __restrict__ cell_start, const int* __restrict__ entries,
                       const double4* __restrict__ xq, const int* __restrict__ ts, unsigned* __restrict__ nbr,
                       int2* __restrict__ nn, LBParams P, int* __restrict__ status, int* __restrict__ nn_max,
-                      unsigned long long* __restrict__ nn_tot) {
+                      unsigned long long* __restrict__ nn_tot, const int* __restrict__ cond) {
+    if (cond && *cond == 0) return;
     extern __shared__ __align__(16) unsigned char smem[];
     float4* cpos = reinterpret_cast<float4*>(smem);
     unsigned* ctag = reinterpret_cast<unsigned*>(cpos + LB_TILE);
@@ -391,11 +404,11 @@ int build_list(simox_ctx* c) {
         if (c->fast_cells)
             build_list_kernel<true><<<c->ncell, LB_THREADS, smem, c->stream>>>(
                 c->cell_start, c->entries, c->xq_s, c->t_s, c->nbr, reinterpret_cast<int2*>(c->nn), P, c->status,
-                c->nn_max, c->nn_tot);
+                c->nn_max, c->nn_tot, nullptr);
         else
             build_list_kernel<false><<<c->ncell, LB_THREADS, smem, c->stream>>>(
                 c->cell_start, c->entries, c->xq_s, c->t_s, c->nbr, reinterpret_cast<int2*>(c->nn), P, c->status,
-                c->nn_max, c->nn_tot);
+                c->nn_max, c->nn_tot, nullptr);
     }
     int st = check_launch(c);
     if (st) return st;
@@ -403,19 +416,213 @@ int build_list(simox_ctx* c) {
     return SIMOX_OK;
 }
 
-int ensure_list(simox_ctx* c) {
-    if (!c->cells_valid) return SIMOX_E_STATE;
-    if (!c->gathered) {
-        int st = gather_sorted(c);
-        if (st) return st;
-        c->list_valid = false;
+// ---------------------------------------------------------------------------
+// Verlet skin list.
+//
+// With fresh reference cells, at least 3 cells per axis and every atom inside
+// [-L/2, L/2], the reference's pair set (atoms of adjacent cells with r2 <
+// Rcut2) is exactly the set of minimum-image pairs with r2 < Rcut2.  The pair
+// kernels then run in a private order (atoms binned on a grid of cells >=
+// Rcut + skin) on a list filtered every step from a skin list (cutoff Rcut +
+// skin).  The order and the skin list are rebuilt, on the device, when an atom
+// has moved more than skin/2 since the last rebuild.  The filter (pair.cu,
+// filter_density) applies the reference's exact FP64 r2 < Rcut2 test,
+// recomputes from the current reference cells which atom of each pair is the
+// reference's "i" (RDF), and accumulates the EAM densities of the kept pairs.
+
+// rebuild flag: 1 if any atom moved more than skin/2 since the last rebuild
+// (minimum image: an atom that VV_NVE1 wrapped across the box has not moved by L)
+__global__ void skin_check_kernel(int n, const double* __restrict__ x, const double* __restrict__ x0, double3 box,
+                                  double3 ibox, double lim2, int* __restrict__ flag) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool need = false;
+    if (i < n) {
+        double dx = x[3 * i] - x0[3 * i], dy = x[3 * i + 1] - x0[3 * i + 1], dz = x[3 * i + 2] - x0[3 * i + 2];
+        dx -= box.x * rint(dx * ibox.x);
+        dy -= box.y * rint(dy * ibox.y);
+        dz -= box.z * rint(dz * ibox.z);
+        need = !(dx * dx + dy * dy + dz * dz <= lim2);
     }
-    if (!c->list_valid) return build_list(c);
+    if (__any_sync(0xffffffffu, need) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+
+// bin on the skin grid and remember the positions of this rebuild
+__global__ void skin_bin_kernel(int n, const double* __restrict__ x, double3 hbox, double3 ilc, int3 nc,
+                                int* __restrict__ cell_of, int* __restrict__ count, double* __restrict__ x0,
+                                const int* __restrict__ cond) {
+    if (*cond == 0) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double xx[3] = {x[3 * i], x[3 * i + 1], x[3 * i + 2]};
+    const double h[3] = {hbox.x, hbox.y, hbox.z}, il[3] = {ilc.x, ilc.y, ilc.z};
+    const int m[3] = {nc.x, nc.y, nc.z};
+    int id[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        int v = (int)floor((xx[d] + h[d]) * il[d]);
+        v = v < 0 ? 0 : (v >= m[d] ? m[d] - 1 : v);
+        id[d] = v;
+        x0[3 * i + d] = xx[d];
+    }
+    const int c = id[0] + id[1] * m[0] + id[2] * m[0] * m[1];
+    cell_of[i] = c;
+    atomicAdd(count + c, 1);
+}
+
+// Choose the pair-kernel order for the current state and gather into it.  In
+// skin mode this also runs the (device-conditional) rebuild of the order and
+// of the skin list.
+static int prepare_order(simox_ctx* c) {
+    const bool skin = c->skin_mode && c->cells_fresh && c->in_box;
+    const int n = c->n;
+    cudaStream_t s = c->stream;
+    if (!skin) {
+        c->pair_order = c->sorted;
+        c->using_skin = false;
+        return gather_sorted(c);
+    }
+    c->pair_order = c->perm;
+    c->using_skin = true;
+    int* flag = c->skin_flag;
+    if (!c->skin_valid) {
+        const int one = 1;
+        cudaMemcpyAsync(flag, &one, sizeof(int), cudaMemcpyHostToDevice, s);
+    } else {
+        cudaMemsetAsync(flag, 0, sizeof(int), s);
+        if (n > 0) {
+            Launch L(c, "skin_check");
+            const double h = 0.5 * c->skin;
+            skin_check_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, c->x, c->x0,
+                                                              make_double3(c->box[0], c->box[1], c->box[2]),
+                                                              make_double3(c->inv_box[0], c->inv_box[1], c->inv_box[2]),
+                                                              h * h, flag);
+        }
+    }
+    // conditional rebuild of the order (binning on the skin grid)
+    cudaMemsetAsync(c->cs_count, 0, sizeof(int) * c->ncell_s, s);
+    if (n > 0) {
+        Launch L(c, "skin_bin");
+        skin_bin_kernel<<<(n + 255) / 256, 256, 0, s>>>(
+            n, c->x, make_double3(c->hbox[0], c->hbox[1], c->hbox[2]),
+            make_double3(1.0 / c->lcs[0], 1.0 / c->lcs[1], 1.0 / c->lcs[2]), make_int3(c->ncs[0], c->ncs[1], c->ncs[2]),
+            c->cs_cell_of, c->cs_count, c->x0, flag);
+    }
+    {
+        Launch L(c, "skin_scan");
+        scan_cells_kernel<<<1, 1024, 0, s>>>(c->cs_count, c->cs_start, c->cs_fill, c->ncell_s, c->npt_max_s, c->status,
+                                             flag);
+    }
+    if (n > 0) {
+        Launch L(c, "skin_scatter");
+        scatter_atoms_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, c->cs_cell_of, c->cs_fill, c->perm, flag);
+    }
+    {
+        Launch L(c, "skin_order");
+        cell_rank_sort_kernel<<<c->ncell_s, 128, sizeof(int) * c->npt_max_s, s>>>(c->cs_start, c->perm, c->npt_max_s,
+                                                                                  flag);
+    }
+    int st = gather_sorted(c);
+    if (st) return st;
+    // conditional skin list build on the new order
+    LBParams P;
+    P.box = make_double3(c->box[0], c->box[1], c->box[2]);
+    P.ibox = make_double3(c->inv_box[0], c->inv_box[1], c->inv_box[2]);
+    P.origin = make_double3(-c->hbox[0], -c->hbox[1], -c->hbox[2]);
+    P.lc = make_double3(c->lcs[0], c->lcs[1], c->lcs[2]);
+    P.nc = make_int3(c->ncs[0], c->ncs[1], c->ncs[2]);
+    const double rs = c->rcut + c->skin;
+    P.rcut2 = rs * rs * (1.0 + 1.0e-4);
+    P.r2lo = P.r2hi = (float)P.rcut2;   // a superset is enough: no exact test here
+    P.hlx = (float)(0.5 * c->lcs[0] + 1.0e-3);
+    P.hly = (float)(0.5 * c->lcs[1] + 1.0e-3);
+    P.hlz = (float)(0.5 * c->lcs[2] + 1.0e-3);
+    P.cap = c->cap_s;
+    P.npt_max = c->npt_max_s;
+    const size_t smem = LB_TILE * (sizeof(float4) + sizeof(unsigned)) + sizeof(int2) * c->npt_max_s;
+    {
+        Launch L(c, "skin_list");
+        build_list_kernel<true><<<c->ncell_s, LB_THREADS, smem, s>>>(
+            c->cs_start, c->cs_entries, c->xq_s, c->t_s, c->nbr_s, reinterpret_cast<int2*>(c->nn_s), P, c->status,
+            c->nn_max, c->nn_tot, flag);
+    }
+    c->skin_valid = true;
+    return check_launch(c);
+}
+
+static int filter_list(simox_ctx* c) {
+    cudaMemsetAsync(c->nn_max, 0, sizeof(int), c->stream);
+    cudaMemsetAsync(c->nn_tot, 0, sizeof(unsigned long long), c->stream);
+    int st = filter_density(c);
+    if (st) return st;
+    c->list_valid = true;
     return SIMOX_OK;
 }
 
+int ensure_gathered(simox_ctx* c) {
+    if (!c->cells_valid) return SIMOX_E_STATE;
+    if (c->gathered) return SIMOX_OK;
+    c->list_valid = false;
+    return prepare_order(c);
+}
+
+int ensure_list(simox_ctx* c) {
+    int st = ensure_gathered(c);
+    if (st) return st;
+    if (c->list_valid) return SIMOX_OK;
+    return c->using_skin ? filter_list(c) : build_list(c);
+}
+
+int setup_skin(simox_ctx* c) {
+    c->skin_mode = false;
+    if (!c->fast_cells || !(c->skin > 0.0)) return SIMOX_OK;
+    const double rs = c->rcut + c->skin;
+    for (int d = 0; d < 3; d++) {
+        c->ncs[d] = (int)(c->box[d] / rs);
+        if (c->ncs[d] < 3) return SIMOX_OK;
+        c->lcs[d] = c->box[d] / (double)c->ncs[d];
+        if (!(0.5 * c->box[d] - rs - 0.5 * c->lcs[d] > 0.01)) return SIMOX_OK;
+    }
+    c->ncell_s = c->ncs[0] * c->ncs[1] * c->ncs[2];
+    const size_t N = (size_t)std::max(c->cap, 1);
+    bool ok = cudaMalloc(&c->cs_count, sizeof(int) * c->ncell_s) == cudaSuccess &&
+              cudaMalloc(&c->cs_start, sizeof(int) * (c->ncell_s + 1)) == cudaSuccess &&
+              cudaMalloc(&c->cs_fill, sizeof(int) * c->ncell_s) == cudaSuccess &&
+              cudaMalloc(&c->cs_cell_of, sizeof(int) * N) == cudaSuccess &&
+              cudaMalloc(&c->cs_entries, sizeof(int) * c->ncell_s * kEntries) == cudaSuccess &&
+              cudaMalloc(&c->perm, sizeof(int) * N) == cudaSuccess &&
+              cudaMalloc(&c->x0, sizeof(double) * 3 * N) == cudaSuccess &&
+              cudaMalloc(&c->skin_flag, sizeof(int)) == cudaSuccess &&
+              cudaMalloc(&c->nn_s, sizeof(int) * 2 * N) == cudaSuccess &&
+              cudaMalloc(&c->nbr_s, sizeof(unsigned) * N * (size_t)c->cap_s) == cudaSuccess;
+    if (!ok) return SIMOX_E_NOMEM;
+    // 27-cell stencil of the skin grid (distinct cells: >= 3 per axis)
+    std::vector<int> E((size_t)c->ncell_s * kEntries);
+    for (int k = 0; k < c->ncs[2]; k++)
+        for (int j = 0; j < c->ncs[1]; j++)
+            for (int i = 0; i < c->ncs[0]; i++) {
+                const int cc = i + c->ncs[0] * (j + c->ncs[1] * k);
+                int e = 0;
+                for (int dk = -1; dk <= 1; dk++)
+                    for (int dj = -1; dj <= 1; dj++)
+                        for (int di = -1; di <= 1; di++) {
+                            const int ii = (i + di + c->ncs[0]) % c->ncs[0];
+                            const int jj = (j + dj + c->ncs[1]) % c->ncs[1];
+                            const int kk = (k + dk + c->ncs[2]) % c->ncs[2];
+                            E[(size_t)cc * kEntries + e++] = ii + c->ncs[0] * (jj + c->ncs[1] * kk);
+                        }
+            }
+    if (cudaMemcpyAsync(c->cs_entries, E.data(), E.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream) !=
+        cudaSuccess)
+        return SIMOX_E_CUDA;
+    c->skin_mode = true;
+    c->skin_valid = false;
+    return cuda_status(cudaStreamSynchronize(c->stream));
+}
+
 int list_prepare(simox_ctx* c) {
-    const int bytes = (int)(LB_TILE * (sizeof(float4) + sizeof(unsigned)) + sizeof(int2) * c->npt_max);
+    // a permission, not a reservation: each launch passes its own size
+    const int bytes = std::max(96 * 1024, (int)(LB_TILE * (sizeof(float4) + sizeof(unsigned)) +
+                                                sizeof(int2) * std::max(c->npt_max, c->npt_max_s)));
     cudaError_t e1 = cudaFuncSetAttribute(build_list_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     cudaError_t e2 = cudaFuncSetAttribute(build_list_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e1 != cudaSuccess || e2 != cudaSuccess) return SIMOX_E_ARG;

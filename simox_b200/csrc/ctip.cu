@@ -478,7 +478,7 @@ int ctip_solve(simox_ctx* c, int max_cg, simox_ctip_report* rep) {
     cudaMemsetAsync(c->acc + A_QSUM, 0, sizeof(double), s);
     {
         Launch L(c, "ctip_final");
-        ctip_final_kernel<<<nb, CT_THREADS, 0, s>>>(n, c->t_s, c->sorted, c->qs, c->q, c->xq_s, S, c->acc);
+        ctip_final_kernel<<<nb, CT_THREADS, 0, s>>>(n, c->t_s, c->pair_order, c->qs, c->q, c->xq_s, S, c->acc);
     }
     cudaMemcpyAsync(c->h_acc, c->acc, sizeof(double) * A_COUNT, cudaMemcpyDeviceToHost, s);
     int s2 = cuda_status(cudaStreamSynchronize(s));

@@ -145,6 +145,8 @@ int vv1(simox_ctx* c, double dt, bool reflect) {
     c->gathered = false;
     c->list_valid = false;
     c->eam_valid = false;
+    c->cells_fresh = false;
+    c->in_box = !reflect;   // VV_NVE1 wraps every coordinate into [-L/2, L/2]
     return check_launch(c);
 }
 

@@ -270,6 +270,145 @@ __global__ void __launch_bounds__(PK_THREADS)
     if (eflag) block_add<PK_THREADS>(egroup, acc, A_EGROUP, red);
 }
 
+// Skin-mode list filter fused with pass 1.  Per atom X, the skin row (cutoff
+// Rcut + skin) is tested with the reference's exact FP64 r2 < Rcut2
+// (force.f90:51-54); kept partners are written, compacted with a warp ballot,
+// to the exact row (same species grouping) with bit 31 = "X is the
+// reference's i" (X's cell is home and Y's cell one of the 13 CELL_HIERARCHY
+// cells, or same cell and lower atom index), and their density terms are
+// summed into rho_X; the embedding follows as in density_kernel.
+struct FilterParams {
+    PairParams pp;
+    double rcut2;
+    int3 nc;                 // reference cell grid
+    int cap_s;
+};
+
+__device__ __forceinline__ int wrap_off(int d, int n) { return d > 1 ? d - n : (d < -1 ? d + n : d); }
+
+template <typename R>
+__global__ void __launch_bounds__(256)
+    filter_density_kernel(FilterParams F, const PairTab<R>* __restrict__ tab, const double4* __restrict__ xq,
+                          const int* __restrict__ ts, const int* __restrict__ cx_s, const int* __restrict__ order,
+                          const int2* __restrict__ nn_s, const unsigned* __restrict__ nbr_s, int2* __restrict__ nn,
+                          unsigned* __restrict__ nbr, EmbedParams E, double* __restrict__ rho_s,
+                          double* __restrict__ dF_s, float* __restrict__ dF_f, int* __restrict__ status,
+                          int* __restrict__ nn_max, unsigned long long* __restrict__ nn_tot) {
+    __shared__ PairTab<R> st[kSpecies * kSpecies];
+    for (int k = threadIdx.x; k < kSpecies * kSpecies; k += blockDim.x) st[k] = tab[k];
+    __syncthreads();
+    const PairParams& P = F.pp;
+    const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    int lmax = 0, bad = 0;
+    unsigned long long ltot = 0;
+    for (int X = blockIdx.x * wpb + (threadIdx.x >> 5); X < P.n; X += gridDim.x * wpb) {
+        const double4 xa = xq[X];
+        const int sX = ts[X];
+        const int cX = cx_s[X];
+        const int2 ms = nn_s[X];
+        const unsigned* srow = nbr_s + (size_t)X * F.cap_s;
+        unsigned* row = nbr + (size_t)X * P.cap;
+        int out[2] = {0, 0};
+        double rho = 0.0;
+        for (int g = 0; g < 2; g++) {
+            const int mg = g == 0 ? ms.x : ms.y;
+            // pipelined: entry, position and cell of the next 32-slot batch
+            unsigned Yn = 0;
+            double4 xbn = make_double4(0, 0, 0, 0);
+            int cYn = 0;
+            if (lane < mg) {
+                Yn = srow[g == 0 ? lane : F.cap_s - 1 - lane] & kIdxMask;
+                xbn = xq[Yn];
+                cYn = cx_s[Yn];
+            }
+            for (int base = 0; base < mg; base += 32) {
+                const int k = base + lane;
+                const unsigned Y = Yn;
+                const double4 xb = xbn;
+                const int cY = cYn;
+                if (k + 32 < mg) {
+                    Yn = srow[g == 0 ? k + 32 : F.cap_s - 1 - (k + 32)] & kIdxMask;
+                    xbn = xq[Yn];
+                    cYn = cx_s[Yn];
+                }
+                bool acc = false;
+                double r2d = 0.0;
+                if (k < mg) {
+                    double dx, dy, dz;
+                    min_image(xa, xb, P, dx, dy, dz);
+                    r2d = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+                    acc = r2d < F.rcut2;
+                }
+                const unsigned mask = __ballot_sync(0xffffffffu, acc);
+                if (acc) {
+                    unsigned isa;
+                    if (cY == cX) {
+                        isa = order[X] < order[Y];
+                    } else {
+                        const int ox = wrap_off((cY & 1023) - (cX & 1023), F.nc.x);
+                        const int oy = wrap_off(((cY >> 10) & 1023) - ((cX >> 10) & 1023), F.nc.y);
+                        const int oz = wrap_off((cY >> 20) - (cX >> 20), F.nc.z);
+                        // the 13 forward cells of CELL_HIERARCHY (cellsort.f90:18-30)
+                        isa = oz == -1 || (oz == 0 && (oy == -1 || (oy == 0 && ox == -1)));
+                    }
+                    const int pos = out[g] + __popc(mask & lt);
+                    const int slot = g == 0 ? pos : P.cap - 1 - pos;
+                    if (g == 0 ? pos < P.cap : slot >= out[0]) row[slot] = Y | (isa << 31);
+                    // density of Y at X (force.f90:84-85)
+                    const int sY = g == 1 ? 3 : ts[Y];
+                    if (sX < kSpecies && sY < kSpecies) {
+                        const PairTab<R>& T = st[sX * kSpecies + sY];
+                        if (!T.valid) bad |= ST_UNSUPPORTED;
+                        const R r = sqrt((R)r2d);
+                        rho += (double)(T.d_fe * zhou_val<R>(r, T.d_inv_re, T.d_c, T.d_lam));
+                    } else {
+                        bad |= ST_UNKNOWN_PAIR;
+                    }
+                }
+                out[g] += __popc(mask);
+            }
+        }
+        rho = warp_sum(rho);
+        if (lane == 0) {
+            const int tot = out[0] + out[1];
+            if (tot > P.cap) {
+                atomicOr(status, ST_NBR_OVERFLOW);
+                nn[X] = make_int2(0, 0);
+            } else {
+                nn[X] = make_int2(out[0], out[1]);
+            }
+            lmax = max(lmax, tot);
+            ltot += (unsigned long long)tot;
+            double Fe, dF;
+            if (embed(E, sX, rho, Fe, dF)) bad |= ST_UNKNOWN_ELEMENT;
+            rho_s[X] = rho;
+            dF_s[X] = dF;
+            dF_f[X] = (float)dF;
+        }
+    }
+    if (bad) atomicOr(status, bad);
+    if (lane == 0) {
+        if (lmax) atomicMax(nn_max, lmax);
+        if (ltot) atomicAdd(nn_tot, ltot);
+    }
+}
+
+// Egroup = sum_X F(rho_X) from stored densities (energy steps after a fused pass)
+__global__ void __launch_bounds__(256)
+    embed_energy_kernel(int n, const int* __restrict__ ts, const double* __restrict__ rho_s, EmbedParams E,
+                        double* __restrict__ acc) {
+    __shared__ double red[256 / 32];
+    double eg = 0.0;
+    const int X = blockIdx.x * blockDim.x + threadIdx.x;
+    if (X < n) {
+        double Fe, dF;
+        embed(E, ts[X], rho_s[X], Fe, dF);
+        eg = Fe;
+    }
+    block_add<256>(eg, acc, A_EGROUP, red);
+}
+
 // One pair's scalar force f/r on X (force.f90:81-98, 135-138), specialised on
 //   SAME : the partner has X's species (one density function, one CTIP exponential)
 //   MHOMO: same-species metals, whose pair B-term is the density shape (METAL_HOMO)
@@ -518,6 +657,15 @@ int eam_density(simox_ctx* c, bool eflag) {
     if (c->n == 0) return SIMOX_OK;
     PairParams P = pair_params(c);
     EmbedParams E = embed_params(c->pot);
+    // the skin filter already produced rho and F' in the context's precision
+    if (c->rho_ready && use_fp64(c, eflag) == (c->precision == SIMOX_FP64)) {
+        if (eflag) {
+            Launch L(c, "eam_embed_energy");
+            embed_energy_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->n, c->t_s, c->rho_s, E, c->acc);
+        }
+        c->eam_valid = true;
+        return check_launch(c);
+    }
     Launch L(c, use_fp64(c, eflag) ? "eam_density_fp64" : "eam_density");
     if (!use_fp64(c, eflag))
         density_kernel<float><<<pair_grid(c), PK_THREADS, 0, c->stream>>>(P, c->tab_f, c->xq_s, c->t_s,
@@ -529,7 +677,33 @@ int eam_density(simox_ctx* c, bool eflag) {
                                                                           E, c->rho_s, c->dF_s, c->dF_f, c->acc,
                                                                           c->status, eflag);
     c->eam_valid = true;
+    c->rho_ready = false;   // rho/F' now in the precision of this pass
     return check_launch(c);
+}
+
+int filter_density(simox_ctx* c) {
+    FilterParams F;
+    F.pp = pair_params(c);
+    F.rcut2 = c->rcut2;
+    F.nc = make_int3(c->nc[0], c->nc[1], c->nc[2]);
+    F.cap_s = c->cap_s;
+    EmbedParams E = embed_params(c->pot);
+    if (c->n > 0) {
+        Launch L(c, "neighbor_filter_density");
+        const int g = std::min((c->n + 7) / 8, num_sms(c) * 8);
+        if (c->precision == SIMOX_FP64)
+            filter_density_kernel<double><<<g, 256, 0, c->stream>>>(
+                F, c->tab_d, c->xq_s, c->t_s, c->cx_s, c->pair_order, reinterpret_cast<const int2*>(c->nn_s), c->nbr_s,
+                reinterpret_cast<int2*>(c->nn), c->nbr, E, c->rho_s, c->dF_s, c->dF_f, c->status, c->nn_max, c->nn_tot);
+        else
+            filter_density_kernel<float><<<g, 256, 0, c->stream>>>(
+                F, c->tab_f, c->xq_s, c->t_s, c->cx_s, c->pair_order, reinterpret_cast<const int2*>(c->nn_s), c->nbr_s,
+                reinterpret_cast<int2*>(c->nn), c->nbr, E, c->rho_s, c->dF_s, c->dF_f, c->status, c->nn_max, c->nn_tot);
+    }
+    int st = check_launch(c);
+    if (st) return st;
+    c->rho_ready = true;
+    return SIMOX_OK;
 }
 
 template <typename R>
@@ -541,16 +715,16 @@ static void launch_force(simox_ctx* c, const PairTab<R>* tab, bool eflag, bool r
     if (g < 1) g = 1;
     if (eflag && rdf)
         force_kernel<R, true, true><<<g, PK_THREADS, 0, c->stream>>>(P, tab, c->xq_s, c->t_s, reinterpret_cast<const int2*>(c->nn), c->nbr, c->dF_s, c->dF_f,
-                                                                     c->sorted, c->f, c->acc, c->rdf, c->status);
+                                                                     c->pair_order, c->f, c->acc, c->rdf, c->status);
     else if (eflag)
         force_kernel<R, true, false><<<g, PK_THREADS, 0, c->stream>>>(P, tab, c->xq_s, c->t_s, reinterpret_cast<const int2*>(c->nn), c->nbr, c->dF_s, c->dF_f,
-                                                                      c->sorted, c->f, c->acc, c->rdf, c->status);
+                                                                      c->pair_order, c->f, c->acc, c->rdf, c->status);
     else if (rdf)
         force_kernel<R, false, true><<<g, PK_THREADS, 0, c->stream>>>(P, tab, c->xq_s, c->t_s, reinterpret_cast<const int2*>(c->nn), c->nbr, c->dF_s, c->dF_f,
-                                                                      c->sorted, c->f, c->acc, c->rdf, c->status);
+                                                                      c->pair_order, c->f, c->acc, c->rdf, c->status);
     else
         force_kernel<R, false, false><<<g, PK_THREADS, 0, c->stream>>>(P, tab, c->xq_s, c->t_s, reinterpret_cast<const int2*>(c->nn), c->nbr, c->dF_s, c->dF_f,
-                                                                       c->sorted, c->f, c->acc, c->rdf, c->status);
+                                                                       c->pair_order, c->f, c->acc, c->rdf, c->status);
 }
 
 int pair_forces(simox_ctx* c, bool eflag, bool rdf) {

@@ -458,7 +458,7 @@ static int pme_forces_t(simox_ctx* c, PmeRes& Rs, bool eflag) {
     int st = run_convolution(c, Rs, eflag);
     if (st) return st;
     Launch L(c, "pme_gather_force");
-    gather_force_kernel<R, P><<<(S.n + 127) / 128, 128, 0, c->stream>>>(S, c->xq_s, (const R*)Rs.grid, c->sorted,
+    gather_force_kernel<R, P><<<(S.n + 127) / 128, 128, 0, c->stream>>>(S, c->xq_s, (const R*)Rs.grid, c->pair_order,
                                                                         c->f, c->acc);
     return SIMOX_OK;
 }
@@ -493,10 +493,7 @@ int pme_finalize_forces(simox_ctx* c) {
 
 int pme_forces(simox_ctx* c, bool finalize, bool eflag) {
     if (!c->psi_valid) return SIMOX_E_STATE;
-    if (!c->gathered) {
-        int st = gather_sorted(c);
-        if (st) return st;
-    }
+    if (int st0 = ensure_gathered(c)) return st0;
     if (c->n == 0) return SIMOX_OK;
     cudaMemsetAsync(c->acc + A_FSUM0, 0, 3 * sizeof(double), c->stream);
     int st;

@@ -111,6 +111,7 @@ struct simox_ctx {
 
     // cells
     int* cell_of = nullptr;     // [cap]
+    int* cell_xyz = nullptr;    // [cap] packed cell coordinates x | y<<10 | z<<20
     int* cell_count = nullptr;  // [ncell]
     int* cell_start = nullptr;  // [ncell+1]
     int* cell_fill = nullptr;   // [ncell]
@@ -119,9 +120,33 @@ struct simox_ctx {
     int* entries = nullptr;     // [ncell*27] cell | dir<<28
     std::vector<int> h_pair13;
 
+    // pair-kernel order: the reference cell order (sorted) or, in skin mode,
+    // the skin-grid order (perm) that persists between skin-list rebuilds
+    int* pair_order = nullptr;
+    bool skin_mode = false;     // the box admits the skin list
+    bool skin_valid = false;    // perm / x0 / skin list belong to this atom set
+    bool using_skin = false;    // the current order is the skin order
+    bool cells_fresh = false;   // reference cells binned after the last move
+    bool in_box = false;        // every coordinate in [-L/2, L/2]
+    double skin = 1.0;
+    int ncs[3]{}, ncell_s = 0, npt_max_s = 1024, cap_s = 2048;
+    double lcs[3]{};
+    int* cs_count = nullptr;
+    int* cs_start = nullptr;
+    int* cs_fill = nullptr;
+    int* cs_cell_of = nullptr;
+    int* cs_entries = nullptr;
+    int* perm = nullptr;
+    double* x0 = nullptr;       // positions at the last skin rebuild (original order)
+    int* skin_flag = nullptr;   // device: rebuild needed
+    int* nn_s = nullptr;        // skin list counts (int2)
+    unsigned* nbr_s = nullptr;  // skin list rows [cap*cap_s]
+
     // sorted copies
     double4* xq_s = nullptr;    // x, y, z, q
     int* t_s = nullptr;         // species 0..4
+    int* cx_s = nullptr;        // packed reference-cell coordinates in pair order
+    bool rho_ready = false;     // rho/F' of the filter pass are current (context precision)
 
     // neighbour list
     int* nn = nullptr;          // [cap] int2: (metal partners, oxygen partners)
@@ -206,9 +231,12 @@ int cell_sort(simox_ctx* c);
 int gather_sorted(simox_ctx* c);
 int build_list(simox_ctx* c);
 int ensure_list(simox_ctx* c);
+int ensure_gathered(simox_ctx* c);
+int setup_skin(simox_ctx* c);
 // pair.cu
 int build_pair_tables(simox_ctx* c);
 int eam_density(simox_ctx* c, bool eflag);
+int filter_density(simox_ctx* c);
 int pair_forces(simox_ctx* c, bool eflag, bool rdf);
 // pme.cu
 int pme_setup(simox_ctx* c);

@@ -202,6 +202,67 @@ def test_md_steps_fp64_vs_oracle():
     assert abs(e["Erec"] - erec_o) <= 1e-8 * abs(erec_o)
 
 
+SKIN_BOX = dict(seed=21, n=1900, box=(36.5, 37.0, 38.0), fft=(32, 32, 32), order=6)
+
+
+@pytest.mark.parametrize("skin", [1.0, 0.05, -1.0])
+def test_md_skin_list_vs_oracle(skin):
+    """Five NVT steps in a box large enough for the Verlet skin list (3 skin
+    cells per axis).  skin 1.0: one list for all steps; 0.05: rebuilt every
+    few steps; -1: rebuilt from the reference cells every step.  Positions,
+    velocities, the last step's energies and the RDF must follow the oracle."""
+    s = S.small_alo(**SKIN_BOX)
+    dt = 1.0 / S.TFM
+    T = 600.0 * S.KB
+    o = oracle_system(s)
+    o.pme_self()
+    o.cell_sort()
+    f, *_ = o.force()
+    f, _ = o.pme(f)
+    v = s.v.copy()
+    rdf_o = np.zeros(_abi.RDF_LEN, np.int32)
+    for step in range(1, 6):
+        v = o.vv_nve1(v, f, dt)
+        o.cell_sort()
+        f, e_o, _, _, h = o.force(rdf=True)
+        rdf_o += h
+        f, erec_o = o.pme(f)
+        v, mv2_o = o.vv_nvt2_berend(v, f, dt, T)
+    rdf = np.zeros(_abi.RDF_LEN, np.int32)
+    with gpu_context(s, skin=skin) as g:
+        g.pme_self()
+        g.cell_sort()
+        g.force()
+        g.pme()
+        e = g.md_run(5, dt, first_step=1, thermostat=True, T_given=T, freq_new=0, freq_sort=1, rdf=rdf)
+        st = g.get_state()
+        npt, link = g.get_cells(link_stride=500)
+    assert np.abs(st["x"] - o.x).max() <= 1e-10
+    assert np.abs(st["v"] - v).max() <= 1e-9 * np.abs(v).max()
+    assert np.abs(st["f"] - f).max() <= 1e-8 * np.abs(f).max()
+    for k in ("Epair", "Edir", "Ectip", "Egroup"):
+        assert abs(e[k] - e_o[k]) <= 1e-9 * max(1.0, abs(e_o[k])), k
+    assert abs(e["Erec"] - erec_o) <= 1e-8 * abs(erec_o)
+    assert np.array_equal(rdf, rdf_o)
+    npt_o, link_o = o.cells
+    assert np.array_equal(npt, npt_o)
+
+
+def test_md_skin_mixed_matches_fp64():
+    """Mixed precision with the skin list: forces within 1e-5 of FP64."""
+    s = S.small_alo(**SKIN_BOX)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        with gpu_context(s, precision=prec) as g:
+            g.pme_self()
+            g.cell_sort()
+            g.force(energies=False)
+            g.pme(energies=False)
+            g.md_run(4, 1.0 / S.TFM, first_step=2, thermostat=True, T_given=600 * S.KB, freq_new=0, freq_stat=1000)
+            out[prec] = g.get_state()["f"]
+    assert rel_err(out["mixed"], out["fp64"]) <= 1e-5
+
+
 def test_status_codes():
     """Limit breaches come back as the reference's STOP texts, not faults."""
     from simox_b200.api import SimoxError
