@@ -251,7 +251,7 @@ static void free_ctx(simox_ctx* c) {
     prof_collect(c);
     pme_free(c);
     void* bufs[] = {c->id, c->x, c->v, c->f, c->q, c->xm, c->cell_of, c->cell_xyz, c->cell_count, c->cell_start, c->cell_fill,
-                    c->sorted, c->pair13, c->entries, c->xq_s, c->t_s, c->cx_s, c->nn, c->nbr, c->nn_max, c->nn_tot,
+                    c->sorted, c->pair13, c->entries, c->xq_s, c->t_s, c->rec_s, c->frec_s, c->nn, c->nbr, c->nn_max, c->nn_tot,
                     c->cs_count, c->cs_start, c->cs_fill, c->cs_cell_of, c->cs_entries, c->perm, c->x0,
                     c->skin_flag, c->nn_s, c->nbr_s, c->rho_s, c->dF_s, c->dF_f, c->tab_d, c->tab_f, c->c_const, c->g, c->pv, c->Ap, c->qs, c->jp,
                     c->act, c->line, c->acc, c->status, c->rdf};
@@ -295,6 +295,10 @@ extern "C" int simox_create(const simox_setup* s, const simox_potential* pot, si
     else simox_default_potential(&c->pot);
     c->n = s->n_atoms;
     c->cap = std::max(s->capacity, s->n_atoms);
+    if ((size_t)c->cap > (size_t)sx::kIdxMask) {   // list entries hold 26-bit atom indices
+        delete c;
+        return SIMOX_E_CAPACITY;
+    }
     c->precision = s->precision;
     c->flags = s->flags;
     c->order = order;
@@ -337,7 +341,7 @@ extern "C" int simox_create(const simox_setup* s, const simox_potential* pot, si
               dalloc(&c->q, N) && dalloc(&c->cell_of, N) && dalloc(&c->cell_xyz, N) && dalloc(&c->cell_count, c->ncell) &&
               dalloc(&c->cell_start, c->ncell + 1) && dalloc(&c->cell_fill, c->ncell) && dalloc(&c->sorted, N) &&
               dalloc(&c->pair13, (size_t)c->ncell * 13) && dalloc(&c->entries, (size_t)c->ncell * kEntries) &&
-              dalloc(&c->xq_s, N) && dalloc(&c->t_s, N) && dalloc(&c->cx_s, N) && dalloc(&c->nn, 2 * N) &&
+              dalloc(&c->xq_s, N) && dalloc(&c->t_s, N) && dalloc(&c->rec_s, N) && dalloc(&c->frec_s, N) && dalloc(&c->nn, 2 * N) &&
               dalloc(&c->nbr, N * (size_t)c->nnb_cap) && dalloc(&c->nn_max, 1) && dalloc(&c->nn_tot, 1) &&
               dalloc(&c->rho_s, N) && dalloc(&c->dF_s, N) && dalloc(&c->dF_f, N) && dalloc(&c->tab_d, kSpecies * kSpecies) &&
               dalloc(&c->tab_f, kSpecies * kSpecies) && dalloc(&c->line, 64) && dalloc(&c->acc, A_COUNT) &&
@@ -382,11 +386,14 @@ extern "C" int simox_set_state(simox_ctx* c, int n, const int* id, const double*
     cudaStream_t s = c->stream;
     if (id) {
         bool has_h = false;
+        int g0 = -1;   // species of the non-oxygen atoms: one (>= 0), several (-2) or none (-1)
         for (int i = 0; i < n; i++) {
             if (id[i] < 1 || id[i] > SIMOX_NATOM) return SIMOX_E_ARG;
             has_h |= id[i] == 5;
+            if (id[i] != 4) g0 = (g0 == -1 || g0 == id[i] - 1) ? id[i] - 1 : -2;
         }
         c->has_h = has_h;
+        c->g0_species = g0 >= 0 && g0 < 3 ? g0 : -1;
         cudaMemcpyAsync(c->id, id, sizeof(int) * n, cudaMemcpyHostToDevice, s);
         c->have_ids = true;
     }

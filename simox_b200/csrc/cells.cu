@@ -195,24 +195,61 @@ int cell_sort(simox_ctx* c) {
 
 // ---------------------------------------------------------------------------
 // gather original-order state into cell order
+// Skin-mode records of each atom (pair order): its offset from the centre
+// of the skin cell it was binned into at the last rebuild (minimum image,
+// FP32), with w = reference cell (9 bits per axis) | species << 27 for the
+// list filter and w = charge for the force pass.
+// For a skin pair (X, Y) with stencil offset o, x_Y - x_X = off_Y - off_X +
+// o * Lcs exactly while both atoms stay within skin/2 of their rebuild
+// positions.
+struct RecParams {
+    double3 box, ibox, origin, lc;
+    int3 ncs;
+};
+
 __global__ void gather_sorted_kernel(int n, const int* __restrict__ sorted, const double* __restrict__ x,
                                      const double* __restrict__ q, const int* __restrict__ id,
-                                     const int* __restrict__ cell_xyz, double4* __restrict__ xq,
-                                     int* __restrict__ ts, int* __restrict__ cx) {
+                                     double4* __restrict__ xq, int* __restrict__ ts, const int* __restrict__ cell_xyz,
+                                     const int* __restrict__ cs_cell_of, RecParams R, float4* __restrict__ rec,
+                                     float4* __restrict__ frec) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     int o = sorted[k];
-    xq[k] = make_double4(x[3 * o], x[3 * o + 1], x[3 * o + 2], q[o]);
-    ts[k] = id[o] - 1;
-    cx[k] = cell_xyz[o];
+    const double x0 = x[3 * o], x1 = x[3 * o + 1], x2 = x[3 * o + 2];
+    const int t = id[o] - 1;
+    xq[k] = make_double4(x0, x1, x2, q[o]);
+    ts[k] = t;
+    if (rec) {
+        const int cs = cs_cell_of[o];
+        const int ci = cs % R.ncs.x, cj = (cs / R.ncs.x) % R.ncs.y, ck = cs / (R.ncs.x * R.ncs.y);
+        double ox = x0 - (R.origin.x + (ci + 0.5) * R.lc.x);
+        double oy = x1 - (R.origin.y + (cj + 0.5) * R.lc.y);
+        double oz = x2 - (R.origin.z + (ck + 0.5) * R.lc.z);
+        ox -= R.box.x * rint(ox * R.ibox.x);
+        oy -= R.box.y * rint(oy * R.ibox.y);
+        oz -= R.box.z * rint(oz * R.ibox.z);
+        const unsigned cx = (unsigned)cell_xyz[o];
+        const unsigned sp = (unsigned)t < (unsigned)kSpecies ? (unsigned)t : 7u;
+        const unsigned w = (cx & 511u) | (((cx >> 10) & 511u) << 9) | (((cx >> 20) & 511u) << 18) | (sp << 27);
+        rec[k] = make_float4((float)ox, (float)oy, (float)oz, __uint_as_float(w));
+        frec[k] = make_float4((float)ox, (float)oy, (float)oz, (float)q[o]);
+    }
 }
 
 int gather_sorted(simox_ctx* c) {
     if (!c->cells_valid) return SIMOX_E_STATE;
     if (c->n > 0) {
         Launch L(c, "gather_sorted");
-        gather_sorted_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->n, c->pair_order, c->x, c->q, c->id,
-                                                                        c->cell_xyz, c->xq_s, c->t_s, c->cx_s);
+        RecParams R;
+        R.box = make_double3(c->box[0], c->box[1], c->box[2]);
+        R.ibox = make_double3(c->inv_box[0], c->inv_box[1], c->inv_box[2]);
+        R.origin = make_double3(-c->hbox[0], -c->hbox[1], -c->hbox[2]);
+        R.lc = make_double3(c->lcs[0], c->lcs[1], c->lcs[2]);
+        R.ncs = make_int3(c->ncs[0], c->ncs[1], c->ncs[2]);
+        const bool skin = c->pair_order == c->perm && c->skin_mode;
+        gather_sorted_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(
+            c->n, c->pair_order, c->x, c->q, c->id, c->xq_s, c->t_s, c->cell_xyz, c->cs_cell_of, R,
+            skin ? c->rec_s : nullptr, c->frec_s);
     }
     c->gathered = true;
     c->rho_ready = false;
@@ -233,6 +270,7 @@ struct LBParams {
     double rcut2;
     float r2lo, r2hi, hlx, hly, hlz;
     int cap, npt_max;
+    int skin;   // skin list: entries carry the stencil code instead of "is i"
 };
 
 // reference r2 (force.f90:51-53): rx = dx - box*DNINT(dx/box), no FMA
@@ -244,13 +282,13 @@ __device__ __forceinline__ double exact_r2(double4 a, double4 b, double3 box) {
     return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
 }
 
-__device__ __forceinline__ void list_append(unsigned* row, int2& my, int cap, unsigned j, unsigned isa, int sp) {
+__device__ __forceinline__ void list_append(unsigned* row, int2& my, int cap, unsigned val, int sp) {
     const int used = my.x + my.y;
     if (sp == 3) {
-        if (used < cap) row[cap - 1 - my.y] = j | (isa << 31);
+        if (used < cap) row[cap - 1 - my.y] = val;
         my.y++;
     } else {
-        if (used < cap) row[my.x] = j | (isa << 31);
+        if (used < cap) row[my.x] = val;
         my.x++;
     }
 }
@@ -315,7 +353,8 @@ __global__ void __launch_bounds__(LB_THREADS)
             ry -= P.box.y * rint(ry * P.ibox.y);
             rz -= P.box.z * rint(rz * P.ibox.z);
             cpos[k] = make_float4((float)rx, (float)ry, (float)rz, __int_as_float(ts[j]));
-            ctag[k] = (unsigned)j | ((unsigned)edir[e] << 30);
+            // exact list: j | dir << 30; skin list: j | stencil position << 26
+            ctag[k] = P.skin ? (unsigned)j | ((unsigned)e << kSkinCodeShift) : (unsigned)j | ((unsigned)edir[e] << 30);
         }
         __syncthreads();
         for (int hl = tid; hl < nh; hl += blockDim.x) {
@@ -333,25 +372,26 @@ __global__ void __launch_bounds__(LB_THREADS)
                     const float r2 = dx * dx + dy * dy + dz * dz;
                     if (r2 < P.r2hi) {
                         const unsigned tag = ctag[k];
-                        const int j = (int)(tag & 0x3fffffffu);
+                        const int j = (int)(tag & (P.skin ? kSkinIdxMask : 0x3fffffffu));
                         bool acc = r2 < P.r2lo;
                         if (!acc) acc = exact_r2(xh, xq[j], P.box) < P.rcut2;
                         if (acc && j != h) {
                             const unsigned dir = tag >> 30;
                             const unsigned isa = dir == 0 ? (unsigned)(h < j) : (unsigned)(dir == 1);
-                            list_append(row, my, P.cap, (unsigned)j, isa, __float_as_int(cp.w));
+                            list_append(row, my, P.cap, P.skin ? tag : (unsigned)j | (isa << 31), __float_as_int(cp.w));
                         }
                     }
                 }
             } else {
                 for (int k = 0; k < tn; k++) {
                     const unsigned tag = ctag[k];
-                    const int j = (int)(tag & 0x3fffffffu);
+                    const int j = (int)(tag & (P.skin ? kSkinIdxMask : 0x3fffffffu));
                     if (j == h) continue;
                     if (exact_r2(xh, xq[j], P.box) < P.rcut2) {
                         const unsigned dir = tag >> 30;
                         const unsigned isa = dir == 0 ? (unsigned)(h < j) : (unsigned)(dir == 1);
-                        list_append(row, my, P.cap, (unsigned)j, isa, __float_as_int(cpos[k].w));
+                        list_append(row, my, P.cap, P.skin ? tag : (unsigned)j | (isa << 31),
+                                    __float_as_int(cpos[k].w));
                     }
                 }
             }
@@ -388,6 +428,7 @@ int build_list(simox_ctx* c) {
     P.box = make_double3(c->box[0], c->box[1], c->box[2]);
     P.ibox = make_double3(c->inv_box[0], c->inv_box[1], c->inv_box[2]);
     P.origin = make_double3(-c->hbox[0], -c->hbox[1], -c->hbox[2]);
+    P.skin = 0;
     P.lc = make_double3(c->lc[0], c->lc[1], c->lc[2]);
     P.nc = make_int3(c->nc[0], c->nc[1], c->nc[2]);
     P.rcut2 = c->rcut2;
@@ -538,6 +579,7 @@ static int prepare_order(simox_ctx* c) {
     P.hlz = (float)(0.5 * c->lcs[2] + 1.0e-3);
     P.cap = c->cap_s;
     P.npt_max = c->npt_max_s;
+    P.skin = 1;
     const size_t smem = LB_TILE * (sizeof(float4) + sizeof(unsigned)) + sizeof(int2) * c->npt_max_s;
     {
         Launch L(c, "skin_list");
@@ -576,11 +618,17 @@ int setup_skin(simox_ctx* c) {
     c->skin_mode = false;
     if (!c->fast_cells || !(c->skin > 0.0)) return SIMOX_OK;
     const double rs = c->rcut + c->skin;
+    // filter records: reference cells packed in 9 bits per axis, atom index
+    // below the stencil code bits of a skin entry
+    if ((size_t)c->cap > (size_t)kSkinIdxMask) return SIMOX_OK;
     for (int d = 0; d < 3; d++) {
+        if (c->nc[d] > 511) return SIMOX_OK;
         c->ncs[d] = (int)(c->box[d] / rs);
         if (c->ncs[d] < 3) return SIMOX_OK;
         c->lcs[d] = c->box[d] / (double)c->ncs[d];
         if (!(0.5 * c->box[d] - rs - 0.5 * c->lcs[d] > 0.01)) return SIMOX_OK;
+        // a listed pair stays closer than L/2 until the next rebuild
+        if (!(0.5 * c->box[d] - 1.0001 * rs - c->skin > 0.01)) return SIMOX_OK;
     }
     c->ncell_s = c->ncs[0] * c->ncs[1] * c->ncs[2];
     const size_t N = (size_t)std::max(c->cap, 1);

@@ -324,7 +324,8 @@ __global__ void __launch_bounds__(CT_THREADS)
 // write charges back (original order and the sorted copy); Eself pieces (ctip.f90:194-209)
 __global__ void __launch_bounds__(CT_THREADS)
     ctip_final_kernel(int n, const int* __restrict__ ts, const int* __restrict__ sorted, const double* __restrict__ qs,
-                      double* __restrict__ q, double4* __restrict__ xq, CtipSpecies S, double* __restrict__ acc) {
+                      double* __restrict__ q, double4* __restrict__ xq, float4* __restrict__ frec, CtipSpecies S,
+                      double* __restrict__ acc) {
     __shared__ double red[CT_THREADS / 32];
     double q2 = 0.0, es = 0.0, qsum = 0.0;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -333,6 +334,7 @@ __global__ void __launch_bounds__(CT_THREADS)
         const double qi = qs[i];
         q[sorted[i]] = qi;
         xq[i].w = qi;
+        frec[i].w = (float)qi;   // skin-mode force record (unused otherwise)
         q2 = -(qi * qi);
         qsum = qi;
         es = S.chi[s] * qi + 0.5 * S.Jp[s] * (qi * qi);
@@ -478,7 +480,8 @@ int ctip_solve(simox_ctx* c, int max_cg, simox_ctip_report* rep) {
     cudaMemsetAsync(c->acc + A_QSUM, 0, sizeof(double), s);
     {
         Launch L(c, "ctip_final");
-        ctip_final_kernel<<<nb, CT_THREADS, 0, s>>>(n, c->t_s, c->pair_order, c->qs, c->q, c->xq_s, S, c->acc);
+        ctip_final_kernel<<<nb, CT_THREADS, 0, s>>>(n, c->t_s, c->pair_order, c->qs, c->q, c->xq_s, c->frec_s, S,
+                                                              c->acc);
     }
     cudaMemcpyAsync(c->h_acc, c->acc, sizeof(double) * A_COUNT, cudaMemcpyDeviceToHost, s);
     int s2 = cuda_status(cudaStreamSynchronize(s));

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 
 namespace sx {
 
@@ -271,31 +272,57 @@ __global__ void __launch_bounds__(PK_THREADS)
 }
 
 // Skin-mode list filter fused with pass 1.  Per atom X, the skin row (cutoff
-// Rcut + skin) is tested with the reference's exact FP64 r2 < Rcut2
+// Rcut + skin) is tested against the reference's FP64 r2 < Rcut2
 // (force.f90:51-54); kept partners are written, compacted with a warp ballot,
-// to the exact row (same species grouping) with bit 31 = "X is the
-// reference's i" (X's cell is home and Y's cell one of the 13 CELL_HIERARCHY
-// cells, or same cell and lower atom index), and their density terms are
+// to the exact row (same species grouping, stencil position kept) with bit
+// 31 = "X is the reference's i" (Y's reference cell is one of the 13
+// CELL_HIERARCHY cells of X's, or the same cell and X comes first), and their density terms are
 // summed into rho_X; the embedding follows as in density_kernel.
+//
+// FP32 contexts decide membership from the 16-byte filter records: r2 from
+// off_Y - off_X + o*Lcs in FP32, and only pairs whose FP32 r2 lies within the
+// rounding bound `band` of Rcut^2 are re-tested with the FP64 positions.  FP64
+// contexts test every pair in FP64.
 struct FilterParams {
     PairParams pp;
     double rcut2;
-    int3 nc;                 // reference cell grid
+    float rcut2f, band;
+    int3 nc;                 // reference cell grid (>= 3 per axis)
     int cap_s;
+    float4 sh[kEntries];     // stencil position -> o * Lcs
 };
-
-__device__ __forceinline__ int wrap_off(int d, int n) { return d > 1 ? d - n : (d < -1 ? d + n : d); }
 
 template <typename R>
 __global__ void __launch_bounds__(256)
     filter_density_kernel(FilterParams F, const PairTab<R>* __restrict__ tab, const double4* __restrict__ xq,
-                          const int* __restrict__ ts, const int* __restrict__ cx_s, const int* __restrict__ order,
+                          const float4* __restrict__ rec, const int* __restrict__ order,
                           const int2* __restrict__ nn_s, const unsigned* __restrict__ nbr_s, int2* __restrict__ nn,
                           unsigned* __restrict__ nbr, EmbedParams E, double* __restrict__ rho_s,
                           double* __restrict__ dF_s, float* __restrict__ dF_f, int* __restrict__ status,
                           int* __restrict__ nn_max, unsigned long long* __restrict__ nn_tot) {
-    __shared__ PairTab<R> st[kSpecies * kSpecies];
-    for (int k = threadIdx.x; k < kSpecies * kSpecies; k += blockDim.x) st[k] = tab[k];
+    constexpr bool F32 = std::is_same<R, float>::value;
+    using R4 = typename std::conditional<F32, float4, double4>::type;
+    // density terms by (species X, species Y) with species in 3 bits (7:
+    // unknown), and the status bits a pair of that kind raises
+    __shared__ R4 dtab[64];
+    __shared__ int dflag[64];
+    __shared__ float4 ssh[kEntries];
+    for (int k = threadIdx.x; k < 64; k += blockDim.x) {
+        const int a = k >> 3, b = k & 7;
+        R4 d;
+        int fl;
+        if (a < kSpecies && b < kSpecies) {
+            const PairTab<R>& T = tab[a * kSpecies + b];
+            d.x = T.d_fe; d.y = T.d_inv_re; d.z = T.d_c; d.w = T.d_lam;
+            fl = T.valid ? 0 : ST_UNSUPPORTED;
+        } else {
+            d.x = 0; d.y = 1; d.z = 0; d.w = 0;
+            fl = ST_UNKNOWN_PAIR;
+        }
+        dtab[k] = d;
+        dflag[k] = fl;
+    }
+    for (int k = threadIdx.x; k < kEntries; k += blockDim.x) ssh[k] = F.sh[k];
     __syncthreads();
     const PairParams& P = F.pp;
     const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
@@ -303,80 +330,102 @@ __global__ void __launch_bounds__(256)
     int lmax = 0, bad = 0;
     unsigned long long ltot = 0;
     for (int X = blockIdx.x * wpb + (threadIdx.x >> 5); X < P.n; X += gridDim.x * wpb) {
-        const double4 xa = xq[X];
-        const int sX = ts[X];
-        const int cX = cx_s[X];
+        const float4 ra = rec[X];
+        const unsigned wa = __float_as_uint(ra.w);
+        const int sX = (int)(wa >> 27);
+        const int ax = wa & 511, ay = (wa >> 9) & 511, az = (wa >> 18) & 511;
+        // the "-1" neighbours of X's reference cell on each axis (periodic)
+        const int xm = ax == 0 ? F.nc.x - 1 : ax - 1;
+        const int ym = ay == 0 ? F.nc.y - 1 : ay - 1;
+        const int zm = az == 0 ? F.nc.z - 1 : az - 1;
+        const int oX = order[X];
+        const double4 xa = F32 ? make_double4(0, 0, 0, 0) : xq[X];
         const int2 ms = nn_s[X];
+        const int m = ms.x + ms.y;
+        const int back = F.cap_s - 1 + ms.x;   // slot of oxygen entry k is back - k
         const unsigned* srow = nbr_s + (size_t)X * F.cap_s;
         unsigned* row = nbr + (size_t)X * P.cap;
-        int out[2] = {0, 0};
+        // one index space over both groups: metals from the front, oxygen from the back
+        auto ent = [&](int k) { return k < m ? srow[k < ms.x ? k : back - k] : 0u; };
+        // software pipeline: entries two batches ahead, records one batch ahead
+        unsigned E1 = ent(lane), E2 = ent(lane + 32);
+        float4 rb1 = rec[E1 & kSkinIdxMask];
+        double4 xb1 = F32 ? make_double4(0, 0, 0, 0) : xq[E1 & kSkinIdxMask];
+        int out0 = 0, out1 = 0;
         double rho = 0.0;
-        for (int g = 0; g < 2; g++) {
-            const int mg = g == 0 ? ms.x : ms.y;
-            // pipelined: entry, position and cell of the next 32-slot batch
-            unsigned Yn = 0;
-            double4 xbn = make_double4(0, 0, 0, 0);
-            int cYn = 0;
-            if (lane < mg) {
-                Yn = srow[g == 0 ? lane : F.cap_s - 1 - lane] & kIdxMask;
-                xbn = xq[Yn];
-                cYn = cx_s[Yn];
-            }
-            for (int base = 0; base < mg; base += 32) {
-                const int k = base + lane;
-                const unsigned Y = Yn;
-                const double4 xb = xbn;
-                const int cY = cYn;
-                if (k + 32 < mg) {
-                    Yn = srow[g == 0 ? k + 32 : F.cap_s - 1 - (k + 32)] & kIdxMask;
-                    xbn = xq[Yn];
-                    cYn = cx_s[Yn];
-                }
-                bool acc = false;
-                double r2d = 0.0;
-                if (k < mg) {
-                    double dx, dy, dz;
-                    min_image(xa, xb, P, dx, dy, dz);
-                    r2d = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-                    acc = r2d < F.rcut2;
-                }
-                const unsigned mask = __ballot_sync(0xffffffffu, acc);
-                if (acc) {
-                    unsigned isa;
-                    if (cY == cX) {
-                        isa = order[X] < order[Y];
-                    } else {
-                        const int ox = wrap_off((cY & 1023) - (cX & 1023), F.nc.x);
-                        const int oy = wrap_off(((cY >> 10) & 1023) - ((cX >> 10) & 1023), F.nc.y);
-                        const int oz = wrap_off((cY >> 20) - (cX >> 20), F.nc.z);
-                        // the 13 forward cells of CELL_HIERARCHY (cellsort.f90:18-30)
-                        isa = oz == -1 || (oz == 0 && (oy == -1 || (oy == 0 && ox == -1)));
-                    }
-                    const int pos = out[g] + __popc(mask & lt);
-                    const int slot = g == 0 ? pos : P.cap - 1 - pos;
-                    if (g == 0 ? pos < P.cap : slot >= out[0]) row[slot] = Y | (isa << 31);
-                    // density of Y at X (force.f90:84-85)
-                    const int sY = g == 1 ? 3 : ts[Y];
-                    if (sX < kSpecies && sY < kSpecies) {
-                        const PairTab<R>& T = st[sX * kSpecies + sY];
-                        if (!T.valid) bad |= ST_UNSUPPORTED;
-                        const R r = sqrt((R)r2d);
-                        rho += (double)(T.d_fe * zhou_val<R>(r, T.d_inv_re, T.d_c, T.d_lam));
-                    } else {
-                        bad |= ST_UNKNOWN_PAIR;
+        for (int base = 0; base < m; base += 32) {
+            const int k = base + lane;
+            const unsigned e = E1;
+            const float4 rb = rb1;
+            const double4 xb = xb1;
+            E1 = E2;
+            rb1 = rec[E1 & kSkinIdxMask];
+            if (!F32) xb1 = xq[E1 & kSkinIdxMask];
+            E2 = ent(k + 64);
+            const unsigned Y = e & kSkinIdxMask;
+            const bool live = k < m;
+            bool acc;
+            R r2;
+            if constexpr (F32) {
+                const float4 o = ssh[e >> kSkinCodeShift];
+                const float dx = (rb.x - ra.x) + o.x, dy = (rb.y - ra.y) + o.y, dz = (rb.z - ra.z) + o.z;
+                const float r2f = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                acc = live & (r2f < F.rcut2f);
+                const bool inband = live & (fabsf(r2f - F.rcut2f) <= F.band);
+                if (__any_sync(0xffffffffu, inband)) {
+                    if (inband) {
+                        // within FP32 rounding of the cutoff: the reference's FP64 test
+                        double ddx, ddy, ddz;
+                        min_image(xq[X], xq[Y], P, ddx, ddy, ddz);
+                        acc = __dadd_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)), __dmul_rn(ddz, ddz)) <
+                              F.rcut2;
                     }
                 }
-                out[g] += __popc(mask);
+                r2 = r2f;
+            } else {
+                double dx, dy, dz;
+                min_image(xa, xb, P, dx, dy, dz);
+                const double r2d = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+                acc = live & (r2d < F.rcut2);
+                r2 = r2d;
             }
+            // X is the reference's i: Y's reference cell is one of the 13
+            // forward cells of X's (cellsort.f90:18-30), or the same cell and
+            // X comes first in it
+            const unsigned wb = __float_as_uint(rb.w);
+            const int bx = wb & 511, by = (wb >> 9) & 511, bz = (wb >> 18) & 511;
+            const bool same = ((wb ^ wa) & 0x07ffffffu) == 0u;
+            int oY = 0x7fffffff;
+            if (acc & same) oY = order[Y];
+            const bool isa = (bz == zm) | ((bz == az) & ((by == ym) | ((by == ay) & ((bx == xm) | (same & (oX < oY))))));
+            // compaction per group (lanes >= split hold oxygen entries)
+            const unsigned mask = __ballot_sync(0xffffffffu, acc);
+            const int split = ms.x - base;
+            const unsigned gm1 = split <= 0 ? 0xffffffffu : (split >= 32 ? 0u : (0xffffffffu << split));
+            const unsigned m1 = mask & gm1, m0 = mask & ~gm1;
+            const bool g1 = k >= ms.x;
+            const int pos = (g1 ? out1 : out0) + __popc((g1 ? m1 : m0) & lt);
+            if (acc & (pos < P.cap)) row[g1 ? P.cap - 1 - pos : pos] = e | ((unsigned)isa << 31);
+            out0 += __popc(m0);
+            out1 += __popc(m1);
+            // density of Y at X (force.f90:84-85)
+            const int ti = (sX << 3) | (int)(wb >> 27);
+            const R4 d = dtab[ti];
+            R r;
+            if constexpr (F32) r = r2 * rsqrtf(r2);
+            else r = sqrt(r2);
+            const R v = d.x * zhou_val<R>(r, d.y, d.z, d.w);
+            rho += acc ? (double)v : 0.0;
+            bad |= acc ? dflag[ti] : 0;
         }
         rho = warp_sum(rho);
         if (lane == 0) {
-            const int tot = out[0] + out[1];
+            const int tot = out0 + out1;
             if (tot > P.cap) {
                 atomicOr(status, ST_NBR_OVERFLOW);
                 nn[X] = make_int2(0, 0);
             } else {
-                nn[X] = make_int2(out[0], out[1]);
+                nn[X] = make_int2(out0, out1);
             }
             lmax = max(lmax, tot);
             ltot += (unsigned long long)tot;
@@ -525,6 +574,132 @@ __device__ __forceinline__ void force_group(const PairParams& P, const PairTab<R
             else bin = (int)((float)r * (float)(1.0 / P.dr_rdf));
             bin = min(max(bin, 0), NB - 1);
             atomicAdd(&hist[(sX + kSpecies * sY) * NB + bin], 2);
+        }
+    }
+}
+
+// Skin-mode FP32 force pass.  The separation comes from the force records,
+// x_X - x_Y = off_X - off_Y - o * Lcs (o: the entry's stencil position), so
+// no FP64 minimum image is needed; each lane sums its share of f_X in
+// compensated FP32 (hi + lo, Knuth's two-sum), and the lanes' sums are added
+// in FP64.  Needs one non-oxygen species (the partner species of every group
+// is then fixed) and no energies.
+__device__ __forceinline__ void two_sum_acc(float& hi, float& lo, float b) {
+    const float s = hi + b;
+    const float bp = s - hi;
+    const float ap = s - bp;
+    lo += (hi - ap) + (b - bp);
+    hi = s;
+}
+
+struct RecParams32 {
+    float a, two_a_sqrtpi, kc, inv_dr;
+    float4 sh[kEntries];
+};
+
+template <bool SAME, bool MHOMO, bool RDF>
+__device__ __forceinline__ void force_group_rec(const PairParams& P, const RecParams32& Q, const PairTab<float>& T,
+                                                const float4* ssh, const unsigned* row, int g, int mg, int lane,
+                                                const float4& ra, int sX, int sY, float dFX,
+                                                const float4* __restrict__ frec, const float* __restrict__ dF_f,
+                                                float (&fh)[3], float (&fl)[3], int* hist) {
+    constexpr int NB = SIMOX_NRDF + 2;
+    unsigned ent_n = 0;
+    float4 rb_n = make_float4(0.f, 0.f, 0.f, 0.f);
+    float dFY_n = 0.f;
+    if (lane < mg) {
+        ent_n = row[row_slot(g, lane, P.cap)];
+        rb_n = frec[ent_n & kIdxMask];
+        dFY_n = dF_f[ent_n & kIdxMask];
+    }
+    for (int k = lane; k < mg; k += 32) {
+        const unsigned ent = ent_n;
+        const float4 rb = rb_n;
+        const float dFY = dFY_n;
+        if (k + 32 < mg) {
+            ent_n = row[row_slot(g, k + 32, P.cap)];
+            rb_n = frec[ent_n & kIdxMask];
+            dFY_n = dF_f[ent_n & kIdxMask];
+        }
+        const float4 o = ssh[(ent >> kSkinCodeShift) & kCodeMask];
+        const float dx = (ra.x - rb.x) - o.x, dy = (ra.y - rb.y) - o.y, dz = (ra.z - rb.z) - o.z;
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        const float ir = rsqrtf(r2), r = r2 * ir;
+        float erfcv;
+        double ep, ed, ec;
+        const float fs = pair_fs<float, SAME, MHOMO, false>(T, r, ir, ra.w, rb.w, dFX, dFY, Q.a, Q.two_a_sqrtpi, Q.kc,
+                                                           erfcv, ep, ed, ec);
+        two_sum_acc(fh[0], fl[0], fs * dx);
+        two_sum_acc(fh[1], fl[1], fs * dy);
+        two_sum_acc(fh[2], fl[2], fs * dz);
+        if (RDF && (ent & kIsA)) {
+            const int bin = min(max((int)(r * Q.inv_dr), 0), NB - 1);
+            atomicAdd(&hist[(sX + kSpecies * sY) * NB + bin], 2);
+        }
+    }
+}
+
+template <bool RDF>
+__global__ void __launch_bounds__(256, 3)
+    force_rec_kernel(PairParams P, RecParams32 Q, const PairTab<float>* __restrict__ tab,
+                     const float4* __restrict__ frec, const int* __restrict__ ts, const int2* __restrict__ nn,
+                     const unsigned* __restrict__ nbr, const float* __restrict__ dF_f, const int* __restrict__ sorted,
+                     int g0, double* __restrict__ f, int* __restrict__ rdf, int* __restrict__ status) {
+    __shared__ PairTab<float> st[kSpecies * kSpecies];
+    __shared__ float4 ssh[kEntries];
+    constexpr int NB = SIMOX_NRDF + 2;
+    __shared__ int hist[RDF ? kSpecies * kSpecies * NB : 1];
+    for (int k = threadIdx.x; k < kSpecies * kSpecies; k += blockDim.x) st[k] = tab[k];
+    for (int k = threadIdx.x; k < kEntries; k += blockDim.x) ssh[k] = Q.sh[k];
+    if (RDF)
+        for (int k = threadIdx.x; k < kSpecies * kSpecies * NB; k += blockDim.x) hist[k] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    int bad = 0;
+    for (int X = blockIdx.x * wpb + (threadIdx.x >> 5); X < P.n; X += gridDim.x * wpb) {
+        const float4 ra = frec[X];
+        const int sX = ts[X];
+        const float dFX = dF_f[X];
+        const int2 m = nn[X];
+        const unsigned* row = nbr + (size_t)X * P.cap;
+        float fh[3] = {0.f, 0.f, 0.f}, fl[3] = {0.f, 0.f, 0.f};
+        if (sX == g0) {          // metal X: metal partners (its own species) then oxygen
+            force_group_rec<true, true, RDF>(P, Q, st[sX * kSpecies + g0], ssh, row, 0, m.x, lane, ra, sX, g0, dFX,
+                                             frec, dF_f, fh, fl, hist);
+            force_group_rec<false, false, RDF>(P, Q, st[sX * kSpecies + 3], ssh, row, 1, m.y, lane, ra, sX, 3, dFX,
+                                               frec, dF_f, fh, fl, hist);
+        } else if (sX == 3) {    // oxygen X: metal partners then oxygen
+            force_group_rec<false, false, RDF>(P, Q, st[3 * kSpecies + g0], ssh, row, 0, m.x, lane, ra, 3, g0, dFX,
+                                               frec, dF_f, fh, fl, hist);
+            force_group_rec<true, false, RDF>(P, Q, st[3 * kSpecies + 3], ssh, row, 1, m.y, lane, ra, 3, 3, dFX,
+                                              frec, dF_f, fh, fl, hist);
+        } else if (m.x + m.y > 0) {
+            bad |= ST_UNKNOWN_PAIR;
+        }
+        double fx = (double)fh[0] + (double)fl[0];
+        double fy = (double)fh[1] + (double)fl[1];
+        double fz = (double)fh[2] + (double)fl[2];
+        fx = warp_sum(fx);
+        fy = warp_sum(fy);
+        fz = warp_sum(fz);
+        if (lane == 0) {
+            const int o = sorted[X];
+            f[3 * o] = fx;
+            f[3 * o + 1] = fy;
+            f[3 * o + 2] = fz;
+        }
+    }
+    if (bad) atomicOr(status, bad);
+    if (RDF) {
+        __syncthreads();
+        for (int k = threadIdx.x; k < kSpecies * kSpecies * NB; k += blockDim.x) {
+            int v = hist[k];
+            if (v) {
+                int pr = k / NB, bin = k % NB;
+                int si = pr % kSpecies, sj = pr / kSpecies;
+                atomicAdd(&rdf[si + 5 * sj + 25 * bin], v);
+            }
         }
     }
 }
@@ -681,23 +856,49 @@ int eam_density(simox_ctx* c, bool eflag) {
     return check_launch(c);
 }
 
+// Rounding bound of the FP32 r2 of a listed pair near the cutoff.  Offsets
+// |off| <= A = Lcs/2 + skin/2 (+ slack) are rounded once (u = 2^-24), their
+// difference once, o*Lcs once and the sum once: |err dx| <= u (6A + 2 Lcs);
+// r2 = dx^2 + dy^2 + dz^2 with two fused steps adds <= 3u r2.  The band is
+// four times that bound at r = Rcut.
+static float filter_band(const simox_ctx* c) {
+    const double u = std::ldexp(1.0, -24);
+    double lmax = 0.0;
+    for (int d = 0; d < 3; d++) lmax = std::max(lmax, c->lcs[d]);
+    const double A = 0.5 * lmax + 0.5 * c->skin + 1.0e-3;
+    const double e = u * (6.0 * A + 2.0 * lmax);
+    const double bound = 2.0 * std::sqrt(3.0) * c->rcut * e + 3.0 * e * e + 3.0 * u * c->rcut2 * 1.01;
+    return (float)(4.0 * bound);
+}
+
+// skin stencil position e = (dk+1)*9 + (dj+1)*3 + (di+1) -> o * Lcs
+static void stencil_shifts(const simox_ctx* c, float4* sh) {
+    for (int e = 0; e < kEntries; e++) {
+        const int di = e % 3 - 1, dj = (e / 3) % 3 - 1, dk = e / 9 - 1;
+        sh[e] = make_float4((float)(di * c->lcs[0]), (float)(dj * c->lcs[1]), (float)(dk * c->lcs[2]), 0.f);
+    }
+}
+
 int filter_density(simox_ctx* c) {
     FilterParams F;
     F.pp = pair_params(c);
     F.rcut2 = c->rcut2;
+    F.rcut2f = (float)c->rcut2;
+    F.band = filter_band(c);
     F.nc = make_int3(c->nc[0], c->nc[1], c->nc[2]);
     F.cap_s = c->cap_s;
+    stencil_shifts(c, F.sh);
     EmbedParams E = embed_params(c->pot);
     if (c->n > 0) {
         Launch L(c, "neighbor_filter_density");
         const int g = std::min((c->n + 7) / 8, num_sms(c) * 8);
         if (c->precision == SIMOX_FP64)
             filter_density_kernel<double><<<g, 256, 0, c->stream>>>(
-                F, c->tab_d, c->xq_s, c->t_s, c->cx_s, c->pair_order, reinterpret_cast<const int2*>(c->nn_s), c->nbr_s,
+                F, c->tab_d, c->xq_s, c->rec_s, c->pair_order, reinterpret_cast<const int2*>(c->nn_s), c->nbr_s,
                 reinterpret_cast<int2*>(c->nn), c->nbr, E, c->rho_s, c->dF_s, c->dF_f, c->status, c->nn_max, c->nn_tot);
         else
             filter_density_kernel<float><<<g, 256, 0, c->stream>>>(
-                F, c->tab_f, c->xq_s, c->t_s, c->cx_s, c->pair_order, reinterpret_cast<const int2*>(c->nn_s), c->nbr_s,
+                F, c->tab_f, c->xq_s, c->rec_s, c->pair_order, reinterpret_cast<const int2*>(c->nn_s), c->nbr_s,
                 reinterpret_cast<int2*>(c->nn), c->nbr, E, c->rho_s, c->dF_s, c->dF_f, c->status, c->nn_max, c->nn_tot);
     }
     int st = check_launch(c);
@@ -730,6 +931,26 @@ static void launch_force(simox_ctx* c, const PairTab<R>* tab, bool eflag, bool r
 int pair_forces(simox_ctx* c, bool eflag, bool rdf) {
     if (!c->eam_valid) return SIMOX_E_STATE;
     if (c->n == 0) return SIMOX_OK;
+    if (!use_fp64(c, eflag) && c->using_skin && c->g0_species >= 0) {
+        Launch L(c, "pair_force");
+        PairParams P = pair_params(c);
+        RecParams32 Q;
+        Q.a = (float)P.a;
+        Q.two_a_sqrtpi = (float)(2.0 * P.a / SX_SQRTPI);
+        Q.kc = (float)P.kc;
+        Q.inv_dr = (float)(1.0 / P.dr_rdf);
+        stencil_shifts(c, Q.sh);
+        const int g = std::max(1, std::min((c->n + 7) / 8, num_sms(c) * 3 * 2));
+        if (rdf)
+            force_rec_kernel<true><<<g, 256, 0, c->stream>>>(P, Q, c->tab_f, c->frec_s, c->t_s,
+                                                             reinterpret_cast<const int2*>(c->nn), c->nbr, c->dF_f,
+                                                             c->pair_order, c->g0_species, c->f, c->rdf, c->status);
+        else
+            force_rec_kernel<false><<<g, 256, 0, c->stream>>>(P, Q, c->tab_f, c->frec_s, c->t_s,
+                                                              reinterpret_cast<const int2*>(c->nn), c->nbr, c->dF_f,
+                                                              c->pair_order, c->g0_species, c->f, c->rdf, c->status);
+        return check_launch(c);
+    }
     Launch L(c, use_fp64(c, eflag) ? "pair_force_fp64" : "pair_force");
     if (!use_fp64(c, eflag)) launch_force<float>(c, c->tab_f, eflag, rdf);
     else launch_force<double>(c, c->tab_d, eflag, rdf);

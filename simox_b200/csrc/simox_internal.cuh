@@ -22,8 +22,14 @@ namespace sx {
 constexpr int kSpecies = 4;           // Al, Ni, Fe, O on the device tables (H is rejected)
 constexpr int kMaxOrder = 8;
 constexpr int kEntries = 27;          // self + 13 forward + 13 reverse stencil cells
-constexpr unsigned kIsA = 0x80000000u;  // list entry bit: this atom is the reference's "i"
-constexpr unsigned kIdxMask = 0x7fffffffu;
+// Neighbour-list entry: atom index (bits 0-25) | skin-grid stencil position
+// of the partner (bits 26-30, skin mode) | "this atom is the reference's i"
+// (bit 31, exact lists).
+constexpr unsigned kIsA = 0x80000000u;
+constexpr unsigned kIdxMask = 0x03ffffffu;
+constexpr unsigned kSkinIdxMask = kIdxMask;
+constexpr int kSkinCodeShift = 26;
+constexpr unsigned kCodeMask = 31u;
 
 // Device status bits (OR-ed by kernels, read by the host after a call).
 enum : int {
@@ -145,7 +151,9 @@ struct simox_ctx {
     // sorted copies
     double4* xq_s = nullptr;    // x, y, z, q
     int* t_s = nullptr;         // species 0..4
-    int* cx_s = nullptr;        // packed reference-cell coordinates in pair order
+    float4* rec_s = nullptr;    // skin filter record in pair order: skin-cell offset, (cell, species)
+    float4* frec_s = nullptr;   // skin force record in pair order: skin-cell offset, charge
+    int g0_species = -1;        // the one non-oxygen species present, or -1
     bool rho_ready = false;     // rho/F' of the filter pass are current (context precision)
 
     // neighbour list

@@ -249,18 +249,75 @@ def test_md_skin_list_vs_oracle(skin):
 
 
 def test_md_skin_mixed_matches_fp64():
-    """Mixed precision with the skin list: forces within 1e-5 of FP64."""
+    """Mixed precision with the skin list (FP32 filter records, record-based
+    FP32 force pass): forces within 1e-5 of FP64; the same pairs, each
+    counted once with the reference's i, so per species pair the RDF totals
+    are identical (bins may differ at bin edges: FP32 r)."""
     s = S.small_alo(**SKIN_BOX)
-    out = {}
+    out, hist = {}, {}
     for prec in ("fp64", "mixed"):
+        rdf = np.zeros(_abi.RDF_LEN, np.int32)
         with gpu_context(s, precision=prec) as g:
             g.pme_self()
             g.cell_sort()
             g.force(energies=False)
             g.pme(energies=False)
-            g.md_run(4, 1.0 / S.TFM, first_step=2, thermostat=True, T_given=600 * S.KB, freq_new=0, freq_stat=1000)
+            g.md_run(4, 1.0 / S.TFM, first_step=2, thermostat=True, T_given=600 * S.KB, freq_new=0, freq_stat=1000,
+                     rdf=rdf)
             out[prec] = g.get_state()["f"]
+        hist[prec] = rdf.reshape(-1, 25).sum(0)
     assert rel_err(out["mixed"], out["fp64"]) <= 1e-5
+    assert np.array_equal(hist["mixed"], hist["fp64"]) and hist["fp64"].sum() > 0
+
+
+def _cutoff_lattice(seed=3, m=16, a=2.5, jitter=1.0e-7):
+    """Simple cubic Al/O lattice (a = Rcut/4): every atom has six partners at
+    r = Rcut up to a jitter of 1e-7 A, inside the FP32 rounding band of the
+    mixed filter, so membership is decided by the FP64 re-test."""
+    rng = np.random.default_rng(seed)
+    g = np.arange(m) * a - m * a / 2
+    x = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    x = x + rng.uniform(-jitter, jitter, x.shape)
+    par = (np.indices((m, m, m)).sum(0) % 2).reshape(-1)
+    ids = np.where(par == 0, 1, 4).astype(np.int32)
+    q = np.where(ids == 1, 0.5, -0.5)
+    box = np.full(3, m * a)
+    return S.AtomSystem("cutoff_lattice", ids, S.wrap_centered(x, box), np.zeros_like(x), q, box, (32, 32, 32), 4,
+                        10.0, {})
+
+
+def test_mixed_filter_membership_at_cutoff():
+    """Pairs within FP32 rounding of Rcut: the mixed context's exact list and
+    its FP64 energies equal the FP64 context's."""
+    s = _cutoff_lattice()
+    out = {}
+    for prec in ("fp64", "mixed"):
+        with gpu_context(s, precision=prec) as g:
+            g.pme_self()
+            g.cell_sort()
+            e = g.force()
+            out[prec] = (g.neighbor_stats(), e)
+    (mx64, tot64), e64 = out["fp64"]
+    (mxm, totm), em = out["mixed"]
+    assert (mxm, totm) == (mx64, tot64)
+    # the reference's r2 < Rcut2 over all pairs (force.f90:51-54, DNINT half away)
+    x, L = s.x, s.box
+    inside = near_in = near = 0
+    for i0 in range(0, s.n, 256):
+        d = x[i0:i0 + 256, None, :] - x[None, :, :]
+        t = d / L
+        d = d - L * np.trunc(t + np.copysign(0.5, t))
+        r2 = (d[..., 0] * d[..., 0] + d[..., 1] * d[..., 1]) + d[..., 2] * d[..., 2]
+        idx = np.arange(i0, min(i0 + 256, s.n))
+        r2[idx - i0, idx] = np.inf
+        inside += int((r2 < 100.0).sum())
+        band = np.abs(r2 - 100.0) < 1e-4
+        near += int(band.sum())
+        near_in += int((band & (r2 < 100.0)).sum())
+    assert tot64 == inside
+    assert near == 6 * s.n and 0 < near_in < near
+    for k in ("Epair", "Egroup", "Edir"):
+        assert abs(em[k] - e64[k]) <= 1e-10 * abs(e64[k]), k
 
 
 def test_status_codes():
