@@ -91,6 +91,7 @@ int build_pair_tables(simox_ctx* c) {
     PairTab<float> tf[kSpecies * kSpecies];
     fill_tab<double>(c->pot, td);
     fill_tab<float>(c->pot, tf);
+    std::memcpy(c->h_tab_f, tf, sizeof(tf));
     cudaError_t e1 = cudaMemcpyAsync(c->tab_d, td, sizeof(td), cudaMemcpyHostToDevice, c->stream);
     cudaError_t e2 = cudaMemcpyAsync(c->tab_f, tf, sizeof(tf), cudaMemcpyHostToDevice, c->stream);
     if (e1 != cudaSuccess || e2 != cudaSuccess) return SIMOX_E_CUDA;
@@ -592,13 +593,18 @@ __device__ __forceinline__ void two_sum_acc(float& hi, float& lo, float b) {
     hi = s;
 }
 
+// The four species-pair tables of a one-metal system travel as kernel
+// parameters (constant bank): (metal, metal), (metal, O), (O, metal), (O, O).
+constexpr int kRecBlocks = 5;   // resident 256-thread CTAs per SM (<= 48 registers)
+
 struct RecParams32 {
     float a, two_a_sqrtpi, kc, inv_dr;
     float4 sh[kEntries];
+    PairTab<float> tab[4];
 };
 
-template <bool SAME, bool MHOMO, bool RDF>
-__device__ __forceinline__ void force_group_rec(const PairParams& P, const RecParams32& Q, const PairTab<float>& T,
+template <bool SAME, bool MHOMO, bool RDF, int TI>
+__device__ __forceinline__ void force_group_rec(const PairParams& P, const RecParams32& Q,
                                                 const float4* ssh, const unsigned* row, int g, int mg, int lane,
                                                 const float4& ra, int sX, int sY, float dFX,
                                                 const float4* __restrict__ frec, const float* __restrict__ dF_f,
@@ -627,8 +633,8 @@ __device__ __forceinline__ void force_group_rec(const PairParams& P, const RecPa
         const float ir = rsqrtf(r2), r = r2 * ir;
         float erfcv;
         double ep, ed, ec;
-        const float fs = pair_fs<float, SAME, MHOMO, false>(T, r, ir, ra.w, rb.w, dFX, dFY, Q.a, Q.two_a_sqrtpi, Q.kc,
-                                                           erfcv, ep, ed, ec);
+        const float fs = pair_fs<float, SAME, MHOMO, false>(Q.tab[TI], r, ir, ra.w, rb.w, dFX, dFY, Q.a,
+                                                           Q.two_a_sqrtpi, Q.kc, erfcv, ep, ed, ec);
         two_sum_acc(fh[0], fl[0], fs * dx);
         two_sum_acc(fh[1], fl[1], fs * dy);
         two_sum_acc(fh[2], fl[2], fs * dz);
@@ -640,16 +646,13 @@ __device__ __forceinline__ void force_group_rec(const PairParams& P, const RecPa
 }
 
 template <bool RDF>
-__global__ void __launch_bounds__(256, 3)
-    force_rec_kernel(PairParams P, RecParams32 Q, const PairTab<float>* __restrict__ tab,
-                     const float4* __restrict__ frec, const int* __restrict__ ts, const int2* __restrict__ nn,
+__global__ void __launch_bounds__(256, kRecBlocks)
+    force_rec_kernel(PairParams P, const __grid_constant__ RecParams32 Q, const float4* __restrict__ frec, const int* __restrict__ ts, const int2* __restrict__ nn,
                      const unsigned* __restrict__ nbr, const float* __restrict__ dF_f, const int* __restrict__ sorted,
                      int g0, double* __restrict__ f, int* __restrict__ rdf, int* __restrict__ status) {
-    __shared__ PairTab<float> st[kSpecies * kSpecies];
     __shared__ float4 ssh[kEntries];
     constexpr int NB = SIMOX_NRDF + 2;
     __shared__ int hist[RDF ? kSpecies * kSpecies * NB : 1];
-    for (int k = threadIdx.x; k < kSpecies * kSpecies; k += blockDim.x) st[k] = tab[k];
     for (int k = threadIdx.x; k < kEntries; k += blockDim.x) ssh[k] = Q.sh[k];
     if (RDF)
         for (int k = threadIdx.x; k < kSpecies * kSpecies * NB; k += blockDim.x) hist[k] = 0;
@@ -665,15 +668,15 @@ __global__ void __launch_bounds__(256, 3)
         const unsigned* row = nbr + (size_t)X * P.cap;
         float fh[3] = {0.f, 0.f, 0.f}, fl[3] = {0.f, 0.f, 0.f};
         if (sX == g0) {          // metal X: metal partners (its own species) then oxygen
-            force_group_rec<true, true, RDF>(P, Q, st[sX * kSpecies + g0], ssh, row, 0, m.x, lane, ra, sX, g0, dFX,
-                                             frec, dF_f, fh, fl, hist);
-            force_group_rec<false, false, RDF>(P, Q, st[sX * kSpecies + 3], ssh, row, 1, m.y, lane, ra, sX, 3, dFX,
-                                               frec, dF_f, fh, fl, hist);
+            force_group_rec<true, true, RDF, 0>(P, Q, ssh, row, 0, m.x, lane, ra, sX, g0, dFX, frec, dF_f, fh, fl,
+                                                hist);
+            force_group_rec<false, false, RDF, 1>(P, Q, ssh, row, 1, m.y, lane, ra, sX, 3, dFX, frec, dF_f, fh, fl,
+                                                  hist);
         } else if (sX == 3) {    // oxygen X: metal partners then oxygen
-            force_group_rec<false, false, RDF>(P, Q, st[3 * kSpecies + g0], ssh, row, 0, m.x, lane, ra, 3, g0, dFX,
-                                               frec, dF_f, fh, fl, hist);
-            force_group_rec<true, false, RDF>(P, Q, st[3 * kSpecies + 3], ssh, row, 1, m.y, lane, ra, 3, 3, dFX,
-                                              frec, dF_f, fh, fl, hist);
+            force_group_rec<false, false, RDF, 2>(P, Q, ssh, row, 0, m.x, lane, ra, 3, g0, dFX, frec, dF_f, fh, fl,
+                                                  hist);
+            force_group_rec<true, false, RDF, 3>(P, Q, ssh, row, 1, m.y, lane, ra, 3, 3, dFX, frec, dF_f, fh, fl,
+                                                 hist);
         } else if (m.x + m.y > 0) {
             bad |= ST_UNKNOWN_PAIR;
         }
@@ -940,13 +943,19 @@ int pair_forces(simox_ctx* c, bool eflag, bool rdf) {
         Q.kc = (float)P.kc;
         Q.inv_dr = (float)(1.0 / P.dr_rdf);
         stencil_shifts(c, Q.sh);
-        const int g = std::max(1, std::min((c->n + 7) / 8, num_sms(c) * 3 * 2));
+        const int g0 = c->g0_species;
+        const PairTab<float>* h = c->h_tab_f;
+        Q.tab[0] = h[g0 * kSpecies + g0];
+        Q.tab[1] = h[g0 * kSpecies + 3];
+        Q.tab[2] = h[3 * kSpecies + g0];
+        Q.tab[3] = h[3 * kSpecies + 3];
+        const int g = std::max(1, std::min((c->n + 7) / 8, num_sms(c) * kRecBlocks * 2));
         if (rdf)
-            force_rec_kernel<true><<<g, 256, 0, c->stream>>>(P, Q, c->tab_f, c->frec_s, c->t_s,
+            force_rec_kernel<true><<<g, 256, 0, c->stream>>>(P, Q, c->frec_s, c->t_s,
                                                              reinterpret_cast<const int2*>(c->nn), c->nbr, c->dF_f,
                                                              c->pair_order, c->g0_species, c->f, c->rdf, c->status);
         else
-            force_rec_kernel<false><<<g, 256, 0, c->stream>>>(P, Q, c->tab_f, c->frec_s, c->t_s,
+            force_rec_kernel<false><<<g, 256, 0, c->stream>>>(P, Q, c->frec_s, c->t_s,
                                                               reinterpret_cast<const int2*>(c->nn), c->nbr, c->dF_f,
                                                               c->pair_order, c->g0_species, c->f, c->rdf, c->status);
         return check_launch(c);

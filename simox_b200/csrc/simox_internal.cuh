@@ -170,6 +170,7 @@ struct simox_ctx {
     // pair tables
     sx::PairTab<double>* tab_d = nullptr;
     sx::PairTab<float>* tab_f = nullptr;
+    sx::PairTab<float> h_tab_f[sx::kSpecies * sx::kSpecies];   // host copy (kernel-parameter tables)
 
     // PME: pme[0] in the context's precision; pme[1] the FP64 twin that a
     // mixed-precision context uses when energies are requested
