@@ -81,6 +81,7 @@ void prof_end(simox_ctx* c, int id, cudaEvent_t a, cudaEvent_t b) {
 void prof_collect(simox_ctx* c) {
     if (c->ev_pending.empty()) return;
     cudaStreamSynchronize(c->stream);
+    if (c->side) cudaStreamSynchronize(c->side);
     for (auto& p : c->ev_pending) {
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, p.second.first, p.second.second) == cudaSuccess) c->prof.ms[p.first] += ms;
@@ -109,12 +110,25 @@ int md_run(simox_ctx* c, const simox_md_opts* o, int first, int nsteps, simox_en
             simox_ctip_report rep;
             if ((st = ctip_solve(c, 0, &rep))) return st;
         }
+        // PME (positions and charges only) runs on the side stream while the
+        // pair passes run; its forces land in f_rec and the second half kick
+        // adds them: f = f_pair + f_rec - Fsum/N, as FORCE + PME would leave f.
+        if ((st = ensure_gathered(c))) return st;
+        cudaEventRecord(c->ev_fork, c->stream);
+        cudaStreamWaitEvent(c->side, c->ev_fork, 0);
+        std::swap(c->stream, c->side);
+        pme_bind_stream(c);
+        st = pme_forces(c, false, estep, c->f_rec);
+        std::swap(c->stream, c->side);
+        pme_bind_stream(c);
+        if (st) return st;
+        cudaEventRecord(c->ev_join, c->side);
         if ((st = ensure_list(c))) return st;
         if ((st = eam_density(c, estep))) return st;
         if ((st = pair_forces(c, estep, want_rdf))) return st;
-        if ((st = pme_forces(c, false, estep))) return st;
-        if (o->thermostat) st = nvt2_berend(c, o->dt, o->T_given, true);
-        else st = vv2(c, o->dt, true);
+        cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+        if (o->thermostat) st = nvt2_berend(c, o->dt, o->T_given, true, c->f_rec);
+        else st = vv2(c, o->dt, true, c->f_rec);
         if (st) return st;
     }
     if ((st = read_status(c))) return st;
@@ -254,7 +268,7 @@ static void free_ctx(simox_ctx* c) {
                     c->sorted, c->pair13, c->entries, c->xq_s, c->t_s, c->rec_s, c->frec_s, c->nn, c->nbr, c->nn_max, c->nn_tot,
                     c->cs_count, c->cs_start, c->cs_fill, c->cs_cell_of, c->cs_entries, c->perm, c->x0,
                     c->skin_flag, c->nn_s, c->nbr_s, c->rho_s, c->dF_s, c->dF_f, c->tab_d, c->tab_f, c->c_const, c->g, c->pv, c->Ap, c->qs, c->jp,
-                    c->act, c->line, c->acc, c->status, c->rdf};
+                    c->act, c->line, c->acc, c->status, c->rdf, c->f_rec};
     for (void* p : bufs)
         if (p) cudaFree(p);
     if (c->h_acc) cudaFreeHost(c->h_acc);
@@ -263,6 +277,9 @@ static void free_ctx(simox_ctx* c) {
     for (auto& p : c->ev_pending) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
     if (c->t0) cudaEventDestroy(c->t0);
     if (c->t1) cudaEventDestroy(c->t1);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
+    if (c->side) cudaStreamDestroy(c->side);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -335,9 +352,15 @@ extern "C" int simox_create(const simox_setup* s, const simox_potential* pot, si
     c->ncell = c->nc[0] * c->nc[1] * c->nc[2];
 
     int st = SIMOX_OK;
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { free_ctx(c); return SIMOX_E_CUDA; }
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        free_ctx(c);
+        return SIMOX_E_CUDA;
+    }
     const size_t N = (size_t)c->cap;
-    bool ok = dalloc(&c->id, N) && dalloc(&c->x, 3 * N) && dalloc(&c->v, 3 * N) && dalloc(&c->f, 3 * N) &&
+    bool ok = dalloc(&c->id, N) && dalloc(&c->x, 3 * N) && dalloc(&c->v, 3 * N) && dalloc(&c->f, 3 * N) && dalloc(&c->f_rec, 3 * N) &&
               dalloc(&c->q, N) && dalloc(&c->cell_of, N) && dalloc(&c->cell_xyz, N) && dalloc(&c->cell_count, c->ncell) &&
               dalloc(&c->cell_start, c->ncell + 1) && dalloc(&c->cell_fill, c->ncell) && dalloc(&c->sorted, N) &&
               dalloc(&c->pair13, (size_t)c->ncell * 13) && dalloc(&c->entries, (size_t)c->ncell * kEntries) &&

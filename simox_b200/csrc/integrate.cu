@@ -50,8 +50,8 @@ __global__ void vv1_kernel(int n, const int* __restrict__ id, double* __restrict
 // second half kick (+ optional mean-force removal); mv2 and per-species sums
 template <bool BEREND>
 __global__ void __launch_bounds__(256)
-    vv2_kernel(int n, const int* __restrict__ id, double* __restrict__ v, double* __restrict__ f, double dt,
-               Masses M, double* __restrict__ acc, int subtract_mean) {
+    vv2_kernel(int n, const int* __restrict__ id, double* __restrict__ v, double* __restrict__ f,
+               const double* __restrict__ f_add, double dt, Masses M, double* __restrict__ acc, int subtract_mean) {
     __shared__ double red[256 / 32];
     double mv2 = 0.0;
     double ms[5] = {0, 0, 0, 0, 0};
@@ -64,10 +64,9 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
         for (int d = 0; d < 3; d++) {
             double ff = f[3 * i + d];
-            if (subtract_mean) {
-                ff = __dsub_rn(ff, __ddiv_rn(acc[A_FSUM0 + d], (double)n));
-                f[3 * i + d] = ff;
-            }
+            if (f_add) ff = __dadd_rn(ff, f_add[3 * i + d]);   // ff + ff_rec - Fsum (force.f90:459)
+            if (subtract_mean) ff = __dsub_rn(ff, __ddiv_rn(acc[A_FSUM0 + d], (double)n));
+            if (f_add || subtract_mean) f[3 * i + d] = ff;
             const double vv = half_kick(v[3 * i + d], ff, dt, xm);
             v[3 * i + d] = vv;
             if (BEREND) t = __dadd_rn(t, __dmul_rn(xm, __dmul_rn(vv, vv)));
@@ -150,24 +149,24 @@ int vv1(simox_ctx* c, double dt, bool reflect) {
     return check_launch(c);
 }
 
-int vv2(simox_ctx* c, double dt, bool subtract_mean) {
+int vv2(simox_ctx* c, double dt, bool subtract_mean, const double* f_add) {
     cudaMemsetAsync(c->acc + A_MV2, 0, sizeof(double), c->stream);
     if (c->n == 0) return SIMOX_OK;
     {
         Launch L(c, "vv_nve2");
-        vv2_kernel<false><<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->n, c->id, c->v, c->f, dt, masses(c), c->acc,
-                                                                     subtract_mean ? 1 : 0);
+        vv2_kernel<false><<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->n, c->id, c->v, c->f, f_add, dt, masses(c),
+                                                                     c->acc, subtract_mean ? 1 : 0);
     }
     return check_launch(c);
 }
 
-int nvt2_berend(simox_ctx* c, double dt, double T_given, bool subtract_mean) {
+int nvt2_berend(simox_ctx* c, double dt, double T_given, bool subtract_mean, const double* f_add) {
     cudaMemsetAsync(c->acc + A_MV2, 0, sizeof(double) * (A_NS4 + 1 - A_MV2), c->stream);
     if (c->n == 0) return SIMOX_OK;
     {
         Launch L(c, "vv_nvt2_kick");
-        vv2_kernel<true><<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->n, c->id, c->v, c->f, dt, masses(c), c->acc,
-                                                                    subtract_mean ? 1 : 0);
+        vv2_kernel<true><<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->n, c->id, c->v, c->f, f_add, dt, masses(c),
+                                                                    c->acc, subtract_mean ? 1 : 0);
     }
     {
         Launch L(c, "vv_nvt2_scale");

@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(256)
 template <typename R, int P>
 __global__ void __launch_bounds__(128)
     gather_force_kernel(PmeParams S, const double4* __restrict__ xq, const R* __restrict__ grid,
-                        const int* __restrict__ sorted, double* __restrict__ f, double* __restrict__ acc) {
+                        const int* __restrict__ sorted, double* __restrict__ f, double* __restrict__ acc, int store) {
     __shared__ double red[128 / 32];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     double fo[3] = {0.0, 0.0, 0.0};
@@ -192,9 +192,15 @@ __global__ void __launch_bounds__(128)
         fo[1] = pre * sy * S.kx.y;
         fo[2] = pre * sz * S.kx.z;
         const int o = sorted[k];
-        f[3 * o] += fo[0];
-        f[3 * o + 1] += fo[1];
-        f[3 * o + 2] += fo[2];
+        if (store) {   // separate reciprocal-force buffer
+            f[3 * o] = fo[0];
+            f[3 * o + 1] = fo[1];
+            f[3 * o + 2] = fo[2];
+        } else {
+            f[3 * o] += fo[0];
+            f[3 * o + 1] += fo[1];
+            f[3 * o + 2] += fo[2];
+        }
     }
     block_add<128>(fo[0], acc, A_FSUM0, red);
     block_add<128>(fo[1], acc, A_FSUM1, red);
@@ -452,14 +458,14 @@ static PmeParams pme_params(const simox_ctx* c) {
 }
 
 template <typename R, int P>
-static int pme_forces_t(simox_ctx* c, PmeRes& Rs, bool eflag) {
+static int pme_forces_t(simox_ctx* c, PmeRes& Rs, bool eflag, double* f_store) {
     PmeParams S = pme_params(c);
     run_spread<R, P>(c, Rs, S, nullptr);
     int st = run_convolution(c, Rs, eflag);
     if (st) return st;
     Launch L(c, "pme_gather_force");
-    gather_force_kernel<R, P><<<(S.n + 127) / 128, 128, 0, c->stream>>>(S, c->xq_s, (const R*)Rs.grid, c->pair_order,
-                                                                        c->f, c->acc);
+    gather_force_kernel<R, P><<<(S.n + 127) / 128, 128, 0, c->stream>>>(
+        S, c->xq_s, (const R*)Rs.grid, c->pair_order, f_store ? f_store : c->f, c->acc, f_store ? 1 : 0);
     return SIMOX_OK;
 }
 
@@ -484,6 +490,15 @@ __global__ void subtract_mean_kernel(int n, double* __restrict__ f, const double
     f[3 * i + 2] = __dsub_rn(f[3 * i + 2], __ddiv_rn(acc[A_FSUM2], (double)n));
 }
 
+// cuFFT plans follow the context's current stream
+void pme_bind_stream(simox_ctx* c) {
+    for (PmeRes& R : c->pme)
+        if (R.ready) {
+            cufftSetStream(R.r2c, c->stream);
+            cufftSetStream(R.c2r, c->stream);
+        }
+}
+
 int pme_finalize_forces(simox_ctx* c) {
     if (c->n == 0) return SIMOX_OK;
     Launch L(c, "pme_mean_force");
@@ -491,7 +506,8 @@ int pme_finalize_forces(simox_ctx* c) {
     return check_launch(c);
 }
 
-int pme_forces(simox_ctx* c, bool finalize, bool eflag) {
+// f_store: write the reciprocal forces there instead of adding them to f
+int pme_forces(simox_ctx* c, bool finalize, bool eflag, double* f_store) {
     if (!c->psi_valid) return SIMOX_E_STATE;
     if (int st0 = ensure_gathered(c)) return st0;
     if (c->n == 0) return SIMOX_OK;
@@ -501,9 +517,9 @@ int pme_forces(simox_ctx* c, bool finalize, bool eflag) {
     PmeRes& Rs = (eflag && c->pme[1].ready) ? c->pme[1] : c->pme[0];
     const bool dbl = Rs.dbl;
     switch (c->order) {
-        case 4: st = dbl ? pme_forces_t<double, 4>(c, Rs, eflag) : pme_forces_t<float, 4>(c, Rs, eflag); break;
-        case 6: st = dbl ? pme_forces_t<double, 6>(c, Rs, eflag) : pme_forces_t<float, 6>(c, Rs, eflag); break;
-        case 8: st = dbl ? pme_forces_t<double, 8>(c, Rs, eflag) : pme_forces_t<float, 8>(c, Rs, eflag); break;
+        case 4: st = dbl ? pme_forces_t<double, 4>(c, Rs, eflag, f_store) : pme_forces_t<float, 4>(c, Rs, eflag, f_store); break;
+        case 6: st = dbl ? pme_forces_t<double, 6>(c, Rs, eflag, f_store) : pme_forces_t<float, 6>(c, Rs, eflag, f_store); break;
+        case 8: st = dbl ? pme_forces_t<double, 8>(c, Rs, eflag, f_store) : pme_forces_t<float, 8>(c, Rs, eflag, f_store); break;
         default: return SIMOX_E_ARG;
     }
     if (st) return st;

@@ -89,7 +89,10 @@ struct Profile {
 
 struct simox_ctx {
     int device = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;      // the stream every entry point issues on
+    cudaStream_t side = nullptr;        // md_run: PME overlapped with the pair passes
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    double* f_rec = nullptr;            // reciprocal forces of the overlapped PME (original order)
     simox_setup setup{};
     simox_potential pot{};
     int n = 0, cap = 0;
@@ -251,7 +254,8 @@ int pair_forces(simox_ctx* c, bool eflag, bool rdf);
 int pme_setup(simox_ctx* c);
 int pme_free(simox_ctx* c);
 int pme_self(simox_ctx* c);
-int pme_forces(simox_ctx* c, bool finalize, bool eflag);
+int pme_forces(simox_ctx* c, bool finalize, bool eflag, double* f_store = nullptr);
+void pme_bind_stream(simox_ctx* c);
 int pme_potential(simox_ctx* c, const double* charges_sorted, double* phi_out, double scale);
 int pme_finalize_forces(simox_ctx* c);
 // ctip.cu
@@ -259,8 +263,8 @@ int ctip_solve(simox_ctx* c, int max_cg, simox_ctip_report* rep);
 int ctip_alloc(simox_ctx* c);
 // integrate.cu
 int vv1(simox_ctx* c, double dt, bool reflect);
-int vv2(simox_ctx* c, double dt, bool subtract_mean);
-int nvt2_berend(simox_ctx* c, double dt, double T_given, bool subtract_mean);
+int vv2(simox_ctx* c, double dt, bool subtract_mean, const double* f_add = nullptr);
+int nvt2_berend(simox_ctx* c, double dt, double T_given, bool subtract_mean, const double* f_add = nullptr);
 int update_masses(simox_ctx* c);
 // md
 int md_run(simox_ctx* c, const simox_md_opts* o, int first, int nsteps, simox_energies* e, int* rdf);
