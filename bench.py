@@ -190,6 +190,26 @@ def equilibrated_context(s, precision, device=0):
     return g
 
 
+def force_error(s, device=0):
+    """Mixed-precision FORCE + PME forces against the all-FP64 path on the
+    same input: ||F_mixed - F_fp64|| / ||F_fp64|| over all components, and
+    the largest per-atom |dF| relative to the RMS atom force."""
+    from simox_b200 import api
+    out = {}
+    for prec in ("fp64", "mixed"):
+        with api.from_system(s, precision=prec, device=device) as g:
+            g.pme_self()
+            g.cell_sort()
+            g.force(energies=False)
+            g.pme(energies=False)
+            out[prec] = g.get_state()["f"]
+    d = out["mixed"] - out["fp64"]
+    nrm = np.linalg.norm(out["fp64"])
+    frms = nrm / np.sqrt(s.n)
+    return {"rel_norm": float(np.linalg.norm(d) / nrm),
+            "max_atom_rel_rms": float(np.linalg.norm(d, axis=1).max() / frms)}
+
+
 def run_md(g, s, first, nsteps, rdf):
     from simox_b200 import systems as S
     return g.md_run(nsteps, 1.0 / S.TFM, first_step=first, thermostat=True, T_given=600.0 * S.KB,
@@ -399,6 +419,8 @@ def main():
         ms64 = reduce_max(dist, ms64, device)
         fp64 = {"value": world * s.n * args.steps / (ms64 / 1e3), "unit": UNIT, "ms_per_step": ms64 / args.steps}
 
+    ferr = force_error(s, device=local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         el = cpu_baseline_sample(s)
@@ -420,6 +442,7 @@ def main():
                        "mean_neighbours": round(nnb, 1), "max_neighbours": mx_nnb},
             "fp64": fp64,
             "mixed_over_fp64": (value / fp64["value"]) if fp64 else None,
+            "force_err_vs_fp64": ferr,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
             "gpu_launches": launches,
             "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -15,6 +15,7 @@
 // Precision: R = double (FP64 path) or float (mixed path: per-pair terms in
 // FP32 from an FP64 separation; per-atom sums, energies in FP64).
 #include "simox_internal.cuh"
+#include "simox_packed.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -579,110 +580,248 @@ __device__ __forceinline__ void force_group(const PairParams& P, const PairTab<R
     }
 }
 
-// Skin-mode FP32 force pass.  The separation comes from the force records,
-// x_X - x_Y = off_X - off_Y - o * Lcs (o: the entry's stencil position), so
-// no FP64 minimum image is needed; each lane sums its share of f_X in
-// compensated FP32 (hi + lo, Knuth's two-sum), and the lanes' sums are added
-// in FP64.  Needs one non-oxygen species (the partner species of every group
-// is then fixed) and no energies.
-__device__ __forceinline__ void two_sum_acc(float& hi, float& lo, float b) {
-    const float s = hi + b;
-    const float bp = s - hi;
-    const float ap = s - bp;
-    lo += (hi - ap) + (b - bp);
-    hi = s;
-}
-
-// The four species-pair tables of a one-metal system travel as kernel
-// parameters (constant bank): (metal, metal), (metal, O), (O, metal), (O, O).
-constexpr int kRecBlocks = 5;   // resident 256-thread CTAs per SM (<= 48 registers)
-
-struct RecParams32 {
-    float a, two_a_sqrtpi, kc, inv_dr;
-    float4 sh[kEntries];
-    PairTab<float> tab[4];
+// Skin-mode FP32 force pass (one metal species plus oxygen, no energies).
+//
+// The separation comes from the force records, x_X - x_Y = off_X - off_Y -
+// o * Lcs (o: the entry's stencil position), so no FP64 minimum image is
+// needed.  Each thread evaluates two entries of X's row at once (entries k and
+// k + 32 of a 64-entry batch) as the halves of packed FP32 values, so every
+// FP32 step of the pair function is one FFMA2/FMUL2/FADD2 for both
+// (simox_packed.cuh).  The pair function is force.f90:81-98 and 101-140 with
+// the constants folded per species pair (PackTab); each lane sums its share
+// of f_X in compensated FP32 (hi + lo, TwoSum) and the lanes' sums are added
+// in FP64.
+//
+// Zhou term w(r) = Amp exp(-c (r/re - 1)) / (1 + (r/re - lam)^20) (eam.f90:16-31):
+//   t = r ire + nlam, w = 2^(k1 r + k0) / (1 + t^20) with k0 = c log2(e) + log2|Amp|,
+//   -dw/dr = w (m20 q + mc), q = t^19 / (1 + t^20), m20 = 20 s ire, mc = s c ire,
+// s = sign(Amp).  Two terms share one reciprocal: 1/a = b / (ab), 1/b = a / (ab)
+// (a, b <= 1 + 2e10 for r < Rcut = 10 A with the reference parameters).
+struct ZhouC {
+    float ire, nlam, k1, k0, m20, mc;
 };
 
-template <bool SAME, bool MHOMO, bool RDF, int TI>
-__device__ __forceinline__ void force_group_rec(const PairParams& P, const RecParams32& Q,
-                                                const float4* ssh, const unsigned* row, int g, int mg, int lane,
-                                                const float4& ra, int sX, int sY, float dFX,
-                                                const float4* __restrict__ frec, const float* __restrict__ dF_f,
-                                                float (&fh)[3], float (&fl)[3], int* hist) {
-    constexpr int NB = SIMOX_NRDF + 2;
-    unsigned ent_n = 0;
-    float4 rb_n = make_float4(0.f, 0.f, 0.f, 0.f);
-    float dFY_n = 0.f;
-    if (lane < mg) {
-        ent_n = row[row_slot(g, lane, P.cap)];
-        rb_n = frec[ent_n & kIdxMask];
-        dFY_n = dF_f[ent_n & kIdxMask];
-    }
-    for (int k = lane; k < mg; k += 32) {
-        const unsigned ent = ent_n;
-        const float4 rb = rb_n;
-        const float dFY = dFY_n;
-        if (k + 32 < mg) {
-            ent_n = row[row_slot(g, k + 32, P.cap)];
-            rb_n = frec[ent_n & kIdxMask];
-            dFY_n = dF_f[ent_n & kIdxMask];
+struct PackTab {
+    ZhouC D, E, A, B;        // density at X from Y, density at Y from X, pair terms A and -B
+    float cB;                // same-metal pairs: -B / fe (the B term has the density's shape)
+    float ex1x, ex1y;        // -2 xi_X log2(e), -2 xi_Y log2(e)
+    float txx, txy, x2x, x2y;  // 2 xi_X, 2 xi_Y, 2 xi_X^2, 2 xi_Y^2
+    float Qx[5], Qy0, Qy3, Qy4;
+    float kcZX, kcZY;        // kc Z_X, kc Z_Y
+};
+
+
+struct PackParams {
+    float pa, na2l, tas, kc, inv_dr;   // p a, -a^2 log2(e), 2a/sqrt(pi), kc, 1/dr
+    int cap;
+    float4 sh[kEntries];
+    PackTab tab[4];          // (metal, metal), (metal, O), (O, metal), (O, O)
+};
+
+__device__ __forceinline__ void zhou_parts(v2 r, const ZhouC& z, v2& t19, v2& den, v2& ex) {
+    const v2 t = fma2(r, bc(z.ire), bc(z.nlam));
+    const v2 t2 = t * t;
+    const v2 t3 = t2 * t;
+    const v2 t4 = t2 * t2;
+    const v2 t8 = t4 * t4;
+    const v2 t16 = t8 * t8;
+    t19 = t16 * t3;
+    den = fma2(t19, t, bc(1.f));
+    ex = ex2(fma2(r, bc(z.k1), bc(z.k0)));
+}
+// -dw/dr given u = 1/den
+__device__ __forceinline__ v2 zhou_nd(const ZhouC& z, v2 t19, v2 u, v2 ex) {
+    const v2 w = ex * u;
+    return w * fma2(t19 * u, bc(z.m20), bc(z.mc));
+}
+
+// f/r of one pair for the X-Y pair kind of T (force.f90:81-98, 101-140)
+template <bool SAME, bool MHOMO>
+__device__ __forceinline__ v2 pair_fs_pk(const PackTab& T, const PackParams& Q, v2 r2, v2 qb, v2 dFY, float dFX,
+                                         float kcqa, float kcqaZY) {
+    const v2 ir = rsqrt(r2);
+    const v2 r = r2 * ir;
+    const v2 ir2 = ir * ir;
+    v2 eam;
+    if (MHOMO) {
+        v2 t19D, denD, exD, t19A, denA, exA;
+        zhou_parts(r, T.D, t19D, denD, exD);
+        zhou_parts(r, T.A, t19A, denA, exA);
+        const v2 R = rcp(denD * denA);
+        const v2 nD = zhou_nd(T.D, t19D, denA * R, exD);
+        const v2 nA = zhou_nd(T.A, t19A, denD * R, exA);
+        eam = fma2(dFY + bc(dFX + T.cB), nD, nA);
+    } else {
+        v2 t19A, denA, exA, t19B, denB, exB, t19D, denD, exD;
+        zhou_parts(r, T.A, t19A, denA, exA);
+        zhou_parts(r, T.B, t19B, denB, exB);
+        const v2 R = rcp(denA * denB);
+        eam = zhou_nd(T.A, t19A, denB * R, exA) + zhou_nd(T.B, t19B, denA * R, exB);
+        zhou_parts(r, T.D, t19D, denD, exD);
+        if (SAME) {
+            eam = fma2(dFY + bc(dFX), zhou_nd(T.D, t19D, rcp(denD), exD), eam);
+        } else {
+            v2 t19E, denE, exE;
+            zhou_parts(r, T.E, t19E, denE, exE);
+            const v2 S = rcp(denD * denE);
+            eam = fma2(bc(dFX), zhou_nd(T.D, t19D, denE * S, exD), eam);
+            eam = fma2(dFY, zhou_nd(T.E, t19E, denD * S, exE), eam);
         }
-        const float4 o = ssh[(ent >> kSkinCodeShift) & kCodeMask];
-        const float dx = (ra.x - rb.x) - o.x, dy = (ra.y - rb.y) - o.y, dz = (ra.z - rb.z) - o.z;
-        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        const float ir = rsqrtf(r2), r = r2 * ir;
-        float erfcv;
-        double ep, ed, ec;
-        const float fs = pair_fs<float, SAME, MHOMO, false>(Q.tab[TI], r, ir, ra.w, rb.w, dFX, dFY, Q.a,
-                                                           Q.two_a_sqrtpi, Q.kc, erfcv, ep, ed, ec);
-        two_sum_acc(fh[0], fl[0], fs * dx);
-        two_sum_acc(fh[1], fl[1], fs * dy);
-        two_sum_acc(fh[2], fl[2], fs * dz);
-        if (RDF && (ent & kIsA)) {
-            const int bin = min(max((int)(r * Q.inv_dr), 0), NB - 1);
-            atomicAdd(&hist[(sX + kSpecies * sY) * NB + bin], 2);
+    }
+    // Ewald real space: kc qa qb (2a/sqrt(pi) r e^{-a^2 r^2} + erfc(a r)) / r^3
+    const v2 kq = bc(kcqa) * qb;
+    const v2 tt = rcp(fma2(r, bc(Q.pa), bc(1.f)));
+    const v2 ez2 = ex2(r2 * bc(Q.na2l));
+    const v2 ew = (kq * ez2) * (fma2(r, bc(Q.tas), tt * erfc_poly(tt)) * ir2);
+    // CTIP Slater-1s terms
+    const v2 eX = ex2(r * bc(T.ex1x));
+    const v2 djfi = eX * fma2(fma2(r, bc(T.txx), bc(1.f)), ir2, bc(T.x2x));
+    v2 ct;
+    if (SAME) {
+        const v2 QX = fma2(r, fma2(r, bc(T.Qx[2]), bc(T.Qx[1])), bc(T.Qx[0])) + ir * fma2(ir, bc(T.Qx[4]), bc(T.Qx[3]));
+        const v2 dfifj = eX * QX;
+        ct = fma2(qb, bc(T.kcZX), bc(kcqaZY)) * (dfifj - djfi) - kq * dfifj;
+    } else {
+        const v2 eY = ex2(r * bc(T.ex1y));
+        const v2 difj = eY * fma2(fma2(r, bc(T.txy), bc(1.f)), ir2, bc(T.x2y));
+        v2 dfifj = eX * fma2(ir, fma2(ir, bc(T.Qx[4]), bc(T.Qx[3])), bc(T.Qx[0]));
+        dfifj = fma2(eY, fma2(ir, fma2(ir, bc(T.Qy4), bc(T.Qy3)), bc(T.Qy0)), dfifj);
+        ct = fma2(bc(kcqaZY), dfifj - djfi, (qb * bc(T.kcZX)) * (dfifj - difj)) - kq * dfifj;
+    }
+    return ((eam + ew) + ct) * ir;
+}
+
+// Per-thread asynchronous copies global -> shared (cp.async, PTX ISA): the
+// partner records of later batches are in flight while a batch is computed,
+// without holding registers.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Cell-tiled force pass.  Atoms are in skin-cell order, and every entry of a
+// row names its partner's cell by the stencil position e (0..26) relative to
+// the atom's own cell.  One CTA takes the atoms of one skin cell (or a part
+// of it) and first copies the records and F' of the 27 cells around it into
+// shared memory (cp.async); a row entry then resolves with one table lookup
+// (the stencil shift o_e * Lcs and the index delta of cell e's tile) and two
+// shared loads.  A neighbourhood larger than the tile reads the same data
+// from global memory instead.
+constexpr int kTileThreads = 256;
+constexpr int kTileBlocks = 2;             // resident CTAs per SM (tile ~110 KB each)
+constexpr int kTileCap = 5500;             // records per tile (16 B record + 4 B F')
+constexpr int kSelfEntry = 13;             // stencil position (0, 0, 0)
+
+template <bool SAME, bool MHOMO, bool RDF, bool TILED, int TI>
+__device__ __forceinline__ void force_batch_tile(const PackParams& Q, const float4* etab, const float4* __restrict__ rsrc,
+                                                 const float* __restrict__ dsrc, int total, unsigned E1, unsigned E2,
+                                                 bool v1, bool v2ok, const float4& ra, float dFX, int hbase,
+                                                 v2 (&fh)[3], v2 (&fl)[3], int* hist) {
+    constexpr int NB = SIMOX_NRDF + 2;
+    const PackTab& T = Q.tab[TI];
+    const float kcqa = Q.kc * ra.w;
+    const float kcqaZY = T.kcZY * ra.w;
+    const float4 t1 = etab[(E1 >> kSkinCodeShift) & kCodeMask];
+    const float4 t2 = etab[(E2 >> kSkinCodeShift) & kCodeMask];
+    int i1 = (int)(E1 & kIdxMask) + __float_as_int(t1.w);
+    int i2 = (int)(E2 & kIdxMask) + __float_as_int(t2.w);
+    if (TILED) {   // keep every shared load inside the tile
+        i1 = (unsigned)i1 < (unsigned)total ? i1 : 0;
+        i2 = (unsigned)i2 < (unsigned)total ? i2 : 0;
+    }
+    const float4 B1 = rsrc[i1], B2 = rsrc[i2];
+    const float D1 = dsrc[i1], D2 = dsrc[i2];
+    const v2 dx = mk2((ra.x - B1.x) - t1.x, (ra.x - B2.x) - t2.x);
+    const v2 dy = mk2((ra.y - B1.y) - t1.y, (ra.y - B2.y) - t2.y);
+    const v2 dz = mk2((ra.z - B1.z) - t1.z, (ra.z - B2.z) - t2.z);
+    const v2 r2 = fma2(dx, dx, fma2(dy, dy, dz * dz));
+    v2 fs = pair_fs_pk<SAME, MHOMO>(T, Q, r2, mk2(B1.w, B2.w), mk2(D1, D2), dFX, kcqa, kcqaZY);
+    // slots past the end of a group evaluated a placeholder pair: drop it
+    fs = mk2(v1 ? fs.v.x : 0.f, v2ok ? fs.v.y : 0.f);
+    two_sum2(fh[0], fl[0], fs * dx);
+    two_sum2(fh[1], fl[1], fs * dy);
+    two_sum2(fh[2], fl[2], fs * dz);
+    if (RDF) {
+        // INT(r/dr) of the pair's FP32 distance, counted once, by the reference's i
+        if (E1 & kIsA) {
+            const float r = r2.v.x * rsqrt_approx(r2.v.x);
+            atomicAdd(&hist[hbase + min(max((int)(r * Q.inv_dr), 0), NB - 1)], 2);
+        }
+        if (E2 & kIsA) {
+            const float r = r2.v.y * rsqrt_approx(r2.v.y);
+            atomicAdd(&hist[hbase + min(max((int)(r * Q.inv_dr), 0), NB - 1)], 2);
         }
     }
 }
 
-template <bool RDF>
-__global__ void __launch_bounds__(256, kRecBlocks)
-    force_rec_kernel(PairParams P, const __grid_constant__ RecParams32 Q, const float4* __restrict__ frec, const int* __restrict__ ts, const int2* __restrict__ nn,
-                     const unsigned* __restrict__ nbr, const float* __restrict__ dF_f, const int* __restrict__ sorted,
-                     int g0, double* __restrict__ f, int* __restrict__ rdf, int* __restrict__ status) {
-    __shared__ float4 ssh[kEntries];
+// The atoms [b0, b1) of one CTA, one warp per atom (taken from a shared
+// counter), two row entries per lane per batch, the next batch's entries
+// loaded before this batch's arithmetic.
+template <bool RDF, bool TILED>
+__device__ __forceinline__ void force_tile_atoms(const PackParams& Q, const float4* etab, const float4* __restrict__ rsrc,
+                                                 const float* __restrict__ dsrc, int total, int b0, int b1, int* next,
+                                                 const float4* __restrict__ frec, const int* __restrict__ ts,
+                                                 const int2* __restrict__ nn, const unsigned* __restrict__ nbr,
+                                                 const float* __restrict__ dF_f, const int* __restrict__ sorted, int g0,
+                                                 double* __restrict__ f, int* hist, int& bad) {
     constexpr int NB = SIMOX_NRDF + 2;
-    __shared__ int hist[RDF ? kSpecies * kSpecies * NB : 1];
-    for (int k = threadIdx.x; k < kEntries; k += blockDim.x) ssh[k] = Q.sh[k];
-    if (RDF)
-        for (int k = threadIdx.x; k < kSpecies * kSpecies * NB; k += blockDim.x) hist[k] = 0;
-    __syncthreads();
     const int lane = threadIdx.x & 31;
-    const int wpb = blockDim.x >> 5;
-    int bad = 0;
-    for (int X = blockIdx.x * wpb + (threadIdx.x >> 5); X < P.n; X += gridDim.x * wpb) {
+    const int cap = Q.cap;
+    for (;;) {
+        int X = 0;
+        if (lane == 0) X = atomicAdd(next, 1);
+        X = __shfl_sync(0xffffffffu, X, 0) + b0;
+        if (X >= b1) break;
         const float4 ra = frec[X];
         const int sX = ts[X];
         const float dFX = dF_f[X];
         const int2 m = nn[X];
-        const unsigned* row = nbr + (size_t)X * P.cap;
-        float fh[3] = {0.f, 0.f, 0.f}, fl[3] = {0.f, 0.f, 0.f};
-        if (sX == g0) {          // metal X: metal partners (its own species) then oxygen
-            force_group_rec<true, true, RDF, 0>(P, Q, ssh, row, 0, m.x, lane, ra, sX, g0, dFX, frec, dF_f, fh, fl,
-                                                hist);
-            force_group_rec<false, false, RDF, 1>(P, Q, ssh, row, 1, m.y, lane, ra, sX, 3, dFX, frec, dF_f, fh, fl,
-                                                  hist);
-        } else if (sX == 3) {    // oxygen X: metal partners then oxygen
-            force_group_rec<false, false, RDF, 2>(P, Q, ssh, row, 0, m.x, lane, ra, 3, g0, dFX, frec, dF_f, fh, fl,
-                                                  hist);
-            force_group_rec<true, false, RDF, 3>(P, Q, ssh, row, 1, m.y, lane, ra, 3, 3, dFX, frec, dF_f, fh, fl,
-                                                 hist);
-        } else if (m.x + m.y > 0) {
-            bad |= ST_UNKNOWN_PAIR;
+        const unsigned* row = nbr + (size_t)X * cap;
+        v2 fh[3] = {bc(0.f), bc(0.f), bc(0.f)}, fl[3] = {bc(0.f), bc(0.f), bc(0.f)};
+        const bool metal = sX == g0;
+        if (!metal && sX != 3) {
+            if (m.x + m.y > 0) bad |= ST_UNKNOWN_PAIR;
+        } else {
+            // one stream of 64-entry batches over both groups: metal partners
+            // (row[k]) then oxygen partners (row[cap - 1 - k])
+            const int nb0 = (m.x + 63) >> 6, nb = nb0 + ((m.y + 63) >> 6);
+            const unsigned pad = ((unsigned)kSelfEntry << kSkinCodeShift) | (unsigned)X;   // an in-tile placeholder
+            auto load = [&](int j, unsigned& a, unsigned& b) {
+                const bool g1 = j >= nb0;
+                const int kb = (g1 ? j - nb0 : j) << 6, mg = g1 ? m.y : m.x;
+                const unsigned* p = g1 ? row + (cap - 1 - kb - lane) : row + kb + lane;
+                const int dir = g1 ? -32 : 32;
+                a = kb + lane < mg ? p[0] : pad;
+                b = kb + 32 + lane < mg ? p[dir] : pad;
+            };
+            unsigned na = pad, nbE = pad;
+            if (nb > 0) load(0, na, nbE);
+            for (int j = 0; j < nb; j++) {
+                const unsigned E1 = na, E2 = nbE;
+                if (j + 1 < nb) load(j + 1, na, nbE);
+                const bool g1 = j >= nb0;
+                const int kb = (g1 ? j - nb0 : j) << 6, mg = g1 ? m.y : m.x;
+                const bool v1 = kb + lane < mg, v2ok = kb + 32 + lane < mg;
+                const int hb = ((metal ? 0 : 2) + (g1 ? 1 : 0)) * NB;
+                if (metal) {
+                    if (!g1) force_batch_tile<true, true, RDF, TILED, 0>(Q, etab, rsrc, dsrc, total, E1, E2, v1, v2ok, ra, dFX, hb, fh, fl, hist);
+                    else force_batch_tile<false, false, RDF, TILED, 1>(Q, etab, rsrc, dsrc, total, E1, E2, v1, v2ok, ra, dFX, hb, fh, fl, hist);
+                } else {
+                    if (!g1) force_batch_tile<false, false, RDF, TILED, 2>(Q, etab, rsrc, dsrc, total, E1, E2, v1, v2ok, ra, dFX, hb, fh, fl, hist);
+                    else force_batch_tile<true, false, RDF, TILED, 3>(Q, etab, rsrc, dsrc, total, E1, E2, v1, v2ok, ra, dFX, hb, fh, fl, hist);
+                }
+            }
         }
-        double fx = (double)fh[0] + (double)fl[0];
-        double fy = (double)fh[1] + (double)fl[1];
-        double fz = (double)fh[2] + (double)fl[2];
+        double fx = ((double)fh[0].v.x + (double)fl[0].v.x) + ((double)fh[0].v.y + (double)fl[0].v.y);
+        double fy = ((double)fh[1].v.x + (double)fl[1].v.x) + ((double)fh[1].v.y + (double)fl[1].v.y);
+        double fz = ((double)fh[2].v.x + (double)fl[2].v.x) + ((double)fh[2].v.y + (double)fl[2].v.y);
         fx = warp_sum(fx);
         fy = warp_sum(fy);
         fz = warp_sum(fz);
@@ -693,18 +832,150 @@ __global__ void __launch_bounds__(256, kRecBlocks)
             f[3 * o + 2] = fz;
         }
     }
+}
+
+template <bool RDF>
+__global__ void __launch_bounds__(kTileThreads, kTileBlocks)
+    force_tile_kernel(const __grid_constant__ PackParams Q, int splits, const int* __restrict__ cs_start,
+                      const int* __restrict__ cs_entries, const float4* __restrict__ frec,
+                      const int* __restrict__ ts, const int2* __restrict__ nn, const unsigned* __restrict__ nbr,
+                      const float* __restrict__ dF_f, const int* __restrict__ sorted, int g0,
+                      double* __restrict__ f, int* __restrict__ rdf, int* __restrict__ status) {
+    extern __shared__ __align__(16) unsigned char tile_smem[];
+    float4* trec = reinterpret_cast<float4*>(tile_smem);
+    float* tdf = reinterpret_cast<float*>(trec + kTileCap);
+    __shared__ float4 etab[kEntries];          // o_e * Lcs (x, y, z) and tile index delta (w)
+    __shared__ int eoff[kEntries + 1], estart[kEntries];
+    __shared__ int next;
+    constexpr int NB = SIMOX_NRDF + 2;
+    __shared__ int hist[RDF ? 4 * NB : 1];     // (metal, O) x (metal, O) partner kinds
+    const int cell = blockIdx.x / splits, part = blockIdx.x - cell * splits;
+    const int tid = threadIdx.x;
+    if (tid < kEntries) {
+        const int nc = cs_entries[cell * kEntries + tid];
+        const int s0 = cs_start[nc];
+        estart[tid] = s0;
+        eoff[tid + 1] = cs_start[nc + 1] - s0;
+    }
+    if (tid == 0) {
+        eoff[0] = 0;
+        next = 0;
+    }
+    if (RDF)
+        for (int k = tid; k < 4 * NB; k += kTileThreads) hist[k] = 0;
+    __syncthreads();
+    if (tid == 0)
+        for (int e = 0; e < kEntries; e++) eoff[e + 1] += eoff[e];
+    __syncthreads();
+    const int total = eoff[kEntries];
+    const bool tiled = total <= kTileCap;
+    if (tid < kEntries) {
+        const float4 o = Q.sh[tid];
+        etab[tid] = make_float4(o.x, o.y, o.z, __int_as_float(tiled ? eoff[tid] - estart[tid] : 0));
+    }
+    if (tiled) {
+        int e = 0;
+        for (int i = tid; i < total; i += kTileThreads) {
+            while (eoff[e + 1] <= i) e++;
+            const int src = estart[e] + (i - eoff[e]);
+            cp_async16(&trec[i], frec + src);
+            cp_async4(&tdf[i], dF_f + src);
+        }
+        cp_async_commit();
+        cp_async_wait<0>();
+    }
+    __syncthreads();
+    const int a0 = cs_start[cell], na = cs_start[cell + 1] - a0;
+    const int b0 = a0 + (int)((long long)na * part / splits);
+    const int b1 = a0 + (int)((long long)na * (part + 1) / splits);
+    int bad = 0;
+    if (tiled)
+        force_tile_atoms<RDF, true>(Q, etab, trec, tdf, total, b0, b1, &next, frec, ts, nn, nbr, dF_f, sorted, g0, f,
+                                    hist, bad);
+    else
+        force_tile_atoms<RDF, false>(Q, etab, frec, dF_f, total, b0, b1, &next, frec, ts, nn, nbr, dF_f, sorted, g0,
+                                     f, hist, bad);
     if (bad) atomicOr(status, bad);
     if (RDF) {
         __syncthreads();
-        for (int k = threadIdx.x; k < kSpecies * kSpecies * NB; k += blockDim.x) {
-            int v = hist[k];
+        for (int k = tid; k < 4 * NB; k += kTileThreads) {
+            const int v = hist[k];
             if (v) {
-                int pr = k / NB, bin = k % NB;
-                int si = pr % kSpecies, sj = pr / kSpecies;
+                const int pr = k / NB, bin = k - pr * NB;
+                const int si = pr >= 2 ? 3 : g0, sj = (pr & 1) ? 3 : g0;
                 atomicAdd(&rdf[si + 5 * sj + 25 * bin], v);
             }
         }
     }
+}
+
+// host: folded constants of the packed pair function for species X, Y
+static ZhouC zhou_const(double amp, double re, double c, double lam) {
+    const double L2E = 1.4426950408889634;
+    const double s = amp < 0.0 ? -1.0 : 1.0;
+    ZhouC z;
+    z.ire = (float)(1.0 / re);
+    z.nlam = (float)(-lam);
+    z.k1 = (float)(-c * L2E / re);
+    z.k0 = amp != 0.0 ? (float)(c * L2E + std::log2(std::fabs(amp))) : -INFINITY;
+    z.m20 = (float)(20.0 * s / re);
+    z.mc = (float)(s * c / re);
+    return z;
+}
+
+static PackTab pack_tab(const simox_potential& P, int X, int Y) {
+    PackTab t;
+    std::memset(&t, 0, sizeof(t));
+    const bool mX = X < 3, mY = Y < 3;
+    const simox_oxid& o = P.oxygn;
+    auto dens = [&](int at, int from) {
+        if (from < 3) {
+            const simox_metl& e = P.eam[from];
+            return zhou_const(e.f_e, e.r_e, e.beta, e.lambda);
+        }
+        const double re = at < 3 ? o.r_e[at] : o.r_e[3];     // eam.f90:196 / 297
+        return zhou_const(o.fe, re, o.gamm, o.nu);
+    };
+    t.D = dens(X, Y);
+    t.E = dens(Y, X);
+    if (mX && mY) {                                          // METAL_HOMO eam.f90:29
+        const simox_metl& e = P.eam[X];
+        t.A = zhou_const(e.A, e.r_e, e.alpha, e.kappa);
+        t.B = zhou_const(-e.B, e.r_e, e.beta, e.lambda);
+        t.cB = (float)(-e.B / e.f_e);
+    } else {                                                 // METAL_OXYGEN / OXYGEN_ONLY
+        const int m = mX ? X : (mY ? Y : 3);
+        t.A = zhou_const(o.A[m], o.r_e[m], o.alph[m], o.kapp[m]);
+        t.B = zhou_const(-o.B[m], o.r_e[m], o.beta[m], o.lamb[m]);
+    }
+    const double L2E = 1.4426950408889634;
+    const simox_potn& pX = P.param[X];
+    const simox_potn& pY = P.param[Y];
+    t.ex1x = (float)(-2.0 * pX.xi * L2E);
+    t.ex1y = (float)(-2.0 * pY.xi * L2E);
+    t.txx = (float)(2.0 * pX.xi);
+    t.txy = (float)(2.0 * pY.xi);
+    t.x2x = (float)(2.0 * pX.xi * pX.xi);
+    t.x2y = (float)(2.0 * pY.xi * pY.xi);
+    t.kcZX = (float)(SX_KC * pX.Z);
+    t.kcZY = (float)(SX_KC * pY.Z);
+    const double* f = pX.fafb[Y];
+    if (X == Y) {       // force.f90:111-118
+        const double xi = pX.xi;
+        t.Qx[0] = (float)(2 * xi * f[1] - f[2]);
+        t.Qx[1] = (float)(2 * xi * f[2] - 2 * f[3]);
+        t.Qx[2] = (float)(2 * xi * f[3]);
+        t.Qx[3] = (float)(2 * xi);
+        t.Qx[4] = 1.f;
+    } else {            // force.f90:130-133
+        t.Qx[0] = (float)(2 * pX.xi * f[0]);
+        t.Qx[3] = (float)(2 * pX.xi * f[2]);
+        t.Qx[4] = (float)f[2];
+        t.Qy0 = (float)(2 * pY.xi * f[1]);
+        t.Qy3 = (float)(2 * pY.xi * f[3]);
+        t.Qy4 = (float)f[3];
+    }
+    return t;
 }
 
 // pass 2 -------------------------------------------------------------------
@@ -931,33 +1202,56 @@ static void launch_force(simox_ctx* c, const PairTab<R>* tab, bool eflag, bool r
                                                                        c->pair_order, c->f, c->acc, c->rdf, c->status);
 }
 
+static constexpr size_t kTileSmem = (size_t)kTileCap * (sizeof(float4) + sizeof(float));
+
+// dynamic shared memory of the tiled force pass, once per device
+static int tile_prepare(int device) {
+    static bool done[64] = {};
+    if (device >= 0 && device < 64 && done[device]) return SIMOX_OK;
+    const int b = (int)kTileSmem;
+    cudaError_t e1 = cudaFuncSetAttribute(force_tile_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    cudaError_t e2 = cudaFuncSetAttribute(force_tile_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    cudaError_t e3 = cudaFuncSetAttribute(force_tile_kernel<true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                          cudaSharedmemCarveoutMaxShared);
+    cudaError_t e4 = cudaFuncSetAttribute(force_tile_kernel<false>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                          cudaSharedmemCarveoutMaxShared);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess || e4 != cudaSuccess) return SIMOX_E_CUDA;
+    if (device >= 0 && device < 64) done[device] = true;
+    return SIMOX_OK;
+}
+
 int pair_forces(simox_ctx* c, bool eflag, bool rdf) {
     if (!c->eam_valid) return SIMOX_E_STATE;
     if (c->n == 0) return SIMOX_OK;
     if (!use_fp64(c, eflag) && c->using_skin && c->g0_species >= 0) {
         Launch L(c, "pair_force");
         PairParams P = pair_params(c);
-        RecParams32 Q;
-        Q.a = (float)P.a;
-        Q.two_a_sqrtpi = (float)(2.0 * P.a / SX_SQRTPI);
+        if (int st = tile_prepare(c->device)) return st;
+        PackParams Q;
+        std::memset(&Q, 0, sizeof(Q));
+        Q.pa = (float)(kErfcP * P.a);
+        Q.na2l = (float)(-P.a * P.a * 1.4426950408889634);
+        Q.tas = (float)(2.0 * P.a / SX_SQRTPI);
         Q.kc = (float)P.kc;
         Q.inv_dr = (float)(1.0 / P.dr_rdf);
+        Q.cap = P.cap;
         stencil_shifts(c, Q.sh);
         const int g0 = c->g0_species;
-        const PairTab<float>* h = c->h_tab_f;
-        Q.tab[0] = h[g0 * kSpecies + g0];
-        Q.tab[1] = h[g0 * kSpecies + 3];
-        Q.tab[2] = h[3 * kSpecies + g0];
-        Q.tab[3] = h[3 * kSpecies + 3];
-        const int g = std::max(1, std::min((c->n + 7) / 8, num_sms(c) * kRecBlocks * 2));
+        Q.tab[0] = pack_tab(c->pot, g0, g0);
+        Q.tab[1] = pack_tab(c->pot, g0, 3);
+        Q.tab[2] = pack_tab(c->pot, 3, g0);
+        Q.tab[3] = pack_tab(c->pot, 3, 3);
+        const int splits = 2;
+        const int g = c->ncell_s * splits;
+        const int2* nn = reinterpret_cast<const int2*>(c->nn);
         if (rdf)
-            force_rec_kernel<true><<<g, 256, 0, c->stream>>>(P, Q, c->frec_s, c->t_s,
-                                                             reinterpret_cast<const int2*>(c->nn), c->nbr, c->dF_f,
-                                                             c->pair_order, c->g0_species, c->f, c->rdf, c->status);
+            force_tile_kernel<true><<<g, kTileThreads, kTileSmem, c->stream>>>(
+                Q, splits, c->cs_start, c->cs_entries, c->frec_s, c->t_s, nn, c->nbr, c->dF_f, c->pair_order, g0,
+                c->f, c->rdf, c->status);
         else
-            force_rec_kernel<false><<<g, 256, 0, c->stream>>>(P, Q, c->frec_s, c->t_s,
-                                                              reinterpret_cast<const int2*>(c->nn), c->nbr, c->dF_f,
-                                                              c->pair_order, c->g0_species, c->f, c->rdf, c->status);
+            force_tile_kernel<false><<<g, kTileThreads, kTileSmem, c->stream>>>(
+                Q, splits, c->cs_start, c->cs_entries, c->frec_s, c->t_s, nn, c->nbr, c->dF_f, c->pair_order, g0,
+                c->f, c->rdf, c->status);
         return check_launch(c);
     }
     Launch L(c, use_fp64(c, eflag) ? "pair_force_fp64" : "pair_force");
