@@ -1060,6 +1060,122 @@ __global__ void __launch_bounds__(ForceShape<R>::threads, ForceShape<R>::blocks)
     }
 }
 
+// FP64 energies of the mixed-precision mode (force.f90:84-98, 101-140, 256-351).
+// Per atom X (one warp) the FP64 density rho_X is summed over the whole exact
+// row and gives the embedding energy F(rho_X); the pair energies (phi, Ewald
+// real space, CTIP) are evaluated once per pair, on the side of the
+// reference's i (list bit 31).  Those entries are queued per warp in shared
+// memory and evaluated 32 at a time, so the FP64 exponentials run on full
+// warps.
+constexpr int EN_THREADS = 128;
+
+__device__ __forceinline__ void pair_energy_fp64(const PairTab<double>& T, double r, double ir, double qa, double qb,
+                                                 double a, double& ep, double& ed, double& ec) {
+    ep += T.p_A * zhou_val<double>(r, T.p_inv_re, T.p_alpha, T.p_kappa) -
+          T.p_B * zhou_val<double>(r, T.p_inv_re, T.p_beta, T.p_lambda);   // eam.f90 phi
+    ed += qa * qb * erfc(a * r) * ir;                                       // force.f90:94
+    const double eX = exp(-2.0 * T.xi_x * r), eY = exp(-2.0 * T.xi_y * r);
+    const double jfi = -eX * (T.xi_x + ir);
+    const double ifj = -eY * (T.xi_y + ir);
+    const double fifj = -eX * (T.Px[0] + r * (T.Px[1] + r * (T.Px[2] + r * T.Px[3])) + T.Px[4] * ir) -
+                        eY * (T.Py[0] + T.Py[4] * ir);
+    ec += qa * T.Z_y * (jfi - fifj) + qb * T.Z_x * (ifj - fifj) + qa * qb * fifj;   // force.f90:135-138
+}
+
+struct EnQueue {
+    double r[64];
+    double qb[64];
+    int t[64];
+};
+
+__global__ void __launch_bounds__(EN_THREADS)
+    energy_kernel(PairParams P, const PairTab<double>* __restrict__ tab, const double4* __restrict__ xq,
+                  const int* __restrict__ ts, const int2* __restrict__ nn, const unsigned* __restrict__ nbr,
+                  EmbedParams E, double* __restrict__ acc, int* __restrict__ status) {
+    __shared__ PairTab<double> st[kSpecies * kSpecies];
+    __shared__ EnQueue qu[EN_THREADS / 32];
+    __shared__ double red[EN_THREADS / 32];
+    for (int k = threadIdx.x; k < kSpecies * kSpecies; k += blockDim.x) st[k] = tab[k];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    EnQueue& Qw = qu[threadIdx.x >> 5];
+    const unsigned lt = (1u << lane) - 1u;
+    double ep = 0.0, ed = 0.0, ec = 0.0, eg = 0.0;
+    int bad = 0;
+    for (int X = blockIdx.x * wpb + (threadIdx.x >> 5); X < P.n; X += gridDim.x * wpb) {
+        const double4 xa = xq[X];
+        const int sX = ts[X];
+        const int2 m = nn[X];
+        const int mt = m.x + m.y;
+        const unsigned* row = nbr + (size_t)X * P.cap;
+        double rho = 0.0;
+        int qn = 0;   // queued pairs (warp-uniform)
+        if (sX < kSpecies) {
+            for (int base = 0; base < mt; base += 32) {
+                const int k = base + lane;
+                bool isa = false;
+                double r = 0.0, qb = 0.0;
+                int t = 0;
+                if (k < mt) {
+                    const unsigned ent = row[row_slot(2, k, P.cap, m.x)];
+                    const int Y = (int)(ent & kIdxMask);
+                    const int sY = ts[Y];
+                    if (sY < kSpecies) {
+                        const double4 xb = xq[Y];
+                        double dx, dy, dz;
+                        min_image(xa, xb, P, dx, dy, dz);
+                        r = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+                        t = sX * kSpecies + sY;
+                        const PairTab<double>& T = st[t];
+                        rho += T.d_fe * zhou_val<double>(r, T.d_inv_re, T.d_c, T.d_lam);   // force.f90:84
+                        isa = (ent & kIsA) != 0u;
+                        qb = xb.w;
+                    } else {
+                        bad |= ST_UNKNOWN_PAIR;
+                    }
+                }
+                const unsigned mk = __ballot_sync(0xffffffffu, isa);
+                if (isa) {
+                    const int pos = qn + __popc(mk & lt);
+                    Qw.r[pos] = r;
+                    Qw.qb[pos] = qb;
+                    Qw.t[pos] = t;
+                }
+                qn += __popc(mk);
+                __syncwarp();
+                if (qn >= 32) {   // a full warp of pair energies
+                    const double rr = Qw.r[lane], qq = Qw.qb[lane];
+                    const int tt = Qw.t[lane];
+                    __syncwarp();
+                    if (lane < qn - 32) {
+                        Qw.r[lane] = Qw.r[lane + 32];
+                        Qw.qb[lane] = Qw.qb[lane + 32];
+                        Qw.t[lane] = Qw.t[lane + 32];
+                    }
+                    qn -= 32;
+                    __syncwarp();
+                    pair_energy_fp64(st[tt], rr, 1.0 / rr, xa.w, qq, P.a, ep, ed, ec);
+                }
+            }
+            if (lane < qn) pair_energy_fp64(st[Qw.t[lane]], Qw.r[lane], 1.0 / Qw.r[lane], xa.w, Qw.qb[lane], P.a, ep, ed, ec);
+            __syncwarp();
+        } else if (mt > 0) {
+            bad |= ST_UNKNOWN_PAIR;
+        }
+        rho = warp_sum(rho);
+        if (lane == 0) {
+            double F, dF;
+            if (embed(E, sX, rho, F, dF)) bad |= ST_UNKNOWN_ELEMENT;
+            eg += F;
+        }
+    }
+    if (bad) atomicOr(status, bad);
+    block_add<EN_THREADS>(ep, acc, A_EPAIR, red);
+    block_add<EN_THREADS>(ed, acc, A_EDIR, red);
+    block_add<EN_THREADS>(ec, acc, A_ECTIP, red);
+    block_add<EN_THREADS>(eg, acc, A_EGROUP, red);
+}
+
 static EmbedParams embed_params(const simox_potential& P) {
     EmbedParams E;
     std::memset(&E, 0, sizeof(E));
@@ -1096,9 +1212,10 @@ static int pair_grid(simox_ctx* c) {
     return need < lim ? (need > 0 ? need : 1) : lim;
 }
 
-// In the mixed mode the energies are FP64: a pass that must produce energies
-// runs the FP64 kernels (densities, embedding, forces and energies).
-static bool use_fp64(const simox_ctx* c, bool eflag) { return c->precision == SIMOX_FP64 || eflag; }
+// Forces use the context's precision.  Energies are FP64 in both modes: the
+// FP64 context evaluates them inside its force pass, the mixed context with
+// the separate FP64 energy pass (energy_kernel) after its mixed force pass.
+static bool use_fp64(const simox_ctx* c, bool) { return c->precision == SIMOX_FP64; }
 
 int eam_density(simox_ctx* c, bool eflag) {
     int st = ensure_list(c);
@@ -1107,8 +1224,8 @@ int eam_density(simox_ctx* c, bool eflag) {
     PairParams P = pair_params(c);
     EmbedParams E = embed_params(c->pot);
     // the skin filter already produced rho and F' in the context's precision
-    if (c->rho_ready && use_fp64(c, eflag) == (c->precision == SIMOX_FP64)) {
-        if (eflag) {
+    if (c->rho_ready) {
+        if (eflag && c->precision == SIMOX_FP64) {
             Launch L(c, "eam_embed_energy");
             embed_energy_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->n, c->t_s, c->rho_s, E, c->acc);
         }
@@ -1119,7 +1236,7 @@ int eam_density(simox_ctx* c, bool eflag) {
     if (!use_fp64(c, eflag))
         density_kernel<float><<<pair_grid(c), PK_THREADS, 0, c->stream>>>(P, c->tab_f, c->xq_s, c->t_s,
                                                                          reinterpret_cast<const int2*>(c->nn), c->nbr, E,
-                                                                         c->rho_s, c->dF_s, c->dF_f, c->acc, c->status, eflag);
+                                                                         c->rho_s, c->dF_s, c->dF_f, c->acc, c->status, 0);
     else
         density_kernel<double><<<pair_grid(c), PK_THREADS, 0, c->stream>>>(P, c->tab_d, c->xq_s, c->t_s,
                                                                           reinterpret_cast<const int2*>(c->nn), c->nbr,
@@ -1220,9 +1337,32 @@ static int tile_prepare(int device) {
     return SIMOX_OK;
 }
 
+static int energy_pass(simox_ctx* c) {
+    Launch L(c, "pair_energy_fp64");
+    const int wpb = EN_THREADS / 32;
+    const int g = std::max(1, std::min((c->n + wpb - 1) / wpb, num_sms(c) * 12));
+    energy_kernel<<<g, EN_THREADS, 0, c->stream>>>(pair_params(c), c->tab_d, c->xq_s, c->t_s,
+                                                  reinterpret_cast<const int2*>(c->nn), c->nbr, embed_params(c->pot),
+                                                  c->acc, c->status);
+    return check_launch(c);
+}
+
+static int mixed_forces(simox_ctx* c, bool rdf);
+
 int pair_forces(simox_ctx* c, bool eflag, bool rdf) {
     if (!c->eam_valid) return SIMOX_E_STATE;
     if (c->n == 0) return SIMOX_OK;
+    if (c->precision != SIMOX_FP64) {
+        if (int st = mixed_forces(c, rdf)) return st;
+        return eflag ? energy_pass(c) : SIMOX_OK;
+    }
+    Launch L(c, eflag ? "pair_force_fp64_energy" : "pair_force_fp64");
+    launch_force<double>(c, c->tab_d, eflag, rdf);
+    return check_launch(c);
+}
+
+static int mixed_forces(simox_ctx* c, bool rdf) {
+    const bool eflag = false;
     if (!use_fp64(c, eflag) && c->using_skin && c->g0_species >= 0) {
         Launch L(c, "pair_force");
         PairParams P = pair_params(c);
@@ -1254,9 +1394,8 @@ int pair_forces(simox_ctx* c, bool eflag, bool rdf) {
                 c->f, c->rdf, c->status);
         return check_launch(c);
     }
-    Launch L(c, use_fp64(c, eflag) ? "pair_force_fp64" : "pair_force");
-    if (!use_fp64(c, eflag)) launch_force<float>(c, c->tab_f, eflag, rdf);
-    else launch_force<double>(c, c->tab_d, eflag, rdf);
+    Launch L(c, "pair_force");
+    launch_force<float>(c, c->tab_f, eflag, rdf);
     return check_launch(c);
 }
 
