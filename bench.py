@@ -359,6 +359,8 @@ def main():
                     help="profiling run: set-up, then --steps MD steps of the workload (charges as "
                          "generated, no CTIP, no comparison runs); prints nothing else")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="precision of --ncu")
+    ap.add_argument("--freq-stat", type=int, default=FREQ_STAT,
+                    help="--ncu: energies on steps with MOD(step, freq_stat) == 0 (1: every step)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -367,7 +369,9 @@ def main():
         build.build()
         s = build_system()
         g = equilibrated_context(s, args.precision)
-        run_md(g, s, 2, args.steps, None)
+        from simox_b200 import systems as S
+        g.md_run(args.steps, 1.0 / S.TFM, first_step=2, thermostat=True, T_given=600.0 * S.KB, freq_new=FREQ_NEW,
+                 freq_sort=1, freq_stat=args.freq_stat)
         g.sync()
         g.close()
         return 0
