@@ -94,6 +94,91 @@ void prof_collect(simox_ctx* c) {
 
 // ---------------------------------------------------------------------------
 // device-resident main loop (main.f90:40-84 with TAG_SET main.f90:376-414)
+
+// One step without CTIP: VV_NVE1, CELL_SORT, FORCE (+ PME on the side
+// stream), VV_NVE2 / VV_NVT2_BEREND.  Every launch goes to c->stream or, for
+// PME, to c->side forked from and joined back to it, so the whole step can be
+// captured into one CUDA graph.
+static int md_step(simox_ctx* c, const simox_md_opts* o, bool sort, bool estep, bool want_rdf) {
+    int st;
+    if (estep) cudaMemsetAsync(c->acc, 0, sizeof(double) * (A_EREC + 1), c->stream);
+    if ((st = vv1(c, o->dt, o->reflect != 0))) return st;
+    if (sort && (st = cell_sort(c))) return st;
+    // PME (positions and charges only) runs on the side stream while the
+    // pair passes run; its forces land in f_rec and the second half kick
+    // adds them: f = f_pair + f_rec - Fsum/N, as FORCE + PME would leave f.
+    if ((st = ensure_gathered(c))) return st;
+    cudaEventRecord(c->ev_fork, c->stream);
+    cudaStreamWaitEvent(c->side, c->ev_fork, 0);
+    std::swap(c->stream, c->side);
+    pme_bind_stream(c);
+    st = pme_forces(c, false, estep, c->f_rec);
+    std::swap(c->stream, c->side);
+    pme_bind_stream(c);
+    if (st) return st;
+    cudaEventRecord(c->ev_join, c->side);
+    if ((st = ensure_list(c))) return st;
+    if ((st = eam_density(c, estep))) return st;
+    if ((st = pair_forces(c, estep, want_rdf))) return st;
+    cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+    if (o->thermostat) st = nvt2_berend(c, o->dt, o->T_given, true, c->f_rec);
+    else st = vv2(c, o->dt, true, c->f_rec);
+    return st;
+}
+
+void drop_graphs(simox_ctx* c) {
+    for (auto& g : c->graphs) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g = simox_ctx::StepGraph{};
+    }
+}
+
+// The step as a graph: captured on first use of its key, then replayed.
+// A capture that fails (an API call the capture does not allow) turns graphs
+// off for this context and the step runs eagerly.
+static int md_step_graph(simox_ctx* c, const simox_md_opts* o, bool sort, bool estep, bool want_rdf) {
+    const unsigned long long key = 1ull | (sort ? 2ull : 0) | (estep ? 4ull : 0) | (want_rdf ? 8ull : 0) |
+                                   (o->reflect ? 16ull : 0) | (o->thermostat ? 32ull : 0) |
+                                   ((unsigned long long)(unsigned)c->n << 32);
+    simox_ctx::StepGraph* hit = nullptr;
+    for (auto& g : c->graphs)
+        if (g.exec && g.key == key && g.dt == o->dt && g.T == o->T_given) hit = &g;
+    if (!hit) {
+        cudaGraph_t graph = nullptr;
+        if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            c->graphs_on = false;
+            return md_step(c, o, sort, estep, want_rdf);
+        }
+        const long long l0 = c->launches;
+        int st = md_step(c, o, sort, estep, want_rdf);
+        const cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+        cudaGetLastError();
+        cudaGraphExec_t exec = nullptr;
+        if (st || ce != cudaSuccess || !graph || cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+            c->graphs_on = false;
+            if (st) return st;
+            // the capture recorded nothing that ran: run the step eagerly
+            c->launches = l0;
+            return md_step(c, o, sort, estep, want_rdf);
+        }
+        cudaGraphDestroy(graph);
+        simox_ctx::StepGraph& g = c->graphs[c->graph_next];
+        c->graph_next = (c->graph_next + 1) % 4;
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g.key = key;
+        g.dt = o->dt;
+        g.T = o->T_given;
+        g.exec = exec;
+        g.kernels = c->launches - l0;
+        c->launches = l0;
+        hit = &g;
+    }
+    c->launches += hit->kernels;
+    return cuda_status(cudaGraphLaunch(hit->exec, c->stream));
+}
+
 int md_run(simox_ctx* c, const simox_md_opts* o, int first, int nsteps, simox_energies* e, int* rdf) {
     if (!c->psi_valid || !c->cells_valid) return SIMOX_E_STATE;
     const bool want_rdf = rdf != nullptr || o->accumulate_rdf;
@@ -103,32 +188,38 @@ int md_run(simox_ctx* c, const simox_md_opts* o, int first, int nsteps, simox_en
         const bool new_charge = o->freq_new > 0 && (o->charge_every_step || step % o->freq_new == 1);
         const bool sort = o->freq_sort > 0 && step % o->freq_sort == 0;
         const bool estep = o->freq_stat <= 0 || step % o->freq_stat == 0;   // TAG_SET status rule
-        if (estep) cudaMemsetAsync(c->acc, 0, sizeof(double) * (A_EREC + 1), c->stream);
-        if ((st = vv1(c, o->dt, o->reflect != 0))) return st;
-        if (sort && (st = cell_sort(c))) return st;
         if (new_charge) {
+            // CTIP_SOLVER between CELL_SORT and FORCE: eager (host-driven CG)
+            if (estep) cudaMemsetAsync(c->acc, 0, sizeof(double) * (A_EREC + 1), c->stream);
+            if ((st = vv1(c, o->dt, o->reflect != 0))) return st;
+            if (sort && (st = cell_sort(c))) return st;
             simox_ctip_report rep;
             if ((st = ctip_solve(c, 0, &rep))) return st;
+            simox_md_opts o2 = *o;
+            // the rest of the step: FORCE, PME, VV2 (VV1 and CELL_SORT done)
+            if ((st = ensure_gathered(c))) return st;
+            cudaEventRecord(c->ev_fork, c->stream);
+            cudaStreamWaitEvent(c->side, c->ev_fork, 0);
+            std::swap(c->stream, c->side);
+            pme_bind_stream(c);
+            st = pme_forces(c, false, estep, c->f_rec);
+            std::swap(c->stream, c->side);
+            pme_bind_stream(c);
+            if (st) return st;
+            cudaEventRecord(c->ev_join, c->side);
+            if ((st = ensure_list(c))) return st;
+            if ((st = eam_density(c, estep))) return st;
+            if ((st = pair_forces(c, estep, want_rdf))) return st;
+            cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+            if (o2.thermostat) st = nvt2_berend(c, o2.dt, o2.T_given, true, c->f_rec);
+            else st = vv2(c, o2.dt, true, c->f_rec);
+            if (st) return st;
+            continue;
         }
-        // PME (positions and charges only) runs on the side stream while the
-        // pair passes run; its forces land in f_rec and the second half kick
-        // adds them: f = f_pair + f_rec - Fsum/N, as FORCE + PME would leave f.
-        if ((st = ensure_gathered(c))) return st;
-        cudaEventRecord(c->ev_fork, c->stream);
-        cudaStreamWaitEvent(c->side, c->ev_fork, 0);
-        std::swap(c->stream, c->side);
-        pme_bind_stream(c);
-        st = pme_forces(c, false, estep, c->f_rec);
-        std::swap(c->stream, c->side);
-        pme_bind_stream(c);
-        if (st) return st;
-        cudaEventRecord(c->ev_join, c->side);
-        if ((st = ensure_list(c))) return st;
-        if ((st = eam_density(c, estep))) return st;
-        if ((st = pair_forces(c, estep, want_rdf))) return st;
-        cudaStreamWaitEvent(c->stream, c->ev_join, 0);
-        if (o->thermostat) st = nvt2_berend(c, o->dt, o->T_given, true, c->f_rec);
-        else st = vv2(c, o->dt, true, c->f_rec);
+        // a graph replays only the launches it captured: the first step after
+        // a new atom set (skin list seeded from the host) runs eagerly
+        const bool graph_ok = c->graphs_on && !c->profiling && (!c->skin_mode || c->skin_valid);
+        st = graph_ok ? md_step_graph(c, o, sort, estep, want_rdf) : md_step(c, o, sort, estep, want_rdf);
         if (st) return st;
     }
     if ((st = read_status(c))) return st;
@@ -263,6 +354,7 @@ extern "C" const char* simox_version(void) {
 static void free_ctx(simox_ctx* c) {
     if (!c) return;
     prof_collect(c);
+    drop_graphs(c);
     pme_free(c);
     void* bufs[] = {c->id, c->x, c->v, c->f, c->q, c->xm, c->cell_of, c->cell_xyz, c->cell_count, c->cell_start, c->cell_fill,
                     c->sorted, c->pair13, c->entries, c->xq_s, c->t_s, c->rec_s, c->frec_s, c->nn, c->nbr, c->nn_max, c->nn_tot,
@@ -421,7 +513,10 @@ extern "C" int simox_set_state(simox_ctx* c, int n, const int* id, const double*
         c->have_ids = true;
     }
     if (n != c->n) c->cells_valid = false;
-    if (n != c->n || id) c->skin_valid = false;
+    if (n != c->n || id) {
+        c->skin_valid = false;
+        drop_graphs(c);
+    }
     if (x) {
         bool inb = true;
         for (int i = 0; i < 3 * n && inb; i++) inb = std::fabs(x[i]) <= c->hbox[i % 3];

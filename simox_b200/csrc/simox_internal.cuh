@@ -209,6 +209,18 @@ struct simox_ctx {
     std::vector<cudaEvent_t> ev_pool;
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
     long long launches = 0;
+
+    // md_run: instantiated CUDA graphs of one loop step, keyed by everything
+    // that changes the launch sequence; dropped when the atom set changes
+    struct StepGraph {
+        unsigned long long key = 0;
+        double dt = 0.0, T = 0.0;
+        cudaGraphExec_t exec = nullptr;
+        long long kernels = 0;
+    };
+    StepGraph graphs[4];
+    int graph_next = 0;
+    bool graphs_on = true;
     double eself = 0.0;         // sys%Eself of the last PME_SELF or CTIP_SOLVER
     int last_max_nnb = 0;
     long long last_tot_nnb = 0;
@@ -268,6 +280,7 @@ int nvt2_berend(simox_ctx* c, double dt, double T_given, bool subtract_mean, con
 int update_masses(simox_ctx* c);
 // md
 int md_run(simox_ctx* c, const simox_md_opts* o, int first, int nsteps, simox_energies* e, int* rdf);
+void drop_graphs(simox_ctx* c);
 
 // device helpers -------------------------------------------------------------
 __device__ __forceinline__ double warp_sum(double v) {
