@@ -294,6 +294,118 @@ struct FilterParams {
     float4 sh[kEntries];     // stencil position -> o * Lcs
 };
 
+// Density constants of one (X, Y) kind: FP32 filter in folded form
+// (2^(k1 r + k0) / (1 + t^20), t = r ire + nlam, times fe), FP64 in the
+// reference's form.
+template <typename R>
+struct DensC {
+    R fe, ire, c, lam, k1, k0, nlam;
+};
+
+template <typename R>
+__device__ __forceinline__ R dens_term(const DensC<R>& d, R r) {
+    if constexpr (std::is_same<R, float>::value) {
+        const float t = fmaf(r, d.ire, d.nlam);
+        const float t2 = t * t, t4 = t2 * t2, t8 = t4 * t4, t16 = t8 * t8;
+        const float ex = ex2_approx(fmaf(r, d.k1, d.k0));
+        return d.fe * ex * rcp_approx(fmaf(t16, t4, 1.f));
+    } else {
+        return d.fe * zhou_val<double>(r, d.ire, d.c, d.lam);
+    }
+}
+
+// One group of X's skin row (G = 0: metal partners, row front; G = 1: oxygen
+// partners, row back).  UNI: the partner species of the group is fixed (sYf),
+// so its density constants sit in registers; otherwise they are looked up per
+// entry.  Kept entries are compacted into X's exact row (same end of the row)
+// with bit 31 = "X is the reference's i".  Returns the kept count.
+template <typename R, int G, bool UNI>
+__device__ __forceinline__ int filter_group(const FilterParams& F, const float4* ssh, const DensC<R>* dsh,
+                                            const int* dflag, int sX, int sYf, const unsigned* __restrict__ sp,
+                                            int mg, unsigned* __restrict__ dp, const float4& ra, unsigned wa, int xm,
+                                            int ym, int zm, int oX, const double4& xa, int X,
+                                            const double4* __restrict__ xq, const float4* __restrict__ rec,
+                                            const int* __restrict__ order, double& rho, int& bad) {
+    constexpr bool F32 = std::is_same<R, float>::value;
+    const PairParams& P = F.pp;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int ax = wa & 511, ay = (wa >> 9) & 511, az = (wa >> 18) & 511;
+    DensC<R> du{};
+    if (UNI) {
+        du = dsh[(sX << 3) | sYf];
+        if (mg > 0) bad |= dflag[(sX << 3) | sYf];
+    }
+    auto ent = [&](int k) { return k < mg ? sp[G == 0 ? k : -k] : 0u; };
+    unsigned E1 = ent(lane), E2 = ent(lane + 32);
+    float4 rb1 = rec[E1 & kSkinIdxMask];
+    double4 xb1 = F32 ? make_double4(0, 0, 0, 0) : xq[E1 & kSkinIdxMask];
+    int out = 0;
+    for (int base = 0; base < mg; base += 32) {
+        const int k = base + lane;
+        const unsigned e = E1;
+        const float4 rb = rb1;
+        const double4 xb = xb1;
+        E1 = E2;
+        rb1 = rec[E1 & kSkinIdxMask];
+        if (!F32) xb1 = xq[E1 & kSkinIdxMask];
+        E2 = ent(k + 64);
+        const unsigned Y = e & kSkinIdxMask;
+        const bool live = k < mg;
+        bool acc;
+        R r2;
+        if constexpr (F32) {
+            const float4 o = ssh[e >> kSkinCodeShift];
+            const float dx = (rb.x - ra.x) + o.x, dy = (rb.y - ra.y) + o.y, dz = (rb.z - ra.z) + o.z;
+            const float r2f = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            acc = live & (r2f < F.rcut2f);
+            const bool inband = live & (fabsf(r2f - F.rcut2f) <= F.band);
+            if (__any_sync(0xffffffffu, inband)) {
+                if (inband) {
+                    // within FP32 rounding of the cutoff: the reference's FP64 test
+                    double ddx, ddy, ddz;
+                    min_image(xq[X], xq[Y], P, ddx, ddy, ddz);
+                    acc = __dadd_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)), __dmul_rn(ddz, ddz)) <
+                          F.rcut2;
+                }
+            }
+            r2 = r2f;
+        } else {
+            double dx, dy, dz;
+            min_image(xa, xb, P, dx, dy, dz);
+            const double r2d = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+            acc = live & (r2d < F.rcut2);
+            r2 = r2d;
+        }
+        // X is the reference's i: Y's reference cell is one of the 13 forward
+        // cells of X's (cellsort.f90:18-30), or the same cell and X comes first
+        const unsigned wb = __float_as_uint(rb.w);
+        const int bx = wb & 511, by = (wb >> 9) & 511, bz = (wb >> 18) & 511;
+        const bool same = ((wb ^ wa) & 0x07ffffffu) == 0u;
+        int oY = 0x7fffffff;
+        if (acc & same) oY = order[Y];
+        const bool isa = (bz == zm) | ((bz == az) & ((by == ym) | ((by == ay) & ((bx == xm) | (same & (oX < oY))))));
+        const unsigned mask = __ballot_sync(0xffffffffu, acc);
+        const int pos = out + __popc(mask & lt);
+        if (acc & (pos < P.cap)) dp[G == 0 ? pos : -pos] = e | ((unsigned)isa << 31);
+        out += __popc(mask);
+        // density of Y at X (force.f90:84-85)
+        R r;
+        if constexpr (F32) r = r2 * rsqrt_approx(r2);
+        else r = sqrt(r2);
+        R v;
+        if (UNI) {
+            v = dens_term<R>(du, r);
+        } else {
+            const int ti = (sX << 3) | (int)(wb >> 27);
+            v = dens_term<R>(dsh[ti], r);
+            bad |= acc ? dflag[ti] : 0;
+        }
+        rho += acc ? (double)v : 0.0;
+    }
+    return out;
+}
+
 template <typename R>
 __global__ void __launch_bounds__(256)
     filter_density_kernel(FilterParams F, const PairTab<R>* __restrict__ tab, const double4* __restrict__ xq,
@@ -301,34 +413,35 @@ __global__ void __launch_bounds__(256)
                           const int2* __restrict__ nn_s, const unsigned* __restrict__ nbr_s, int2* __restrict__ nn,
                           unsigned* __restrict__ nbr, EmbedParams E, double* __restrict__ rho_s,
                           double* __restrict__ dF_s, float* __restrict__ dF_f, int* __restrict__ status,
-                          int* __restrict__ nn_max, unsigned long long* __restrict__ nn_tot) {
-    constexpr bool F32 = std::is_same<R, float>::value;
-    using R4 = typename std::conditional<F32, float4, double4>::type;
-    // density terms by (species X, species Y) with species in 3 bits (7:
+                          int* __restrict__ nn_max, unsigned long long* __restrict__ nn_tot, int g0) {
+    // density constants by (species X, species Y) with species in 3 bits (7:
     // unknown), and the status bits a pair of that kind raises
-    __shared__ R4 dtab[64];
+    __shared__ DensC<R> dsh[64];
     __shared__ int dflag[64];
     __shared__ float4 ssh[kEntries];
     for (int k = threadIdx.x; k < 64; k += blockDim.x) {
         const int a = k >> 3, b = k & 7;
-        R4 d;
+        DensC<R> d{};
         int fl;
         if (a < kSpecies && b < kSpecies) {
             const PairTab<R>& T = tab[a * kSpecies + b];
-            d.x = T.d_fe; d.y = T.d_inv_re; d.z = T.d_c; d.w = T.d_lam;
+            d.fe = T.d_fe; d.ire = T.d_inv_re; d.c = T.d_c; d.lam = T.d_lam;
+            d.nlam = -T.d_lam;
+            d.k1 = (R)(-1.4426950408889634) * T.d_c * T.d_inv_re;
+            d.k0 = (R)1.4426950408889634 * T.d_c;
             fl = T.valid ? 0 : ST_UNSUPPORTED;
         } else {
-            d.x = 0; d.y = 1; d.z = 0; d.w = 0;
+            d.fe = 0; d.ire = 1; d.c = 0; d.lam = 0; d.nlam = 0; d.k1 = 0; d.k0 = 0;
             fl = ST_UNKNOWN_PAIR;
         }
-        dtab[k] = d;
+        dsh[k] = d;
         dflag[k] = fl;
     }
     for (int k = threadIdx.x; k < kEntries; k += blockDim.x) ssh[k] = F.sh[k];
     __syncthreads();
+    constexpr bool F32 = std::is_same<R, float>::value;
     const PairParams& P = F.pp;
     const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
-    const unsigned lt = (1u << lane) - 1u;
     int lmax = 0, bad = 0;
     unsigned long long ltot = 0;
     for (int X = blockIdx.x * wpb + (threadIdx.x >> 5); X < P.n; X += gridDim.x * wpb) {
@@ -343,83 +456,18 @@ __global__ void __launch_bounds__(256)
         const int oX = order[X];
         const double4 xa = F32 ? make_double4(0, 0, 0, 0) : xq[X];
         const int2 ms = nn_s[X];
-        const int m = ms.x + ms.y;
-        const int back = F.cap_s - 1 + ms.x;   // slot of oxygen entry k is back - k
         const unsigned* srow = nbr_s + (size_t)X * F.cap_s;
         unsigned* row = nbr + (size_t)X * P.cap;
-        // one index space over both groups: metals from the front, oxygen from the back
-        auto ent = [&](int k) { return k < m ? srow[k < ms.x ? k : back - k] : 0u; };
-        // software pipeline: entries two batches ahead, records one batch ahead
-        unsigned E1 = ent(lane), E2 = ent(lane + 32);
-        float4 rb1 = rec[E1 & kSkinIdxMask];
-        double4 xb1 = F32 ? make_double4(0, 0, 0, 0) : xq[E1 & kSkinIdxMask];
-        int out0 = 0, out1 = 0;
         double rho = 0.0;
-        for (int base = 0; base < m; base += 32) {
-            const int k = base + lane;
-            const unsigned e = E1;
-            const float4 rb = rb1;
-            const double4 xb = xb1;
-            E1 = E2;
-            rb1 = rec[E1 & kSkinIdxMask];
-            if (!F32) xb1 = xq[E1 & kSkinIdxMask];
-            E2 = ent(k + 64);
-            const unsigned Y = e & kSkinIdxMask;
-            const bool live = k < m;
-            bool acc;
-            R r2;
-            if constexpr (F32) {
-                const float4 o = ssh[e >> kSkinCodeShift];
-                const float dx = (rb.x - ra.x) + o.x, dy = (rb.y - ra.y) + o.y, dz = (rb.z - ra.z) + o.z;
-                const float r2f = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                acc = live & (r2f < F.rcut2f);
-                const bool inband = live & (fabsf(r2f - F.rcut2f) <= F.band);
-                if (__any_sync(0xffffffffu, inband)) {
-                    if (inband) {
-                        // within FP32 rounding of the cutoff: the reference's FP64 test
-                        double ddx, ddy, ddz;
-                        min_image(xq[X], xq[Y], P, ddx, ddy, ddz);
-                        acc = __dadd_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)), __dmul_rn(ddz, ddz)) <
-                              F.rcut2;
-                    }
-                }
-                r2 = r2f;
-            } else {
-                double dx, dy, dz;
-                min_image(xa, xb, P, dx, dy, dz);
-                const double r2d = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-                acc = live & (r2d < F.rcut2);
-                r2 = r2d;
-            }
-            // X is the reference's i: Y's reference cell is one of the 13
-            // forward cells of X's (cellsort.f90:18-30), or the same cell and
-            // X comes first in it
-            const unsigned wb = __float_as_uint(rb.w);
-            const int bx = wb & 511, by = (wb >> 9) & 511, bz = (wb >> 18) & 511;
-            const bool same = ((wb ^ wa) & 0x07ffffffu) == 0u;
-            int oY = 0x7fffffff;
-            if (acc & same) oY = order[Y];
-            const bool isa = (bz == zm) | ((bz == az) & ((by == ym) | ((by == ay) & ((bx == xm) | (same & (oX < oY))))));
-            // compaction per group (lanes >= split hold oxygen entries)
-            const unsigned mask = __ballot_sync(0xffffffffu, acc);
-            const int split = ms.x - base;
-            const unsigned gm1 = split <= 0 ? 0xffffffffu : (split >= 32 ? 0u : (0xffffffffu << split));
-            const unsigned m1 = mask & gm1, m0 = mask & ~gm1;
-            const bool g1 = k >= ms.x;
-            const int pos = (g1 ? out1 : out0) + __popc((g1 ? m1 : m0) & lt);
-            if (acc & (pos < P.cap)) row[g1 ? P.cap - 1 - pos : pos] = e | ((unsigned)isa << 31);
-            out0 += __popc(m0);
-            out1 += __popc(m1);
-            // density of Y at X (force.f90:84-85)
-            const int ti = (sX << 3) | (int)(wb >> 27);
-            const R4 d = dtab[ti];
-            R r;
-            if constexpr (F32) r = r2 * rsqrtf(r2);
-            else r = sqrt(r2);
-            const R v = d.x * zhou_val<R>(r, d.y, d.z, d.w);
-            rho += acc ? (double)v : 0.0;
-            bad |= acc ? dflag[ti] : 0;
-        }
+        int out0, out1;
+        if (g0 >= 0)
+            out0 = filter_group<R, 0, true>(F, ssh, dsh, dflag, sX, g0, srow, ms.x, row, ra, wa, xm, ym, zm, oX, xa,
+                                            X, xq, rec, order, rho, bad);
+        else
+            out0 = filter_group<R, 0, false>(F, ssh, dsh, dflag, sX, 0, srow, ms.x, row, ra, wa, xm, ym, zm, oX, xa,
+                                             X, xq, rec, order, rho, bad);
+        out1 = filter_group<R, 1, true>(F, ssh, dsh, dflag, sX, 3, srow + (F.cap_s - 1), ms.y, row + (P.cap - 1), ra,
+                                        wa, xm, ym, zm, oX, xa, X, xq, rec, order, rho, bad);
         rho = warp_sum(rho);
         if (lane == 0) {
             const int tot = out0 + out1;
@@ -1286,11 +1334,13 @@ int filter_density(simox_ctx* c) {
         if (c->precision == SIMOX_FP64)
             filter_density_kernel<double><<<g, 256, 0, c->stream>>>(
                 F, c->tab_d, c->xq_s, c->rec_s, c->pair_order, reinterpret_cast<const int2*>(c->nn_s), c->nbr_s,
-                reinterpret_cast<int2*>(c->nn), c->nbr, E, c->rho_s, c->dF_s, c->dF_f, c->status, c->nn_max, c->nn_tot);
+                reinterpret_cast<int2*>(c->nn), c->nbr, E, c->rho_s, c->dF_s, c->dF_f, c->status, c->nn_max, c->nn_tot,
+                c->g0_species);
         else
             filter_density_kernel<float><<<g, 256, 0, c->stream>>>(
                 F, c->tab_f, c->xq_s, c->rec_s, c->pair_order, reinterpret_cast<const int2*>(c->nn_s), c->nbr_s,
-                reinterpret_cast<int2*>(c->nn), c->nbr, E, c->rho_s, c->dF_s, c->dF_f, c->status, c->nn_max, c->nn_tot);
+                reinterpret_cast<int2*>(c->nn), c->nbr, E, c->rho_s, c->dF_s, c->dF_f, c->status, c->nn_max, c->nn_tot,
+                c->g0_species);
     }
     int st = check_launch(c);
     if (st) return st;
