@@ -238,6 +238,44 @@ int simox_sync(simox_ctx* ctx);
 /* Neighbour statistics of the last list build: max and total list length. */
 int simox_neighbor_stats(simox_ctx* ctx, int* max_nnb, long long* total_nnb);
 
+/* ---- launch-shape tuning -------------------------------------------------
+ * No counterpart in the reference (a GPU launch choice).  Results do not
+ * depend on it: every atom's force is summed by one warp in the same order
+ * whatever the CTA split. */
+typedef struct {
+    int force_splits;    /* CTAs per skin cell in the mixed force pass, 1..16 (default 2) */
+} simox_tuning;
+int simox_set_tuning(simox_ctx* ctx, const simox_tuning* t);
+int simox_get_tuning(simox_ctx* ctx, simox_tuning* t);
+
+/* ---- batched independent systems ----------------------------------------
+ * No counterpart in the reference (which runs one system per process): many
+ * independent systems of different sizes, each a context created and set up
+ * by the caller (simox_create, simox_set_state, simox_pme_self,
+ * simox_cell_sort, charges), advanced together.  After one eager step per
+ * system, one MD step of ALL systems is captured into one CUDA graph (one
+ * branch per system, each with its PME side branch) and every further step
+ * is a single graph launch.  The contexts must live on one device, use the
+ * same freq_new/freq_sort/freq_stat, and have freq_new = 0 (charges held).
+ * The batch does not own the contexts; after changing a member's atom set,
+ * destroy and recreate the batch. */
+typedef struct simox_batch simox_batch;
+int simox_batch_create(int nsys, simox_ctx* const* ctxs, simox_batch** out);
+int simox_batch_destroy(simox_batch* b);
+/* Steps first_step .. first_step+nsteps-1 of main.f90:40-61 for every system;
+ * opts[k] and last[k] (may be NULL) belong to system k. */
+int simox_batch_md_run(simox_batch* b, const simox_md_opts* opts, int first_step, int nsteps,
+                       simox_energies* last);
+/* Autotuner: times `trial_steps` batch steps (real MD steps, after one
+ * untimed step) for each candidate rule "force_splits = clamp(ceil(target /
+ * skin cells), 1, 16)" with target in {0 (one CTA per cell), 148, 296, 592,
+ * 1184} CTAs, keeps the fastest and applies it to every system.  times_ms[5]
+ * (may be NULL) receives the per-step time of each candidate; *best the index. */
+int simox_batch_autotune(simox_batch* b, const simox_md_opts* opts, int first_step, int trial_steps,
+                         double* times_ms, int* best);
+/* Kernels launched by the batch (graph kernel nodes counted per replay). */
+int simox_batch_launch_count(simox_batch* b, long long* n);
+
 /* ---- allocation-free cell binning ---------------------------------------
  * No counterpart in the reference.  For callers that cannot let a library
  * allocate device memory -- programs whose GPU memory belongs to another

@@ -128,4 +128,12 @@ EXPORTED = [
     "simox_md_run", "simox_timer_begin", "simox_timer_end", "simox_profile_enable",
     "simox_profile_read", "simox_profile_reset", "simox_launch_count", "simox_sync",
     "simox_neighbor_stats", "simox_cell_sort_noalloc",
+    "simox_set_tuning", "simox_get_tuning",
+    "simox_batch_create", "simox_batch_destroy", "simox_batch_md_run", "simox_batch_autotune",
+    "simox_batch_launch_count",
 ]
+
+
+class Tuning(C.Structure):
+    """simox_tuning: launch-shape choices (results do not depend on them)."""
+    _fields_ = [("force_splits", C.c_int)]

@@ -19,7 +19,7 @@ import os
 import numpy as np
 
 from . import _abi
-from ._abi import (CtipReport, Energies, MdOpts, Potential, Setup, SIMOX_FP64, SIMOX_MIXED,
+from ._abi import (CtipReport, Energies, MdOpts, Potential, Setup, SIMOX_FP64, SIMOX_MIXED, Tuning,
                    status_text)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -77,6 +77,13 @@ def lib():
         "simox_sync": [_vp],
         "simox_neighbor_stats": [_vp, _ip, C.POINTER(C.c_longlong)],
         "simox_cell_sort_noalloc": [_vp, C.c_int, _dp, C.c_double, _vp, _vp, C.c_int, _vp],
+        "simox_set_tuning": [_vp, C.POINTER(Tuning)],
+        "simox_get_tuning": [_vp, C.POINTER(Tuning)],
+        "simox_batch_create": [C.c_int, C.POINTER(_vp), C.POINTER(_vp)],
+        "simox_batch_destroy": [_vp],
+        "simox_batch_md_run": [_vp, C.POINTER(MdOpts), C.c_int, C.c_int, C.POINTER(Energies)],
+        "simox_batch_autotune": [_vp, C.POINTER(MdOpts), C.c_int, C.c_int, _dp, _ip],
+        "simox_batch_launch_count": [_vp, C.POINTER(C.c_longlong)],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -328,6 +335,16 @@ class Simox:
     def sync(self):
         _check(lib().simox_sync(self._ctx), "sync")
 
+    def set_tuning(self, force_splits: int):
+        t = Tuning()
+        t.force_splits = int(force_splits)
+        _check(lib().simox_set_tuning(self._ctx, C.byref(t)), "set_tuning")
+
+    def get_tuning(self) -> dict:
+        t = Tuning()
+        _check(lib().simox_get_tuning(self._ctx, C.byref(t)), "get_tuning")
+        return {"force_splits": t.force_splits}
+
     def neighbor_stats(self):
         mx = C.c_int(0)
         tot = C.c_longlong(0)
@@ -339,3 +356,80 @@ def from_system(sys_, precision="fp64", **kw) -> Simox:
     """Context for a :class:`simox_b200.systems.AtomSystem`."""
     return Simox(sys_.ids, sys_.x, sys_.box, sys_.fft, rcut=sys_.rcut, q=sys_.q, v=sys_.v,
                  order=sys_.order, precision=precision, **kw)
+
+
+def md_opts(dt: float, thermostat: bool = False, T_given: float = 0.0, freq_new: int = 0, freq_sort: int = 1,
+            reflect: bool = False, freq_stat: int = 0) -> MdOpts:
+    """simox_md_opts for one system (see Simox.md_run)."""
+    o = MdOpts()
+    o.dt = float(dt)
+    o.thermostat = 1 if thermostat else 0
+    o.T_given = float(T_given)
+    o.freq_new = int(freq_new)
+    o.freq_sort = int(freq_sort)
+    o.reflect = 1 if reflect else 0
+    o.charge_every_step = 0
+    o.accumulate_rdf = 0
+    o.freq_stat = int(freq_stat)
+    return o
+
+
+class Batch:
+    """Independent systems advanced together: one CUDA graph launch per MD
+    step for all of them (simox_batch_*).  The member contexts stay owned by
+    the caller and must outlive the batch."""
+
+    def __init__(self, members):
+        self.members = list(members)
+        arr = (_vp * len(self.members))(*[m._ctx for m in self.members])
+        h = _vp()
+        _check(lib().simox_batch_create(len(self.members), arr, C.byref(h)), "batch_create")
+        self._b = h
+
+    def close(self):
+        if getattr(self, "_b", None):
+            lib().simox_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _opts(self, opts):
+        if isinstance(opts, MdOpts):
+            opts = [opts] * len(self.members)
+        arr = (MdOpts * len(self.members))(*opts)
+        return arr
+
+    def md_run(self, opts, nsteps: int, first_step: int = 1):
+        """Steps first_step .. first_step+nsteps-1 for every member; opts is one
+        MdOpts for all or a list, one per member.  Returns the energies of each
+        member's last energy step."""
+        arr = self._opts(opts)
+        out = (Energies * len(self.members))()
+        _check(lib().simox_batch_md_run(self._b, arr, int(first_step), int(nsteps), out), "batch_md_run")
+        return [e.as_dict() for e in out]
+
+    def autotune(self, opts, first_step: int, trial_steps: int = 5):
+        """Times the five force-split rules on the whole batch (real MD steps,
+        6 per rule) and keeps the fastest; returns (per-step ms of each rule,
+        index of the chosen one)."""
+        arr = self._opts(opts)
+        t = np.zeros(5)
+        best = C.c_int(0)
+        _check(lib().simox_batch_autotune(self._b, arr, int(first_step), int(trial_steps), _d(t), C.byref(best)),
+               "batch_autotune")
+        return t, best.value
+
+    def launch_count(self) -> int:
+        n = C.c_longlong(0)
+        _check(lib().simox_batch_launch_count(self._b, C.byref(n)), "batch_launch_count")
+        return n.value

@@ -99,7 +99,7 @@ void prof_collect(simox_ctx* c) {
 // stream), VV_NVE2 / VV_NVT2_BEREND.  Every launch goes to c->stream or, for
 // PME, to c->side forked from and joined back to it, so the whole step can be
 // captured into one CUDA graph.
-static int md_step(simox_ctx* c, const simox_md_opts* o, bool sort, bool estep, bool want_rdf) {
+int md_step(simox_ctx* c, const simox_md_opts* o, bool sort, bool estep, bool want_rdf) {
     int st;
     if (estep) cudaMemsetAsync(c->acc, 0, sizeof(double) * (A_EREC + 1), c->stream);
     if ((st = vv1(c, o->dt, o->reflect != 0))) return st;
@@ -725,6 +725,22 @@ extern "C" int simox_md_run(simox_ctx* c, const simox_md_opts* o, int first_step
     if (!c || !o || nsteps < 0) return SIMOX_E_ARG;
     cudaSetDevice(c->device);
     return md_run(c, o, first_step, nsteps, e, rdf);
+}
+
+extern "C" int simox_set_tuning(simox_ctx* c, const simox_tuning* t) {
+    if (!c || !t) return SIMOX_E_ARG;
+    if (t->force_splits < 1 || t->force_splits > 16) return SIMOX_E_ARG;
+    if (t->force_splits != c->force_splits) {
+        c->force_splits = t->force_splits;
+        drop_graphs(c);   // the captured launches carry the old grid
+    }
+    return SIMOX_OK;
+}
+
+extern "C" int simox_get_tuning(simox_ctx* c, simox_tuning* t) {
+    if (!c || !t) return SIMOX_E_ARG;
+    t->force_splits = c->force_splits;
+    return SIMOX_OK;
 }
 
 extern "C" int simox_timer_begin(simox_ctx* c) {

@@ -1431,7 +1431,7 @@ static int mixed_forces(simox_ctx* c, bool rdf) {
         Q.tab[1] = pack_tab(c->pot, g0, 3);
         Q.tab[2] = pack_tab(c->pot, 3, g0);
         Q.tab[3] = pack_tab(c->pot, 3, 3);
-        const int splits = 2;
+        const int splits = std::max(1, std::min(16, c->force_splits));
         const int g = c->ncell_s * splits;
         const int2* nn = reinterpret_cast<const int2*>(c->nn);
         if (rdf)

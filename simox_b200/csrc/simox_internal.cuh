@@ -106,6 +106,7 @@ struct simox_ctx {
     int fft[3]{}, order = 4;
     size_t ngrid = 0, nhalf = 0;
     int npt_max = SIMOX_NPT_MAX, nnb_cap = 1024;
+    int force_splits = 2;       // CTAs per skin cell of the mixed force pass (simox_set_tuning)
 
     // species present
     bool has_h = false;
@@ -281,6 +282,7 @@ int update_masses(simox_ctx* c);
 // md
 int md_run(simox_ctx* c, const simox_md_opts* o, int first, int nsteps, simox_energies* e, int* rdf);
 void drop_graphs(simox_ctx* c);
+int md_step(simox_ctx* c, const simox_md_opts* o, bool sort, bool estep, bool want_rdf);
 
 // device helpers -------------------------------------------------------------
 __device__ __forceinline__ double warp_sum(double v) {

@@ -223,6 +223,50 @@ def oxidation_slab(seed: int = 5, cells=(60, 60, 30), n_o: int = 40000, gas_dens
                       dict(seed=seed, T=T, n_al=len(al), n_o=n_o))
 
 
+_FFT_SIZES = (32, 36, 40, 45, 48, 50, 54, 60, 64)
+
+
+def replica(seed: int, n: int, o_frac: float, T: float, order: int = 6, min_box: float = 34.0,
+            a: float = 4.05) -> AtomSystem:
+    """One system of the batched-replica workload: fcc Al with O on randomly
+    chosen octahedral interstitial sites (the lattice is enlarged, with Al
+    vacancies, when there are more O than sites), 0.05 A Gaussian site jitter,
+    Maxwell-Boltzmann velocities at T, each box edge padded to >= min_box
+    (vacuum around small crystals), PME grid >= 1 point per A from 32 to 64
+    per axis.  Charges: Al +0.3 e, O -0.2 e, shifted to neutral."""
+    rng = np.random.default_rng(seed)
+    n_o = int(round(n * o_frac))
+    n_al = n - n_o
+    sites = max(n_al, n_o, 1)
+    m = int(np.ceil((sites / 4.0) ** (1.0 / 3.0)))
+    al_sites = fcc(m, m, m, a)
+    oct_sites = al_sites + np.array([a / 2, 0.0, 0.0])     # octahedral sublattice of fcc
+    ext = m * a
+    box = np.full(3, max(ext, min_box))
+    pick_al = rng.choice(len(al_sites), n_al, replace=False)
+    pick_o = rng.choice(len(oct_sites), n_o, replace=False)
+    x = np.vstack([al_sites[pick_al], oct_sites[pick_o]]) - ext / 2
+    x = x + rng.normal(0.0, 0.05, x.shape)
+    ids = np.concatenate([np.full(n_al, 1, np.int32), np.full(n_o, 4, np.int32)])
+    v = maxwell_boltzmann(ids, T, rng)
+    q = np.where(ids == 1, 0.3, -0.2)
+    q = q - q.mean()
+    fft = tuple(next((k for k in _FFT_SIZES if k >= box[d]), _FFT_SIZES[-1]) for d in range(3))
+    return AtomSystem("replica", ids, wrap_centered(x, box), v, q, box, fft, order, 10.0,
+                      dict(seed=seed, T=T, n_al=n_al, n_o=n_o))
+
+
+def replica_batch(seed: int = 7, nsys: int = 256, n_lo: int = 500, n_hi: int = 8000):
+    """The batched workload: nsys systems with sizes uniform in [n_lo, n_hi],
+    O fraction uniform in [0, 0.6], temperatures uniform in [300, 1200] K."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(nsys):
+        n = int(rng.integers(n_lo, n_hi + 1))
+        out.append(replica(int(rng.integers(1 << 30)), n, float(rng.uniform(0.0, 0.6)), float(rng.uniform(300, 1200))))
+    return out
+
+
 def write_restart_xyz(path: str, s: AtomSystem, f: np.ndarray | None = None) -> None:
     """restart.xyz in the layout READ_INPUT reads with restart=YES
     (main.f90:224-228): ``El x y z vx vy vz fx fy fz q`` (full precision)."""

@@ -1,0 +1,96 @@
+"""Batched independent systems (simox_batch_*): one CUDA graph launch per MD
+step for all members must give each member the trajectory it has when it is
+stepped alone, and the force pass's CTA split (the autotuner's knob) must not
+change any result.
+
+Bars: FP64 positions within 1e-9 A and energies within 1e-9 relative after 8
+steps (the PME spread's FP64 atomics may add in a different order); mixed
+positions within 1e-6 A; forces for CTA splits 1 and 8 bit-identical.
+"""
+import numpy as np
+import pytest
+
+from simox_b200 import api, systems as S
+
+pytestmark = pytest.mark.gpu
+
+DT = 1.0 / S.TFM
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _lib(simox_lib):
+    return simox_lib
+
+
+def _members():
+    return [S.replica(11, 700, 0.0, 300.0), S.replica(12, 1500, 0.3, 600.0),
+            S.replica(13, 2600, 0.5, 900.0), S.replica(14, 4100, 0.6, 1200.0)]
+
+
+def _prepared(s, precision):
+    g = api.from_system(s, precision=precision)
+    g.pme_self()
+    g.cell_sort()
+    g.force()
+    g.pme()
+    return g
+
+
+def _opts(s):
+    return api.md_opts(DT, thermostat=True, T_given=s.meta["T"] * S.KB, freq_stat=4)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("mixed", 1e-6)])
+def test_batch_matches_single_systems(precision, tol):
+    systems = _members()
+    alone = []
+    for s in systems:
+        with _prepared(s, precision) as g:
+            e = g.md_run(8, DT, first_step=1, thermostat=True, T_given=s.meta["T"] * S.KB, freq_stat=4)
+            alone.append((g.get_state()["x"], e))
+    members = [_prepared(s, precision) for s in systems]
+    try:
+        with api.Batch(members) as b:
+            es = b.md_run([_opts(s) for s in systems], 8, first_step=1)
+            assert b.launch_count() > 0
+        for k, g in enumerate(members):
+            x = g.get_state()["x"]
+            d = x - alone[k][0]
+            d -= systems[k].box * np.round(d / systems[k].box)
+            assert np.abs(d).max() <= tol, (k, np.abs(d).max())
+            for key in ("Epair", "Egroup", "Edir", "Ectip", "Erec", "mv2"):
+                ref = alone[k][1][key]
+                assert abs(es[k][key] - ref) <= 1e-9 * max(1.0, abs(ref)) * (1 if precision == "fp64" else 1e3), key
+    finally:
+        for g in members:
+            g.close()
+
+
+def test_force_split_does_not_change_forces():
+    s = S.replica(21, 3000, 0.4, 600.0)
+    out = []
+    for splits in (1, 8):
+        with _prepared(s, "mixed") as g:
+            g.set_tuning(splits)
+            assert g.get_tuning()["force_splits"] == splits
+            g.vv_nve1(DT)
+            g.cell_sort()
+            g.force(energies=False)
+            out.append(g.get_state()["f"])
+    assert np.array_equal(out[0], out[1])
+
+
+def test_batch_autotune_picks_a_rule_and_keeps_running():
+    systems = _members()
+    members = [_prepared(s, "mixed") for s in systems]
+    try:
+        with api.Batch(members) as b:
+            opts = [_opts(s) for s in systems]
+            b.md_run(opts, 2, first_step=1)
+            times, best = b.autotune(opts, first_step=3, trial_steps=2)
+            assert np.all(times > 0) and 0 <= best < 5 and times[best] == times.min()
+            e = b.md_run(opts, 4, first_step=3 + 5 * 3)
+            assert all(np.isfinite(v["mv2"]) and v["mv2"] > 0 for v in e)
+    finally:
+        for g in members:
+            g.close()
