@@ -238,6 +238,49 @@ int simox_sync(simox_ctx* ctx);
 /* Neighbour statistics of the last list build: max and total list length. */
 int simox_neighbor_stats(simox_ctx* ctx, int* max_nnb, long long* total_nnb);
 
+/* ---- parameter adjoint ---------------------------------------------------
+ * No counterpart in the reference (which has fixed parameters and no
+ * derivatives).  The adjoint model is the FORCE + PME + CTIP_SOLVER physics
+ * with the three EAM functions of one metal -- the density f(r) it
+ * contributes (eam.f90 ftn), its pair phi(r) with itself (METAL_HOMO) and its
+ * embedding F(rho) -- as uniform cubic B-splines of SIMOX_SPLINE_N
+ * coefficients each; every term involving oxygen keeps the analytic forms.
+ * Its energy is E = Epair + Egroup + U(q*), U the functional CTIP_SOLVER
+ * minimises (ctip.f90:307-333) and q* its minimiser (the reference's CG, then
+ * Newton steps on the fixed active set to FP64 precision).  Its forces are
+ * FORCE + PME at q* (as-written formulas).  All of it is FP64.
+ * Gradient layout (SIMOX_NGRAD doubles): phi[64], dens[64], emb[64], then for
+ * species 1..5: d/dchi, d/dJ, d/dZ.  Gradients with respect to xi (zeta) are
+ * not provided: the Slater coefficient table fafb depends on xi. */
+#define SIMOX_SPLINE_N 64
+#define SIMOX_NGRAD (3 * SIMOX_SPLINE_N + 3 * SIMOX_NATOM)
+typedef struct {
+    int    metal;            /* species id whose EAM functions are splines (1 = Al) */
+    double r0, r1;           /* domain (A) of the f and phi splines; pairs beyond r1 add nothing */
+    double rho0, rho1;       /* domain of the embedding spline (extrapolated cubically outside) */
+    double phi[SIMOX_SPLINE_N], dens[SIMOX_SPLINE_N], emb[SIMOX_SPLINE_N];
+} simox_eam_spline;
+
+typedef struct {
+    double E, E_eam, U;      /* E = E_eam + U                                   */
+    double loss;             /* sum_i |F_i - T_i|^2 (0 without targets)           */
+    double residual;         /* ||P grad_q U|| after the charge refinement         */
+    double adj_residual;     /* relative residual of the adjoint CG                */
+    int    n_cg, n_newton, n_adjoint;
+} simox_adjoint_report;
+
+/* Spline mode of the adjoint model (NULL switches it off).  The context then
+ * uses the reference cells' exact list (no skin list). */
+int simox_set_eam_spline(simox_ctx* ctx, const simox_eam_spline* s);
+/* CTIP parameters chi, J, Z of species 1..5 (POTN datafmt.f90:54-56). */
+int simox_set_ctip_params(simox_ctx* ctx, int species, double chi, double J, double Z);
+/* Charges q*, energy, forces (original order, [n][3], may be NULL) and the
+ * gradients of E (grad_E) and of L = sum |F - T|^2 (grad_L; needs f_target
+ * [n][3]) with respect to the parameters; either gradient may be NULL.  The
+ * loss gradient runs one adjoint CG (FP64) through the charge solve. */
+int simox_adjoint_eval(simox_ctx* ctx, const double* f_target, simox_adjoint_report* rep,
+                       double* forces, double* grad_E, double* grad_L);
+
 /* ---- launch-shape tuning -------------------------------------------------
  * No counterpart in the reference (a GPU launch choice).  Results do not
  * depend on it: every atom's force is summed by one warp in the same order

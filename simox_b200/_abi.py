@@ -131,9 +131,30 @@ EXPORTED = [
     "simox_set_tuning", "simox_get_tuning",
     "simox_batch_create", "simox_batch_destroy", "simox_batch_md_run", "simox_batch_autotune",
     "simox_batch_launch_count",
+    "simox_set_eam_spline", "simox_set_ctip_params", "simox_adjoint_eval",
 ]
 
 
 class Tuning(C.Structure):
     """simox_tuning: launch-shape choices (results do not depend on them)."""
     _fields_ = [("force_splits", C.c_int)]
+
+
+SPLINE_N = 64
+NGRAD = 3 * SPLINE_N + 3 * NATOM
+
+
+class EamSpline(C.Structure):
+    """simox_eam_spline: cubic B-spline EAM functions of one metal."""
+    _fields_ = [("metal", C.c_int), ("r0", C.c_double), ("r1", C.c_double), ("rho0", C.c_double),
+                ("rho1", C.c_double), ("phi", C.c_double * SPLINE_N), ("dens", C.c_double * SPLINE_N),
+                ("emb", C.c_double * SPLINE_N)]
+
+
+class AdjointReport(C.Structure):
+    _fields_ = [("E", C.c_double), ("E_eam", C.c_double), ("U", C.c_double), ("loss", C.c_double),
+                ("residual", C.c_double), ("adj_residual", C.c_double), ("n_cg", C.c_int), ("n_newton", C.c_int),
+                ("n_adjoint", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}

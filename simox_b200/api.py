@@ -19,8 +19,8 @@ import os
 import numpy as np
 
 from . import _abi
-from ._abi import (CtipReport, Energies, MdOpts, Potential, Setup, SIMOX_FP64, SIMOX_MIXED, Tuning,
-                   status_text)
+from ._abi import (AdjointReport, CtipReport, EamSpline, Energies, MdOpts, NGRAD, Potential, Setup, SIMOX_FP64,
+                   SIMOX_MIXED, Tuning, status_text)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libsimox_b200.so")
@@ -84,6 +84,9 @@ def lib():
         "simox_batch_md_run": [_vp, C.POINTER(MdOpts), C.c_int, C.c_int, C.POINTER(Energies)],
         "simox_batch_autotune": [_vp, C.POINTER(MdOpts), C.c_int, C.c_int, _dp, _ip],
         "simox_batch_launch_count": [_vp, C.POINTER(C.c_longlong)],
+        "simox_set_eam_spline": [_vp, C.POINTER(EamSpline)],
+        "simox_set_ctip_params": [_vp, C.c_int, C.c_double, C.c_double, C.c_double],
+        "simox_adjoint_eval": [_vp, _dp, C.POINTER(AdjointReport), _dp, _dp, _dp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -334,6 +337,27 @@ class Simox:
 
     def sync(self):
         _check(lib().simox_sync(self._ctx), "sync")
+
+    # -- parameter adjoint (no counterpart in the reference) -------------------
+    def set_eam_spline(self, spline: EamSpline | None):
+        """Spline mode of the adjoint model (simox_set_eam_spline); None: off."""
+        _check(lib().simox_set_eam_spline(self._ctx, C.byref(spline) if spline is not None else None),
+               "set_eam_spline")
+
+    def set_ctip_params(self, species: int, chi: float, J: float, Z: float):
+        _check(lib().simox_set_ctip_params(self._ctx, int(species), float(chi), float(J), float(Z)),
+               "set_ctip_params")
+
+    def adjoint_eval(self, f_target=None, gradients: bool = True):
+        """Charges, energy, forces [n][3] and the gradients (NGRAD each) of the
+        energy and of L = sum |F - T|^2 (if f_target is given)."""
+        rep = AdjointReport()
+        f = np.zeros((self.n, 3))
+        gE = np.zeros(NGRAD) if gradients else None
+        gL = np.zeros(NGRAD) if (gradients and f_target is not None) else None
+        t = _f64(f_target, (self.n, 3))
+        _check(lib().simox_adjoint_eval(self._ctx, _d(t), C.byref(rep), _d(f), _d(gE), _d(gL)), "adjoint_eval")
+        return rep.as_dict(), f, gE, gL
 
     def set_tuning(self, force_splits: int):
         t = Tuning()

@@ -355,6 +355,7 @@ static void free_ctx(simox_ctx* c) {
     if (!c) return;
     prof_collect(c);
     drop_graphs(c);
+    adjoint_free(c);
     pme_free(c);
     void* bufs[] = {c->id, c->x, c->v, c->f, c->q, c->xm, c->cell_of, c->cell_xyz, c->cell_count, c->cell_start, c->cell_fill,
                     c->sorted, c->pair13, c->entries, c->xq_s, c->t_s, c->rec_s, c->frec_s, c->nn, c->nbr, c->nn_max, c->nn_tot,

@@ -32,10 +32,6 @@ constexpr int CT_THREADS = 256;
 // scalar slots in c->line
 enum : int { L_GSUM_OLD = 0, L_ALPHA, L_ERROR, L_DONE, L_NEVAL, L_END };
 
-struct CtipSpecies {
-    double chi[5], Jp[5], qmin[5], qmax[5], Z[5];
-};
-
 struct CtipParams {
     double3 box, ibox;
     double a, kc;
@@ -366,7 +362,7 @@ int ctip_alloc(simox_ctx* c) {
     return ok ? SIMOX_OK : SIMOX_E_NOMEM;
 }
 
-static CtipSpecies ctip_species(const simox_ctx* c) {
+CtipSpecies ctip_species(const simox_ctx* c) {
     CtipSpecies S;
     const double kc_const = SX_KC * 2.0 * c->a / SX_SQRTPI;   // ctip.f90:31
     for (int s = 0; s < 5; s++) {
@@ -401,13 +397,13 @@ static void launch_ctip_pair(simox_ctx* c, const PairTab<R>* tab, const double* 
                                                                     nullptr, S);
 }
 
-static void ctip_pair(simox_ctx* c, const double* vin, double* out, double* cconst, const CtipSpecies& S) {
+void ctip_pair(simox_ctx* c, const double* vin, double* out, double* cconst, const CtipSpecies& S) {
     Launch L(c, cconst ? "ctip_setup_pairs" : "ctip_matvec_pairs");
     if (c->precision == SIMOX_MIXED) launch_ctip_pair<float>(c, c->tab_f, vin, out, cconst, S);
     else launch_ctip_pair<double>(c, c->tab_d, vin, out, cconst, S);
 }
 
-int ctip_solve(simox_ctx* c, int max_cg, simox_ctip_report* rep) {
+int ctip_solve(simox_ctx* c, int max_cg, simox_ctip_report* rep, double tol) {
     if (!c->psi_valid) return SIMOX_E_STATE;
     int st = ensure_list(c);
     if (st) return st;
@@ -459,7 +455,7 @@ int ctip_solve(simox_ctx* c, int max_cg, simox_ctip_report* rep) {
         }
         {
             Launch L(c, "ctip_brent");
-            ctip_brent_kernel<<<1, 1024, 0, s>>>(c->t_s, c->qs, c->pv, c->act, nact, S, c->line, c->acc, 1.0e-3,
+            ctip_brent_kernel<<<1, 1024, 0, s>>>(c->t_s, c->qs, c->pv, c->act, nact, S, c->line, c->acc, tol,
                                                  c->status);
         }
         {

@@ -667,6 +667,145 @@ int pme_forces(simox_ctx* c, bool finalize, bool eflag, double* f_store) {
     return check_launch(c);
 }
 
+// ---------------------------------------------------------------------------
+// Charge adjoint of the PME forces (FP64 grids).  With a weight field w on
+// the atoms (mean already removed, as the mean-force subtraction of
+// force.f90:455-460 requires), S = sum_i w_i . F_i^rec and
+// F_i^rec = -cst q_i g_i, g_i = grad of the interpolated (G*Q) at x_i, so
+//   dS/dq_m = -cst [ w_m . g_m + sum_grid W~_m (G*D) ],
+//   D(grid) = sum_i q_i w_i . grad W_i(grid),
+// W~ the spread weights (rounded to single precision as the spread rounds
+// them, force.f90:406) and grad W the unrounded weight derivatives that the
+// force gather uses.
+template <int P>
+__global__ void __launch_bounds__(128)
+    field_dot_kernel(PmeParams S, const double4* __restrict__ xq, const double* __restrict__ grid,
+                     const double* __restrict__ wt, double* __restrict__ out, double scale) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= S.n) return;
+    const double4 a = xq[k];
+    double wx[P], wy[P], wz[P], dx[P], dy[P], dz[P];
+    const double ux = (double)S.K.x * (a.x + S.box.x * 0.5) / S.box.x;
+    const double uy = (double)S.K.y * (a.y + S.box.y * 0.5) / S.box.y;
+    const double uz = (double)S.K.z * (a.z + S.box.z * 0.5) / S.box.z;
+    bspline_w<P>(ux, wx, dx);
+    bspline_w<P>(uy, wy, dy);
+    bspline_w<P>(uz, wz, dz);
+    const int bx = __double2int_rz(ux) - P / 2 + 1;
+    const int by = __double2int_rz(uy) - P / 2 + 1;
+    const int bz = __double2int_rz(uz) - P / 2 + 1;
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int c = 0; c < P; c++) {
+        const size_t gz = (size_t)wrapi(bz + c, S.K.z) * S.K.y;
+        for (int b = 0; b < P; b++) {
+            const size_t gyz = (gz + wrapi(by + b, S.K.y)) * S.K.x;
+            for (int aa = 0; aa < P; aa++) {
+                const double g = grid[gyz + wrapi(bx + aa, S.K.x)];
+                sx += dx[aa] * wy[b] * wz[c] * g;
+                sy += wx[aa] * dy[b] * wz[c] * g;
+                sz += wx[aa] * wy[b] * dz[c] * g;
+            }
+        }
+    }
+    out[k] += scale * (wt[3 * k] * sx * S.kx.x + wt[3 * k + 1] * sy * S.kx.y + wt[3 * k + 2] * sz * S.kx.z);
+}
+
+template <int P>
+__global__ void __launch_bounds__(128)
+    spread_dipole_kernel(PmeParams S, const double4* __restrict__ xq, const double* __restrict__ wt,
+                         double* __restrict__ grid) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= S.n) return;
+    const double4 a = xq[k];
+    if (a.w == 0.0) return;
+    double wx[P], wy[P], wz[P], dx[P], dy[P], dz[P];
+    const double ux = (double)S.K.x * (a.x + S.box.x * 0.5) / S.box.x;
+    const double uy = (double)S.K.y * (a.y + S.box.y * 0.5) / S.box.y;
+    const double uz = (double)S.K.z * (a.z + S.box.z * 0.5) / S.box.z;
+    bspline_w<P>(ux, wx, dx);
+    bspline_w<P>(uy, wy, dy);
+    bspline_w<P>(uz, wz, dz);
+    const int bx = __double2int_rz(ux) - P / 2 + 1;
+    const int by = __double2int_rz(uy) - P / 2 + 1;
+    const int bz = __double2int_rz(uz) - P / 2 + 1;
+    const double px = a.w * wt[3 * k] * S.kx.x, py = a.w * wt[3 * k + 1] * S.kx.y, pz = a.w * wt[3 * k + 2] * S.kx.z;
+    for (int c = 0; c < P; c++) {
+        const size_t gz = (size_t)wrapi(bz + c, S.K.z) * S.K.y;
+        for (int b = 0; b < P; b++) {
+            const size_t gyz = (gz + wrapi(by + b, S.K.y)) * S.K.x;
+            for (int aa = 0; aa < P; aa++) {
+                const double v = px * dx[aa] * wy[b] * wz[c] + py * wx[aa] * dy[b] * wz[c] + pz * wx[aa] * wy[b] * dz[c];
+                atomicAdd(grid + gyz + wrapi(bx + aa, S.K.x), v);
+            }
+        }
+    }
+}
+
+template <int P>
+__global__ void __launch_bounds__(128)
+    gather_rounded_kernel(PmeParams S, const double4* __restrict__ xq, const double* __restrict__ grid,
+                          double* __restrict__ out, double scale) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= S.n) return;
+    const double4 a = xq[k];
+    double wx[P], wy[P], wz[P], d[P];
+    const double ux = (double)S.K.x * (a.x + S.box.x * 0.5) / S.box.x;
+    const double uy = (double)S.K.y * (a.y + S.box.y * 0.5) / S.box.y;
+    const double uz = (double)S.K.z * (a.z + S.box.z * 0.5) / S.box.z;
+    bspline_w<P>(ux, wx, d);
+    bspline_w<P>(uy, wy, d);
+    bspline_w<P>(uz, wz, d);
+    const int bx = __double2int_rz(ux) - P / 2 + 1;
+    const int by = __double2int_rz(uy) - P / 2 + 1;
+    const int bz = __double2int_rz(uz) - P / 2 + 1;
+    double sum = 0.0;
+    for (int c = 0; c < P; c++) {
+        const size_t gz = (size_t)wrapi(bz + c, S.K.z) * S.K.y;
+        for (int b = 0; b < P; b++) {
+            const size_t gyz = (gz + wrapi(by + b, S.K.y)) * S.K.x;
+            for (int aa = 0; aa < P; aa++)
+                sum += (double)(float)(wx[aa] * wy[b] * wz[c]) * grid[gyz + wrapi(bx + aa, S.K.x)];
+        }
+    }
+    out[k] += scale * sum;
+}
+
+template <int P>
+static int force_charge_adjoint_t(simox_ctx* c, PmeRes& Rs, const double* wt, double* out) {
+    PmeParams S = pme_params(c);
+    const int nb = (S.n + 127) / 128;
+    run_spread<double, P>(c, Rs, S, nullptr);
+    int st = run_convolution(c, Rs, false);
+    if (st) return st;
+    {
+        Launch L(c, "adjoint_pme_field");
+        field_dot_kernel<P><<<nb, 128, 0, c->stream>>>(S, c->xq_s, (const double*)Rs.grid, wt, out, -S.cst);
+    }
+    cudaMemsetAsync(Rs.grid, 0, c->ngrid * sizeof(double), c->stream);
+    {
+        Launch L(c, "adjoint_pme_dipole_spread");
+        spread_dipole_kernel<P><<<nb, 128, 0, c->stream>>>(S, c->xq_s, wt, (double*)Rs.grid);
+    }
+    if ((st = run_convolution(c, Rs, false))) return st;
+    Launch L(c, "adjoint_pme_dipole_gather");
+    gather_rounded_kernel<P><<<nb, 128, 0, c->stream>>>(S, c->xq_s, (const double*)Rs.grid, out, -S.cst);
+    return check_launch(c);
+}
+
+// out (sorted order) += dS/dq for S = sum_i wt_i . F_i^rec (FP64 context)
+int pme_force_charge_adjoint(simox_ctx* c, const double* wt, double* out) {
+    if (!c->psi_valid) return SIMOX_E_STATE;
+    if (c->n == 0) return SIMOX_OK;
+    PmeRes& Rs = c->pme[0];
+    if (!Rs.dbl) return SIMOX_E_UNSUPPORTED;
+    switch (c->order) {
+        case 4: return force_charge_adjoint_t<4>(c, Rs, wt, out);
+        case 6: return force_charge_adjoint_t<6>(c, Rs, wt, out);
+        case 8: return force_charge_adjoint_t<8>(c, Rs, wt, out);
+        default: return SIMOX_E_ARG;
+    }
+}
+
 // CTIP's PME potential runs on the FP64 grid in both precision modes: with
 // the FP32 grid the charges of the reference's nonlinear CG drift by ~3e-6 e
 // over a thousand iterations (measured on 500-600 atom Al/O systems), above

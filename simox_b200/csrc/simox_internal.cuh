@@ -87,6 +87,10 @@ struct Profile {
 
 }  // namespace sx
 
+namespace sx {
+struct AdjointState;
+}
+
 struct simox_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;      // the stream every entry point issues on
@@ -107,6 +111,8 @@ struct simox_ctx {
     size_t ngrid = 0, nhalf = 0;
     int npt_max = SIMOX_NPT_MAX, nnb_cap = 1024;
     int force_splits = 2;       // CTAs per skin cell of the mixed force pass (simox_set_tuning)
+    sx::AdjointState* adj = nullptr;   // parameter-adjoint model (simox_set_eam_spline)
+    bool spline_on = false;
 
     // species present
     bool has_h = false;
@@ -271,8 +277,18 @@ int pme_forces(simox_ctx* c, bool finalize, bool eflag, double* f_store = nullpt
 void pme_bind_stream(simox_ctx* c);
 int pme_potential(simox_ctx* c, const double* charges_sorted, double* phi_out, double scale);
 int pme_finalize_forces(simox_ctx* c);
+int pme_force_charge_adjoint(simox_ctx* c, const double* wt, double* out);
+// adjoint.cu
+void adjoint_free(simox_ctx* c);
 // ctip.cu
-int ctip_solve(simox_ctx* c, int max_cg, simox_ctip_report* rep);
+struct CtipSpecies {
+    double chi[5], Jp[5], qmin[5], qmax[5], Z[5];
+};
+
+int ctip_solve(simox_ctx* c, int max_cg, simox_ctip_report* rep, double tol = 1.0e-3);
+CtipSpecies ctip_species(const simox_ctx* c);
+// out = sum_Y sym_XY vin_Y (sorted order); cconst (may be null) = chi + sum_Y Z_Y asym_XY
+void ctip_pair(simox_ctx* c, const double* vin, double* out, double* cconst, const CtipSpecies& S);
 int ctip_alloc(simox_ctx* c);
 // integrate.cu
 int vv1(simox_ctx* c, double dt, bool reflect);
