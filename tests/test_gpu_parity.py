@@ -400,3 +400,29 @@ def test_nve_drift_mixed_not_worse_than_fp64():
         t = np.arange(1, len(E) + 1) * 0.1   # ps
         slope[prec] = np.polyfit(t, np.array(E), 1)[0] / s.n
     assert abs(slope["mixed"]) <= 1.1 * abs(slope["fp64"]) + 1e-4, slope
+
+
+def test_oxidation_slab_full_size_mixed_vs_fp64():
+    """The 472,000-atom oxidation slab (fcc Al 60x60x30 plus 40,000 O at
+    0.02 A^-3, PME 256x256x384, order 6) with neutral test charges (Al +x,
+    O -0.6 e): mixed FORCE + PME within 1e-5 (relative norm) of the FP64 path,
+    then two oxidation-mode steps (VV_NVE1_REFLECT) keep every atom below the
+    top wall and the total charge unchanged."""
+    s = S.oxidation_slab()
+    q = np.where(s.ids == 4, -0.6, 0.0)
+    q[s.ids == 1] = 0.6 * (s.ids == 4).sum() / (s.ids == 1).sum()
+    s.q = q
+    out = {}
+    for prec in ("fp64", "mixed"):
+        with gpu_context(s, precision=prec) as g:
+            g.pme_self()
+            g.cell_sort()
+            g.force(energies=False)
+            g.pme(energies=False)
+            out[prec] = g.get_state()["f"]
+            if prec == "mixed":
+                g.md_run(2, 0.5 / S.TFM, first_step=2, reflect=True, freq_stat=1000)
+                st = g.get_state()
+                assert np.all(st["x"][:, 2] <= s.box[2] / 2) and np.isfinite(st["x"]).all()
+                assert abs(st["q"].sum() - q.sum()) <= 1e-9
+    assert rel_err(out["mixed"], out["fp64"]) <= 1e-5, rel_err(out["mixed"], out["fp64"])
