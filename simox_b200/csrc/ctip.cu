@@ -30,7 +30,7 @@ namespace sx {
 constexpr int CT_THREADS = 256;
 
 // scalar slots in c->line
-enum : int { L_GSUM_OLD = 0, L_ALPHA, L_ERROR, L_DONE, L_NEVAL, L_END };
+enum : int { L_GSUM_OLD = 0, L_ALPHA, L_ERROR, L_DONE, L_NEVAL, L_ITERS, L_CHUNK, L_END };
 
 struct CtipParams {
     double3 box, ibox;
@@ -403,6 +403,124 @@ void ctip_pair(simox_ctx* c, const double* vin, double* out, double* cconst, con
     else launch_ctip_pair<double>(c, c->tab_d, vin, out, cconst, S);
 }
 
+// One nonlinear-CG iteration (ctip.f90:169-190): direction with the
+// reference's beta, mean projection, A p (PME potential + short-range pairs),
+// the Brent line search and the update.  Every launch goes to c->stream, so
+// the iteration can be captured into a graph body.
+static int ctip_iteration(simox_ctx* c, const CtipSpecies& S, double c_pme, double tol, int* nact, int nb) {
+    const int n = c->n;
+    cudaStream_t s = c->stream;
+    cudaMemsetAsync(nact, 0, sizeof(int), s);
+    {
+        Launch L(c, "ctip_direction");
+        ctip_dir_kernel<<<nb, CT_THREADS, 0, s>>>(n, c->g, c->pv, c->line, c->acc);
+    }
+    {
+        Launch L(c, "ctip_project");
+        ctip_proj_kernel<<<nb, CT_THREADS, 0, s>>>(n, c->pv, c->acc);
+    }
+    if (int st = pme_potential(c, c->pv, c->Ap, c_pme)) return st;
+    ctip_pair(c, c->pv, c->jp, nullptr, S);
+    {
+        Launch L(c, "ctip_matvec_finish");
+        ctip_matvec_finish_kernel<<<nb, CT_THREADS, 0, s>>>(n, c->t_s, c->qs, c->g, c->pv, c->jp, c->Ap, S, c->act,
+                                                           nact, c->acc);
+    }
+    {
+        Launch L(c, "ctip_brent");
+        ctip_brent_kernel<<<1, 1024, 0, s>>>(c->t_s, c->qs, c->pv, c->act, nact, S, c->line, c->acc, tol, c->status);
+    }
+    {
+        Launch L(c, "ctip_update");
+        ctip_update_kernel<<<nb, CT_THREADS, 0, s>>>(n, c->t_s, c->qs, c->g, c->pv, c->Ap, S, c->line, c->acc);
+    }
+    return check_launch(c);
+}
+
+// Device-side loop: the iteration is the body of a CUDA graph WHILE node whose
+// condition this kernel sets after every iteration.  One graph launch runs at
+// most kCgChunk iterations, so every launch ends after a bounded time and the
+// host checks the status between launches.
+constexpr int kCgChunk = 256;
+
+__global__ void ctip_loop_cond_kernel(cudaGraphConditionalHandle h, double* __restrict__ line,
+                                      const int* __restrict__ status, int max_cg, int chunk) {
+    const double k = line[L_ITERS] + 1.0;
+    const double kc = line[L_CHUNK] + 1.0;
+    line[L_ITERS] = k;
+    line[L_CHUNK] = kc;
+    const bool stop = line[L_DONE] != 0.0 || *status != 0 || !isfinite(line[L_ERROR]) ||
+                      (max_cg > 0 && k >= (double)max_cg) || kc >= (double)chunk;
+    cudaGraphSetConditional(h, stop ? 0u : 1u);
+}
+
+// Runs the CG loop as graph launches.  *used = false (nothing run) when the
+// graph cannot be built here; the caller then runs the host-driven loop.
+static int ctip_device_loop(simox_ctx* c, const CtipSpecies& S, double c_pme, double tol, int* nact, int nb,
+                            int max_cg, int* k_out, double hbuf[4], bool* used) {
+    *used = false;
+    cudaStream_t s = c->stream;
+    cudaGraph_t outer = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    if (cudaGraphCreate(&outer, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return SIMOX_OK;
+    }
+    cudaGraphConditionalHandle h;
+    cudaGraphNodeParams np{};
+    cudaGraphNode_t node;
+    bool ok = cudaGraphConditionalHandleCreate(&h, outer, 1u, cudaGraphCondAssignDefault) == cudaSuccess;
+    if (ok) {
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        ok = cudaGraphAddNode(&node, outer, nullptr, 0, &np) == cudaSuccess;
+    }
+    long long per_iter = 0;
+    int st = SIMOX_OK;
+    if (ok) {
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        ok = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+             cudaSuccess;
+        if (ok) {
+            const long long l0 = c->launches;
+            st = ctip_iteration(c, S, c_pme, tol, nact, nb);
+            ctip_loop_cond_kernel<<<1, 1, 0, s>>>(h, c->line, c->status, max_cg, kCgChunk);
+            cudaGraph_t cap = nullptr;
+            ok = cudaStreamEndCapture(s, &cap) == cudaSuccess && st == SIMOX_OK;
+            per_iter = c->launches - l0 + 1;
+            c->launches = l0;
+        }
+        ok = ok && cudaGraphInstantiate(&exec, outer, 0) == cudaSuccess;
+    }
+    cudaGetLastError();
+    if (!ok) {
+        if (exec) cudaGraphExecDestroy(exec);
+        cudaGraphDestroy(outer);
+        return st;
+    }
+    *used = true;
+    double lb[6] = {0.0, 1.0, 0.0, 0.0, 0.0, 0.0};
+    int k = 0;
+    while (true) {
+        cudaMemsetAsync(c->line + L_CHUNK, 0, sizeof(double), s);
+        if ((st = cuda_status(cudaGraphLaunch(exec, s)))) break;
+        cudaMemcpyAsync(lb, c->line + L_ALPHA, sizeof(double) * 6, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(c->h_status, c->status, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if ((st = cuda_status(cudaStreamSynchronize(s)))) break;
+        const int k_now = (int)lb[4];
+        c->launches += per_iter * (long long)(k_now - k);
+        k = k_now;
+        if (*c->h_status || lb[2] != 0.0 || !std::isfinite(lb[1]) || (max_cg > 0 && k >= max_cg)) break;
+    }
+    for (int i = 0; i < 4; i++) hbuf[i] = lb[i];
+    *k_out = k;
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(outer);
+    return st;
+}
+
 int ctip_solve(simox_ctx* c, int max_cg, simox_ctip_report* rep, double tol) {
     if (!c->psi_valid) return SIMOX_E_STATE;
     int st = ensure_list(c);
@@ -434,34 +552,18 @@ int ctip_solve(simox_ctx* c, int max_cg, simox_ctip_report* rep, double tol) {
     }
     int k = 0;
     double err = 1.0;
-    double hbuf[4];
-    while (true) {
+    double hbuf[4] = {0.0, 1.0, 0.0, 0.0};
+    bool device_loop = false;
+    if (!c->profiling && (st = ctip_device_loop(c, S, c_pme, tol, nact, nb, max_cg, &k, hbuf, &device_loop))) return st;
+    if (device_loop) {
+        err = hbuf[1];
+        if (*c->h_status) st = read_status(c);                            // Brent limit (ctip.f90:302)
+        else if (!std::isfinite(err)) st = SIMOX_E_BRENT;
+        else if (hbuf[2] == 0.0 && max_cg > 0 && k >= max_cg) st = SIMOX_E_CG_LIMIT;
+    }
+    while (!device_loop) {
         if (max_cg > 0 && k >= max_cg) { st = SIMOX_E_CG_LIMIT; break; }
-        cudaMemsetAsync(nact, 0, sizeof(int), s);
-        {
-            Launch L(c, "ctip_direction");
-            ctip_dir_kernel<<<nb, CT_THREADS, 0, s>>>(n, c->g, c->pv, c->line, c->acc);
-        }
-        {
-            Launch L(c, "ctip_project");
-            ctip_proj_kernel<<<nb, CT_THREADS, 0, s>>>(n, c->pv, c->acc);
-        }
-        if ((st = pme_potential(c, c->pv, c->Ap, c_pme))) return st;
-        ctip_pair(c, c->pv, c->jp, nullptr, S);
-        {
-            Launch L(c, "ctip_matvec_finish");
-            ctip_matvec_finish_kernel<<<nb, CT_THREADS, 0, s>>>(n, c->t_s, c->qs, c->g, c->pv, c->jp, c->Ap, S, c->act,
-                                                               nact, c->acc);
-        }
-        {
-            Launch L(c, "ctip_brent");
-            ctip_brent_kernel<<<1, 1024, 0, s>>>(c->t_s, c->qs, c->pv, c->act, nact, S, c->line, c->acc, tol,
-                                                 c->status);
-        }
-        {
-            Launch L(c, "ctip_update");
-            ctip_update_kernel<<<nb, CT_THREADS, 0, s>>>(n, c->t_s, c->qs, c->g, c->pv, c->Ap, S, c->line, c->acc);
-        }
+        if ((st = ctip_iteration(c, S, c_pme, tol, nact, nb))) return st;
         k++;
         cudaMemcpyAsync(hbuf, c->line + L_ALPHA, sizeof(double) * 4, cudaMemcpyDeviceToHost, s);
         cudaMemcpyAsync(c->h_status, c->status, sizeof(int), cudaMemcpyDeviceToHost, s);
