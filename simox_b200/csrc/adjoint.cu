@@ -645,7 +645,7 @@ static int proj_cg(simox_ctx* c, const CtipSpecies& S, double c_pme, double* b, 
             cudaMemsetAsync(s + 2, 0, sizeof(double), c->stream);
             adj_dot<<<nb, 256, 0, c->stream>>>(n, A->p, A->Hp, s + 2);
             const double pHp = host_scalar(c, s, 2);
-            if (!(pHp > 0.0)) break;
+            if (!(pHp > 0.0)) break;   // not positive definite along p: keep the iterate so far
             double h[2] = {rr / pHp, 0.0};
             cudaMemcpyAsync(s + 4, h, sizeof(double), cudaMemcpyHostToDevice, c->stream);
             adj_axpy<<<nb, 256, 0, c->stream>>>(n, s, 4, 1.0, A->p, x);
@@ -696,10 +696,25 @@ int adjoint_eval(simox_ctx* c, const double* f_target, simox_adjoint_report* rep
         if (Uout) *Uout = host_scalar(c, A->scal, 0);
         return check_launch(c);
     };
+    // ||P G|| at the current charges (G from grad_u)
+    auto resid = [&]() -> double {
+        cudaMemcpyAsync(A->r, A->G, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
+        cudaMemsetAsync(A->scal, 0, sizeof(double) * 8, s);
+        adj_dot<<<nb, 256, 0, s>>>(n, A->r, nullptr, A->scal);
+        adj_sub_mean<<<nb, 256, 0, s>>>(n, A->scal, A->r);
+        cudaMemsetAsync(A->scal + 1, 0, sizeof(double), s);
+        adj_dot<<<nb, 256, 0, s>>>(n, A->r, A->r, A->scal + 1);
+        return std::sqrt(host_scalar(c, A->scal, 1));
+    };
+    // Safeguarded Newton: the CTIP functional is convex only where the charge
+    // penalties hold it (J' is smaller than the Coulomb coupling of an
+    // alternating charge pattern), so a step is solved on the current active
+    // set and accepted (halving up to 4 times) only if it lowers ||P G||.
     double Uq = 0.0;
-    for (int it = 0; it < 4; it++) {
-        if ((st = grad_u(nullptr))) return st;
-        // b = -G, x = 0
+    if ((st = grad_u(nullptr))) return st;
+    double rn = resid();
+    const double abs_tol = 1e-11 * std::sqrt((double)n);
+    for (int it = 0; it < 8 && rn > abs_tol; it++) {
         cudaMemsetAsync(A->lam, 0, sizeof(double) * n, s);
         {
             double m1 = -1.0;
@@ -708,17 +723,28 @@ int adjoint_eval(simox_ctx* c, const double* f_target, simox_adjoint_report* rep
             adj_axpy<<<nb, 256, 0, s>>>(n, A->scal, 4, 1.0, A->G, A->r);   // r = -G
         }
         int its = 0;
-        double rel = 0.0, nrm = 0.0;
-        if ((st = proj_cg(c, S, c_pme, A->r, A->lam, 1e-13, 2000, &its, &rel, 1e-11 * std::sqrt((double)n), &nrm)))
-            return st;
-        if (its == 0) break;   // already stationary to FP64 noise
-        // q += delta (lam holds delta here)
-        {
-            double one = 1.0;
-            cudaMemcpyAsync(A->scal + 5, &one, sizeof(double), cudaMemcpyHostToDevice, s);
+        double rel = 0.0;
+        if ((st = proj_cg(c, S, c_pme, A->r, A->lam, 1e-13, 2000, &its, &rel))) return st;
+        // trial charges q + t delta; the accepted step stays in qs
+        cudaMemcpyAsync(A->gam, c->qs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);   // saved q (gam is free here)
+        bool accepted = false;
+        double t = 1.0;
+        for (int ls = 0; ls < 5 && !accepted; ls++, t *= 0.5) {
+            cudaMemcpyAsync(c->qs, A->gam, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(A->scal + 5, &t, sizeof(double), cudaMemcpyHostToDevice, s);
             adj_axpy<<<nb, 256, 0, s>>>(n, A->scal, 5, 1.0, A->lam, c->qs);
+            if ((st = grad_u(nullptr))) return st;
+            const double rt = resid();
+            if (rt < rn) {
+                rn = rt;
+                accepted = true;
+            }
         }
         R.n_newton = it + 1;
+        if (!accepted) {   // no step lowers the residual: keep the previous charges
+            cudaMemcpyAsync(c->qs, A->gam, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
+            break;
+        }
     }
     if ((st = grad_u(&Uq))) return st;
     {   // residual ||P G||

@@ -406,6 +406,62 @@ __device__ __forceinline__ int filter_group(const FilterParams& F, const float4*
     return out;
 }
 
+// One atom of pass 1: filter X's skin row into its exact row, sum its density,
+// embedding derivative and list statistics.
+template <typename R>
+__device__ __forceinline__ void filter_atom(const FilterParams& F, const float4* ssh, const DensC<R>* dsh,
+                                            const int* dflag, int X, const double4* __restrict__ xq,
+                                            const float4* __restrict__ rec, const int* __restrict__ order,
+                                            const int2* __restrict__ nn_s, const unsigned* __restrict__ nbr_s,
+                                            int2* __restrict__ nn, unsigned* __restrict__ nbr, const EmbedParams& E,
+                                            double* __restrict__ rho_s, double* __restrict__ dF_s,
+                                            float* __restrict__ dF_f, int* __restrict__ status, int& lmax,
+                                            unsigned long long& ltot, int& bad, int g0) {
+    constexpr bool F32 = std::is_same<R, float>::value;
+    const PairParams& P = F.pp;
+    const int lane = threadIdx.x & 31;
+    const float4 ra = rec[X];
+    const unsigned wa = __float_as_uint(ra.w);
+    const int sX = (int)(wa >> 27);
+    const int ax = wa & 511, ay = (wa >> 9) & 511, az = (wa >> 18) & 511;
+    // the "-1" neighbours of X's reference cell on each axis (periodic)
+    const int xm = ax == 0 ? F.nc.x - 1 : ax - 1;
+    const int ym = ay == 0 ? F.nc.y - 1 : ay - 1;
+    const int zm = az == 0 ? F.nc.z - 1 : az - 1;
+    const int oX = order[X];
+    const double4 xa = F32 ? make_double4(0, 0, 0, 0) : xq[X];
+    const int2 ms = nn_s[X];
+    const unsigned* srow = nbr_s + (size_t)X * F.cap_s;
+    unsigned* row = nbr + (size_t)X * P.cap;
+    double rho = 0.0;
+    int out0, out1;
+    if (g0 >= 0)
+        out0 = filter_group<R, 0, true>(F, ssh, dsh, dflag, sX, g0, srow, ms.x, row, ra, wa, xm, ym, zm, oX, xa,
+                                        X, xq, rec, order, rho, bad);
+    else
+        out0 = filter_group<R, 0, false>(F, ssh, dsh, dflag, sX, 0, srow, ms.x, row, ra, wa, xm, ym, zm, oX, xa,
+                                         X, xq, rec, order, rho, bad);
+    out1 = filter_group<R, 1, true>(F, ssh, dsh, dflag, sX, 3, srow + (F.cap_s - 1), ms.y, row + (P.cap - 1), ra,
+                                    wa, xm, ym, zm, oX, xa, X, xq, rec, order, rho, bad);
+    rho = warp_sum(rho);
+    if (lane == 0) {
+        const int tot = out0 + out1;
+        if (tot > P.cap) {
+            atomicOr(status, ST_NBR_OVERFLOW);
+            nn[X] = make_int2(0, 0);
+        } else {
+            nn[X] = make_int2(out0, out1);
+        }
+        lmax = max(lmax, tot);
+        ltot += (unsigned long long)tot;
+        double Fe, dF;
+        if (embed(E, sX, rho, Fe, dF)) bad |= ST_UNKNOWN_ELEMENT;
+        rho_s[X] = rho;
+        dF_s[X] = dF;
+        dF_f[X] = (float)dF;
+    }
+}
+
 template <typename R>
 __global__ void __launch_bounds__(256)
     filter_density_kernel(FilterParams F, const PairTab<R>* __restrict__ tab, const double4* __restrict__ xq,
@@ -444,48 +500,9 @@ __global__ void __launch_bounds__(256)
     const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
     int lmax = 0, bad = 0;
     unsigned long long ltot = 0;
-    for (int X = blockIdx.x * wpb + (threadIdx.x >> 5); X < P.n; X += gridDim.x * wpb) {
-        const float4 ra = rec[X];
-        const unsigned wa = __float_as_uint(ra.w);
-        const int sX = (int)(wa >> 27);
-        const int ax = wa & 511, ay = (wa >> 9) & 511, az = (wa >> 18) & 511;
-        // the "-1" neighbours of X's reference cell on each axis (periodic)
-        const int xm = ax == 0 ? F.nc.x - 1 : ax - 1;
-        const int ym = ay == 0 ? F.nc.y - 1 : ay - 1;
-        const int zm = az == 0 ? F.nc.z - 1 : az - 1;
-        const int oX = order[X];
-        const double4 xa = F32 ? make_double4(0, 0, 0, 0) : xq[X];
-        const int2 ms = nn_s[X];
-        const unsigned* srow = nbr_s + (size_t)X * F.cap_s;
-        unsigned* row = nbr + (size_t)X * P.cap;
-        double rho = 0.0;
-        int out0, out1;
-        if (g0 >= 0)
-            out0 = filter_group<R, 0, true>(F, ssh, dsh, dflag, sX, g0, srow, ms.x, row, ra, wa, xm, ym, zm, oX, xa,
-                                            X, xq, rec, order, rho, bad);
-        else
-            out0 = filter_group<R, 0, false>(F, ssh, dsh, dflag, sX, 0, srow, ms.x, row, ra, wa, xm, ym, zm, oX, xa,
-                                             X, xq, rec, order, rho, bad);
-        out1 = filter_group<R, 1, true>(F, ssh, dsh, dflag, sX, 3, srow + (F.cap_s - 1), ms.y, row + (P.cap - 1), ra,
-                                        wa, xm, ym, zm, oX, xa, X, xq, rec, order, rho, bad);
-        rho = warp_sum(rho);
-        if (lane == 0) {
-            const int tot = out0 + out1;
-            if (tot > P.cap) {
-                atomicOr(status, ST_NBR_OVERFLOW);
-                nn[X] = make_int2(0, 0);
-            } else {
-                nn[X] = make_int2(out0, out1);
-            }
-            lmax = max(lmax, tot);
-            ltot += (unsigned long long)tot;
-            double Fe, dF;
-            if (embed(E, sX, rho, Fe, dF)) bad |= ST_UNKNOWN_ELEMENT;
-            rho_s[X] = rho;
-            dF_s[X] = dF;
-            dF_f[X] = (float)dF;
-        }
-    }
+    for (int X = blockIdx.x * wpb + (threadIdx.x >> 5); X < P.n; X += gridDim.x * wpb)
+        filter_atom<R>(F, ssh, dsh, dflag, X, xq, rec, order, nn_s, nbr_s, nn, nbr, E, rho_s, dF_s, dF_f,
+                              status, lmax, ltot, bad, g0);
     if (bad) atomicOr(status, bad);
     if (lane == 0) {
         if (lmax) atomicMax(nn_max, lmax);
@@ -739,20 +756,6 @@ __device__ __forceinline__ v2 pair_fs_pk(const PackTab& T, const PackParams& Q, 
     return ((eam + ew) + ct) * ir;
 }
 
-// Per-thread asynchronous copies global -> shared (cp.async, PTX ISA): the
-// partner records of later batches are in flight while a batch is computed,
-// without holding registers.
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // Cell-tiled force pass.  Atoms are in skin-cell order, and every entry of a
 // row names its partner's cell by the stencil position e (0..26) relative to
