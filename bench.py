@@ -402,6 +402,55 @@ def run_batch(args):
     return 0
 
 
+def run_adjoint(args):
+    """--adjoint: the parameter-gradient workload -- seeded snapshots of
+    2000-atom Al/O systems (O fraction 0.1-0.5, 300-1000 K), synthetic
+    targets = the FP64 model forces plus Gaussian noise (0.05 eV/A); per
+    snapshot the charges, forces and the gradients of the energy and of the
+    force-matching loss with respect to 3 x 64 spline coefficients and chi, J,
+    Z (FP64, one adjoint CG through the charge solve).  Reports snapshots/s
+    and the summed loss gradient's size.  Not the headline metric."""
+    from simox_b200 import api, build, spline, systems as S
+    build.build()
+    rng = np.random.default_rng(11)
+    P = api.default_potential()
+    spl = spline.fit(P)
+    ctxs, targets = [], []
+    for k in range(args.adjoint):
+        s = S.replica(int(rng.integers(1 << 30)), 2000, float(rng.uniform(0.1, 0.5)), float(rng.uniform(300, 1000)))
+        g = api.from_system(s, precision="fp64")
+        g.pme_self()
+        g.cell_sort()
+        g.set_eam_spline(spl)
+        _, f0, _, _ = g.adjoint_eval(gradients=False)
+        targets.append(f0 + rng.normal(0.0, 0.05, f0.shape))
+        ctxs.append(g)
+    for g, t in zip(ctxs, targets):      # warm-up: charges converged at these parameters
+        g.adjoint_eval(t)
+    t0 = time.perf_counter()
+    gE = gL = None
+    reps = []
+    for g, t in zip(ctxs, targets):
+        rep, _, e, l = g.adjoint_eval(t)
+        reps.append(rep)
+        gE = e if gE is None else gE + e
+        gL = l if gL is None else gL + l
+    el = time.perf_counter() - t0
+    line = {"metric": "parameter-gradient snapshots/s (2000-atom Al/O, FP64 adjoint)", "value": len(ctxs) / el,
+            "unit": "snapshots/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{len(ctxs)} seeded snapshots of 2000 atoms, targets = model forces + N(0, 0.05)",
+                       "parameters": "3 x 64 spline coefficients + chi, J, Z of 5 species (207)"},
+            "ms_per_snapshot": el / len(ctxs) * 1e3,
+            "mean_adjoint_cg_iterations": float(np.mean([r["n_adjoint"] for r in reps])),
+            "max_charge_residual": float(max(r["residual"] for r in reps)),
+            "loss_total": float(sum(r["loss"] for r in reps)),
+            "grad_L_norm": float(np.linalg.norm(gL)), "grad_E_norm": float(np.linalg.norm(gE))}
+    for g in ctxs:
+        g.close()
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -418,7 +467,11 @@ def main():
                     help="--ncu: energies on steps with MOD(step, freq_stat) == 0 (1: every step)")
     ap.add_argument("--batch", type=int, default=0,
                     help="run the batched-replica workload with this many systems (256 in its configuration)")
+    ap.add_argument("--adjoint", type=int, default=0,
+                    help="run the parameter-gradient workload with this many snapshots (32 in its configuration)")
     args = ap.parse_args()
+    if args.adjoint:
+        return run_adjoint(args)
     if args.batch:
         return run_batch(args)
     if args.impl == "reference":
