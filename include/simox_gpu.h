@@ -280,6 +280,13 @@ int simox_set_ctip_params(simox_ctx* ctx, int species, double chi, double J, dou
  * loss gradient runs one adjoint CG (FP64) through the charge solve. */
 int simox_adjoint_eval(simox_ctx* ctx, const double* f_target, simox_adjoint_report* rep,
                        double* forces, double* grad_E, double* grad_L);
+/* simox_adjoint_eval on m distinct contexts (independent snapshots), run
+ * concurrently on `threads` host threads (<= 0: one per context, at most 16),
+ * each context on its own stream.  Any of the array arguments may be NULL, as
+ * may any entry.  Returns the first non-zero status in context order. */
+int simox_adjoint_eval_many(simox_ctx* const* ctxs, int m, const double* const* f_target,
+                            simox_adjoint_report* reps, double* const* forces,
+                            double* const* grad_E, double* const* grad_L, int threads);
 
 /* ---- launch-shape tuning -------------------------------------------------
  * No counterpart in the reference (a GPU launch choice).  Results do not

@@ -131,7 +131,7 @@ EXPORTED = [
     "simox_set_tuning", "simox_get_tuning",
     "simox_batch_create", "simox_batch_destroy", "simox_batch_md_run", "simox_batch_autotune",
     "simox_batch_launch_count",
-    "simox_set_eam_spline", "simox_set_ctip_params", "simox_adjoint_eval",
+    "simox_set_eam_spline", "simox_set_ctip_params", "simox_adjoint_eval", "simox_adjoint_eval_many",
 ]
 
 

@@ -87,6 +87,8 @@ def lib():
         "simox_set_eam_spline": [_vp, C.POINTER(EamSpline)],
         "simox_set_ctip_params": [_vp, C.c_int, C.c_double, C.c_double, C.c_double],
         "simox_adjoint_eval": [_vp, _dp, C.POINTER(AdjointReport), _dp, _dp, _dp],
+        "simox_adjoint_eval_many": [C.POINTER(_vp), C.c_int, C.POINTER(_dp), C.POINTER(AdjointReport),
+                                    C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp), C.c_int],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -396,6 +398,25 @@ def md_opts(dt: float, thermostat: bool = False, T_given: float = 0.0, freq_new:
     o.accumulate_rdf = 0
     o.freq_stat = int(freq_stat)
     return o
+
+
+def adjoint_eval_many(ctxs, targets=None, threads: int = 0, gradients: bool = True):
+    """Simox.adjoint_eval on several contexts at once (simox_adjoint_eval_many:
+    one host thread per context, up to 16, each on its own stream).  Returns
+    a list of (report, forces, grad_E, grad_L) in context order."""
+    m = len(ctxs)
+    if targets is not None and len(targets) != m:
+        raise ValueError("one target array per context")
+    reps = (AdjointReport * max(m, 1))()
+    f = [np.zeros((g.n, 3)) for g in ctxs]
+    gE = [np.zeros(NGRAD) if gradients else None for _ in ctxs]
+    gL = [np.zeros(NGRAD) if (gradients and targets is not None) else None for _ in ctxs]
+    t = [_f64(targets[i], (ctxs[i].n, 3)) for i in range(m)] if targets is not None else [None] * m
+    arr = lambda xs: (_dp * max(m, 1))(*[_d(x) for x in xs])
+    cs = (_vp * max(m, 1))(*[g._ctx for g in ctxs])
+    _check(lib().simox_adjoint_eval_many(cs, int(m), arr(t), reps, arr(f), arr(gE), arr(gL), int(threads)),
+           "adjoint_eval_many")
+    return [(reps[i].as_dict(), f[i], gE[i], gL[i]) for i in range(m)]
 
 
 class Batch:

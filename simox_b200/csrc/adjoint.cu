@@ -19,8 +19,10 @@
 #include "simox_internal.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 namespace sx {
@@ -336,6 +338,57 @@ __global__ void adj_dir(int n, const double* __restrict__ s, const double* __res
     if (i < n) p[i] = r[i] + (s[1] / s[0]) * p[i];
 }
 
+// Scalars of the device-side projected CG (one block of CG_SLOTS doubles).
+enum CgSlot {
+    CG_MEAN = 0,    // sum for the projection onto zero mean
+    CG_RN = 1,      // r.r after the update
+    CG_PHP = 2,     // p.Hp
+    CG_RR = 3,      // r.r of the current iterate
+    CG_ALPHA = 4,   // step length
+    CG_THR = 5,     // stop when r.r <= CG_THR (rtol^2 r0.r0)
+    CG_K = 6,       // completed iterations
+    CG_STOP = 7,    // 0 running, 1 converged, 2 p.Hp <= 0 (iterate kept), 3 non-finite residual
+    CG_CHUNK = 8,   // iterations of the current graph launch
+    CG_BOLD = 10,   // (old, new) r.r for adj_dir
+    CG_BNEW = 11,
+    CG_SLOTS = 16
+};
+
+__global__ void cg_alpha_kernel(double* __restrict__ d) {
+    const double php = d[CG_PHP];
+    if (php > 0.0) {
+        d[CG_ALPHA] = d[CG_RR] / php;
+    } else {   // not positive definite along p: no update, stop
+        d[CG_ALPHA] = 0.0;
+        d[CG_STOP] = 2.0;
+    }
+}
+
+// End of one iteration: count it, test convergence, hand beta's terms to
+// adj_dir and set the WHILE condition (at most `chunk` iterations per launch).
+__global__ void cg_cond_kernel(cudaGraphConditionalHandle h, double* __restrict__ d, int maxit, int chunk) {
+    bool stop = d[CG_STOP] != 0.0;
+    if (!stop) {
+        const double k = d[CG_K] + 1.0, rn = d[CG_RN];
+        d[CG_K] = k;
+        d[CG_BOLD] = d[CG_RR];
+        d[CG_BNEW] = rn;
+        d[CG_RR] = rn;
+        if (!isfinite(rn)) {
+            d[CG_STOP] = 3.0;
+            stop = true;
+        } else if (rn <= d[CG_THR]) {
+            d[CG_STOP] = 1.0;
+            stop = true;
+        } else if (k >= (double)maxit) {
+            stop = true;
+        }
+    }
+    const double kc = d[CG_CHUNK] + 1.0;
+    d[CG_CHUNK] = kc;
+    cudaGraphSetConditional(h, (stop || kc >= (double)chunk) ? 0u : 1u);
+}
+
 // loss weights: w = 2 (F - T) in sorted order, loss, mean of w
 __global__ void adj_weights(int n, const int* __restrict__ sorted, const double* __restrict__ f,
                             const double* __restrict__ T, double* __restrict__ w, double* __restrict__ acc) {
@@ -542,6 +595,7 @@ struct AdjointState {
     double *d2F = nullptr, *w = nullptr, *wt = nullptr, *gam = nullptr, *u = nullptr, *lam = nullptr;
     double *r = nullptr, *p = nullptr, *Hp = nullptr, *sr = nullptr, *cc = nullptr, *G = nullptr, *tgt = nullptr;
     double *scal = nullptr, *gE = nullptr, *gL = nullptr;
+    double* cg = nullptr;   // scalars of the device-side CG loop (CG_* slots)
     int cap = 0;
 };
 
@@ -549,7 +603,7 @@ void adjoint_free(simox_ctx* c) {
     AdjointState* A = c->adj;
     if (!A) return;
     void* b[] = {A->spl, A->d2F, A->w, A->wt, A->gam, A->u, A->lam, A->r, A->p, A->Hp, A->sr, A->cc, A->G, A->tgt,
-                 A->scal, A->gE, A->gL};
+                 A->scal, A->gE, A->gL, A->cg};
     for (void* x : b)
         if (x) cudaFree(x);
     delete A;
@@ -569,6 +623,7 @@ static int adjoint_alloc(simox_ctx* c) {
          cudaMalloc(&A->wt, sizeof(double) * 3 * N) == cudaSuccess &&
          cudaMalloc(&A->tgt, sizeof(double) * 3 * N) == cudaSuccess &&
          cudaMalloc(&A->scal, sizeof(double) * 8) == cudaSuccess &&
+         cudaMalloc(&A->cg, sizeof(double) * CG_SLOTS) == cudaSuccess &&
          cudaMalloc(&A->gE, sizeof(double) * SIMOX_NGRAD) == cudaSuccess &&
          cudaMalloc(&A->gL, sizeof(double) * SIMOX_NGRAD) == cudaSuccess;
     if (!ok) {
@@ -616,19 +671,113 @@ static double host_scalar(simox_ctx* c, const double* d, int k = 0) {
     return h[k];
 }
 
+// y -= mean(y), the sum reduced into *sum
+static void project(simox_ctx* c, double* y, double* sum) {
+    const int n = c->n, nb = (n + 255) / 256;
+    cudaMemsetAsync(sum, 0, sizeof(double), c->stream);
+    adj_dot<<<nb, 256, 0, c->stream>>>(n, y, nullptr, sum);
+    adj_sub_mean<<<nb, 256, 0, c->stream>>>(n, sum, y);
+}
+
+// Iterations per graph launch of the device-side CG loop: every launch ends
+// after a bounded time and the host checks the status between launches.
+constexpr int kCgIterChunk = 256;
+
+// Projected CG iterations on the device.  One iteration (H p, projection,
+// p.Hp, step, residual, direction) is the body of a CUDA graph WHILE node;
+// cg_alpha_kernel and cg_cond_kernel take the decisions the host loop takes.
+// Expects b = r (projected), p = r, x = 0 and r0 = r.r.  *used = false (nothing
+// run) when the graph cannot be built here.
+static int proj_cg_device(simox_ctx* c, const CtipSpecies& S, double c_pme, double* b, double* x, double r0,
+                          double rtol, int maxit, int* k_out, double* rr_out, bool* used) {
+    *used = false;
+    if (c->profiling) return SIMOX_OK;
+    AdjointState* A = c->adj;
+    const int n = c->n, nb = (n + 255) / 256;
+    const cudaStream_t s = c->stream;
+    double* d = A->cg;
+    cudaGraph_t outer = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    if (cudaGraphCreate(&outer, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return SIMOX_OK;
+    }
+    cudaGraphConditionalHandle h;
+    cudaGraphNodeParams np{};
+    cudaGraphNode_t node;
+    bool ok = cudaGraphConditionalHandleCreate(&h, outer, 1u, cudaGraphCondAssignDefault) == cudaSuccess;
+    if (ok) {
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        ok = cudaGraphAddNode(&node, outer, nullptr, 0, &np) == cudaSuccess;
+    }
+    long long per_iter = 0;
+    int st = SIMOX_OK;
+    if (ok) {
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        ok = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+             cudaSuccess;
+        if (ok) {
+            const long long l0 = c->launches;
+            st = hess(c, S, c_pme, A->p, A->Hp);
+            project(c, A->Hp, d + CG_MEAN);
+            cudaMemsetAsync(d + CG_PHP, 0, sizeof(double), s);
+            adj_dot<<<nb, 256, 0, s>>>(n, A->p, A->Hp, d + CG_PHP);
+            cg_alpha_kernel<<<1, 1, 0, s>>>(d);
+            adj_axpy<<<nb, 256, 0, s>>>(n, d, CG_ALPHA, 1.0, A->p, x);
+            adj_axpy<<<nb, 256, 0, s>>>(n, d, CG_ALPHA, -1.0, A->Hp, b);
+            cudaMemsetAsync(d + CG_RN, 0, sizeof(double), s);
+            adj_dot<<<nb, 256, 0, s>>>(n, b, b, d + CG_RN);
+            cg_cond_kernel<<<1, 1, 0, s>>>(h, d, maxit, kCgIterChunk);
+            adj_dir<<<nb, 256, 0, s>>>(n, d + CG_BOLD, b, A->p);
+            cudaGraph_t cap = nullptr;
+            ok = cudaStreamEndCapture(s, &cap) == cudaSuccess && st == SIMOX_OK;
+            per_iter = c->launches - l0 + 9;   // + the nine vector and scalar kernels above
+            c->launches = l0;
+        }
+        ok = ok && cudaGraphInstantiate(&exec, outer, 0) == cudaSuccess;
+    }
+    cudaGetLastError();
+    if (!ok) {
+        if (exec) cudaGraphExecDestroy(exec);
+        cudaGraphDestroy(outer);
+        return st;
+    }
+    *used = true;
+    double hd[CG_SLOTS] = {};
+    hd[CG_RR] = r0;
+    hd[CG_THR] = rtol * rtol * r0;
+    cudaMemcpyAsync(d, hd, sizeof(hd), cudaMemcpyHostToDevice, s);
+    int k = 0;
+    while (true) {
+        cudaMemsetAsync(d + CG_CHUNK, 0, sizeof(double), s);
+        if ((st = cuda_status(cudaGraphLaunch(exec, s)))) break;
+        cudaMemcpyAsync(hd, d, sizeof(hd), cudaMemcpyDeviceToHost, s);
+        if ((st = cuda_status(cudaStreamSynchronize(s)))) break;
+        const int k_now = (int)hd[CG_K];
+        c->launches += per_iter * (long long)(k_now - k);
+        k = k_now;
+        if (hd[CG_STOP] != 0.0 || k >= maxit) break;
+    }
+    *k_out = k;
+    *rr_out = hd[CG_RR];
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(outer);
+    return st;
+}
+
 // projected CG: (P H P) x = P b, x orthogonal to the all-ones vector.
-// x must start at zero; b is overwritten (it becomes the residual).
+// x must start at zero; b is overwritten (it becomes the residual).  The
+// iterations run as a device-side graph loop, or host-driven when the graph
+// cannot be built (and with the per-launch profile on).
 static int proj_cg(simox_ctx* c, const CtipSpecies& S, double c_pme, double* b, double* x, double rtol, int maxit,
                    int* iters, double* relres, double abs_tol = 0.0, double* norm0 = nullptr) {
     AdjointState* A = c->adj;
     const int n = c->n, nb = (n + 255) / 256;
     double* s = A->scal;
-    auto project = [&](double* y) {
-        cudaMemsetAsync(s, 0, sizeof(double), c->stream);
-        adj_dot<<<nb, 256, 0, c->stream>>>(n, y, nullptr, s);
-        adj_sub_mean<<<nb, 256, 0, c->stream>>>(n, s, y);
-    };
-    project(b);   // r = P b (x = 0)
+    project(c, b, s);   // r = P b (x = 0)
     cudaMemcpyAsync(A->p, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream);
     cudaMemsetAsync(s, 0, sizeof(double) * 8, c->stream);
     adj_dot<<<nb, 256, 0, c->stream>>>(n, b, b, s);            // s[0] = r.r
@@ -636,11 +785,16 @@ static int proj_cg(simox_ctx* c, const CtipSpecies& S, double c_pme, double* b, 
     if (norm0) *norm0 = std::sqrt(r0);
     double rr = r0;
     int k = 0;
-    if (r0 > abs_tol * abs_tol) {
+    bool device_loop = false;
+    if (r0 > abs_tol * abs_tol && maxit > 0) {
+        int st = proj_cg_device(c, S, c_pme, b, x, r0, rtol, maxit, &k, &rr, &device_loop);
+        if (st) return st;
+    }
+    if (r0 > abs_tol * abs_tol && !device_loop) {
         for (k = 0; k < maxit; k++) {
             int st = hess(c, S, c_pme, A->p, A->Hp);
             if (st) return st;
-            project(A->Hp);
+            project(c, A->Hp, s);
             // s[2] = p.Hp ; alpha = rr / pHp
             cudaMemsetAsync(s + 2, 0, sizeof(double), c->stream);
             adj_dot<<<nb, 256, 0, c->stream>>>(n, A->p, A->Hp, s + 2);
@@ -877,4 +1031,37 @@ extern "C" int simox_adjoint_eval(simox_ctx* c, const double* f_target, simox_ad
     if (!c) return SIMOX_E_ARG;
     cudaSetDevice(c->device);
     return sx::adjoint_eval(c, f_target, rep, forces, grad_E, grad_L);
+}
+
+extern "C" int simox_adjoint_eval_many(simox_ctx* const* ctxs, int m, const double* const* f_target,
+                                       simox_adjoint_report* reps, double* const* forces, double* const* grad_E,
+                                       double* const* grad_L, int threads) {
+    if (m < 0 || (m > 0 && !ctxs)) return SIMOX_E_ARG;
+    for (int i = 0; i < m; i++) {
+        if (!ctxs[i]) return SIMOX_E_ARG;
+        for (int j = 0; j < i; j++)
+            if (ctxs[j] == ctxs[i]) return SIMOX_E_ARG;   // one host thread per context at a time
+    }
+    if (m == 0) return SIMOX_OK;
+    int nt = threads > 0 ? threads : std::min(m, 16);
+    nt = std::max(1, std::min(nt, m));
+    std::vector<int> st(m, SIMOX_OK);
+    std::atomic<int> next{0};
+    auto work = [&]() {
+        for (int i = next++; i < m; i = next++) {
+            simox_ctx* c = ctxs[i];
+            cudaSetDevice(c->device);
+            st[i] = sx::adjoint_eval(c, f_target ? f_target[i] : nullptr, reps ? reps + i : nullptr,
+                                     forces ? forces[i] : nullptr, grad_E ? grad_E[i] : nullptr,
+                                     grad_L ? grad_L[i] : nullptr);
+        }
+    };
+    std::vector<std::thread> pool;
+    pool.reserve(nt - 1);
+    for (int t = 1; t < nt; t++) pool.emplace_back(work);
+    work();
+    for (std::thread& t : pool) t.join();
+    for (int i = 0; i < m; i++)
+        if (st[i]) return st[i];
+    return SIMOX_OK;
 }

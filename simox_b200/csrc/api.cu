@@ -95,6 +95,28 @@ void prof_collect(simox_ctx* c) {
 // ---------------------------------------------------------------------------
 // device-resident main loop (main.f90:40-84 with TAG_SET main.f90:376-414)
 
+// PME forces into f_rec on c->side, forked from c->stream; ev_join marks
+// their end.  With the per-launch profile on, PME stays on c->stream so that
+// each launch's event span holds that launch alone, not the time it shared
+// the SMs with the concurrent pair passes.
+static int pme_fork(simox_ctx* c, bool estep) {
+    if (c->profiling) {
+        const int st = pme_forces(c, false, estep, c->f_rec);
+        cudaEventRecord(c->ev_join, c->stream);
+        return st;
+    }
+    cudaEventRecord(c->ev_fork, c->stream);
+    cudaStreamWaitEvent(c->side, c->ev_fork, 0);
+    std::swap(c->stream, c->side);
+    pme_bind_stream(c);
+    const int st = pme_forces(c, false, estep, c->f_rec);
+    std::swap(c->stream, c->side);
+    pme_bind_stream(c);
+    if (st) return st;
+    cudaEventRecord(c->ev_join, c->side);
+    return SIMOX_OK;
+}
+
 // One step without CTIP: VV_NVE1, CELL_SORT, FORCE (+ PME on the side
 // stream), VV_NVE2 / VV_NVT2_BEREND.  Every launch goes to c->stream or, for
 // PME, to c->side forked from and joined back to it, so the whole step can be
@@ -108,15 +130,7 @@ int md_step(simox_ctx* c, const simox_md_opts* o, bool sort, bool estep, bool wa
     // pair passes run; its forces land in f_rec and the second half kick
     // adds them: f = f_pair + f_rec - Fsum/N, as FORCE + PME would leave f.
     if ((st = ensure_gathered(c))) return st;
-    cudaEventRecord(c->ev_fork, c->stream);
-    cudaStreamWaitEvent(c->side, c->ev_fork, 0);
-    std::swap(c->stream, c->side);
-    pme_bind_stream(c);
-    st = pme_forces(c, false, estep, c->f_rec);
-    std::swap(c->stream, c->side);
-    pme_bind_stream(c);
-    if (st) return st;
-    cudaEventRecord(c->ev_join, c->side);
+    if ((st = pme_fork(c, estep))) return st;
     if ((st = ensure_list(c))) return st;
     if ((st = eam_density(c, estep))) return st;
     if ((st = pair_forces(c, estep, want_rdf))) return st;
@@ -198,15 +212,7 @@ int md_run(simox_ctx* c, const simox_md_opts* o, int first, int nsteps, simox_en
             simox_md_opts o2 = *o;
             // the rest of the step: FORCE, PME, VV2 (VV1 and CELL_SORT done)
             if ((st = ensure_gathered(c))) return st;
-            cudaEventRecord(c->ev_fork, c->stream);
-            cudaStreamWaitEvent(c->side, c->ev_fork, 0);
-            std::swap(c->stream, c->side);
-            pme_bind_stream(c);
-            st = pme_forces(c, false, estep, c->f_rec);
-            std::swap(c->stream, c->side);
-            pme_bind_stream(c);
-            if (st) return st;
-            cudaEventRecord(c->ev_join, c->side);
+            if ((st = pme_fork(c, estep))) return st;
             if ((st = ensure_list(c))) return st;
             if ((st = eam_density(c, estep))) return st;
             if ((st = pair_forces(c, estep, want_rdf))) return st;
@@ -518,17 +524,19 @@ extern "C" int simox_set_state(simox_ctx* c, int n, const int* id, const double*
         c->skin_valid = false;
         drop_graphs(c);
     }
-    if (x) {
-        bool inb = true;
-        for (int i = 0; i < 3 * n && inb; i++) inb = std::fabs(x[i]) <= c->hbox[i % 3];
-        c->in_box = inb;
-        c->cells_fresh = false;
-    }
     c->n = n;
     if (x) cudaMemcpyAsync(c->x, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s);
     if (v) cudaMemcpyAsync(c->v, v, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s);
     if (f) cudaMemcpyAsync(c->f, f, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s);
     if (q) cudaMemcpyAsync(c->q, q, sizeof(double) * n, cudaMemcpyHostToDevice, s);
+    if (x) {   // while the copies run: are all positions inside the box (no wrap needed)?
+        const double hx = c->hbox[0], hy = c->hbox[1], hz = c->hbox[2];
+        bool inb = true;
+        for (int i = 0; i < n && inb; i++)
+            inb = std::fabs(x[3 * i]) <= hx && std::fabs(x[3 * i + 1]) <= hy && std::fabs(x[3 * i + 2]) <= hz;
+        c->in_box = inb;
+        c->cells_fresh = false;
+    }
     if (x || q || id) { c->gathered = false; c->list_valid = false; c->eam_valid = false; }
     return cuda_status(cudaStreamSynchronize(s));
 }

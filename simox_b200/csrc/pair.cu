@@ -18,6 +18,7 @@
 #include "simox_packed.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <type_traits>
@@ -1376,8 +1377,8 @@ static constexpr size_t kTileSmem = (size_t)kTileCap * (sizeof(float4) + sizeof(
 
 // dynamic shared memory of the tiled force pass, once per device
 static int tile_prepare(int device) {
-    static bool done[64] = {};
-    if (device >= 0 && device < 64 && done[device]) return SIMOX_OK;
+    static std::atomic<bool> done[64] = {};   // contexts may run on several host threads
+    if (device >= 0 && device < 64 && done[device].load()) return SIMOX_OK;
     const int b = (int)kTileSmem;
     cudaError_t e1 = cudaFuncSetAttribute(force_tile_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     cudaError_t e2 = cudaFuncSetAttribute(force_tile_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);

@@ -19,6 +19,7 @@
 // as force.f90:406 / ctip.f90:359 do with a default-kind CMPLX().
 #include "simox_internal.cuh"
 
+#include <atomic>
 #include <cmath>
 #include <type_traits>
 #include <vector>
@@ -529,12 +530,12 @@ int pme_self(simox_ctx* c) {
 
 template <int P>
 static bool spread_tile_ready(int device) {
-    static bool done[64] = {};
+    static std::atomic<bool> done[64] = {};   // contexts may run on several host threads
     if (device < 0 || device >= 64) return false;
-    if (!done[device])
+    if (!done[device].load())
         done[device] = cudaFuncSetAttribute(spread_tile_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)(SP_PATCH * sizeof(float))) == cudaSuccess;
-    return done[device];
+    return done[device].load();
 }
 
 template <typename R, int P>

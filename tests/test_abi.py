@@ -59,3 +59,17 @@ def test_create_without_gpu_reports_status(simox_lib):
     else:
         assert st == 0
         simox_lib.simox_destroy(ctx)
+
+
+def test_adjoint_eval_many_argument_checks(simox_lib):
+    """Host-side checks of simox_adjoint_eval_many (no context is touched):
+    nothing to do for m = 0, E_ARG for a NULL or repeated context."""
+    import ctypes as C
+    from simox_b200.api import _vp
+    assert simox_lib.simox_adjoint_eval_many(None, 0, None, None, None, None, None, 0) == 0
+    assert simox_lib.simox_adjoint_eval_many(None, 2, None, None, None, None, None, 0) == _abi.SIMOX_E_ARG
+    fake = _vp(0x1000)   # never dereferenced: the duplicate check runs first
+    arr = (_vp * 2)(fake, fake)
+    assert simox_lib.simox_adjoint_eval_many(arr, 2, None, None, None, None, None, 0) == _abi.SIMOX_E_ARG
+    arr = (_vp * 2)(fake, None)
+    assert simox_lib.simox_adjoint_eval_many(arr, 2, None, None, None, None, None, 0) == _abi.SIMOX_E_ARG

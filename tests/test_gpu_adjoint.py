@@ -116,3 +116,35 @@ def test_energy_and_loss_gradients_match_finite_differences():
             assert abs(dE - gE[j]) <= 1e-4 * abs(gE[j]) + 1e-6 * np.abs(gE).max(), (k, dE, gE[j])
             assert abs(dL - gL[j]) <= 1e-3 * abs(gL[j]) + 1e-6 * np.abs(gL).max(), (k, dL, gL[j])
         _params(g, P, spl, th0)
+
+
+def test_adjoint_eval_many_matches_one_by_one():
+    """Three snapshots through simox_adjoint_eval_many (host threads, a stream
+    each) against the same snapshots one after another: equal losses and
+    gradients up to the order of the FP64 atomic sums (1e-9 relative)."""
+    P = api.default_potential()
+    spl = spline.fit(P)
+    rng = np.random.default_rng(9)
+    systems = [S.replica(40 + k, 480, 0.2 + 0.1 * k, 500.0 + 100 * k) for k in range(3)]
+    ctxs = [_ctx(s) for s in systems]
+    try:
+        targets = []
+        for g in ctxs:
+            g.set_eam_spline(spl)
+            _, f0, _, _ = g.adjoint_eval(gradients=False)
+            targets.append(f0 + rng.normal(0.0, 0.05, f0.shape))
+        q0 = [g.get_state()["q"] for g in ctxs]
+        one = [g.adjoint_eval(t) for g, t in zip(ctxs, targets)]
+        for g, q in zip(ctxs, q0):
+            g.set_state(q=q)
+        many = api.adjoint_eval_many(ctxs, targets)
+        for (r1, f1, e1, l1), (r2, f2, e2, l2) in zip(one, many):
+            assert abs(r1["loss"] - r2["loss"]) <= 1e-9 * abs(r1["loss"])
+            assert abs(r1["E"] - r2["E"]) <= 1e-9 * abs(r1["E"])
+            assert np.linalg.norm(f1 - f2) <= 1e-9 * np.linalg.norm(f1)
+            assert np.linalg.norm(e1 - e2) <= 1e-9 * np.linalg.norm(e1)
+            assert np.linalg.norm(l1 - l2) <= 1e-9 * np.linalg.norm(l1)
+            assert r2["adj_residual"] <= 1e-10
+    finally:
+        for g in ctxs:
+            g.close()
