@@ -148,3 +148,69 @@ def test_adjoint_eval_many_matches_one_by_one():
     finally:
         for g in ctxs:
             g.close()
+
+
+def test_adjoint_as_autograd_function():
+    """The adjoint wrapped as a torch.autograd.Function of the 207 parameters
+    (test harness only; the library exposes it through the C ABI):
+    backward() of loss + 0.5 E returns grad_L + 0.5 grad_E, and a central
+    difference through the wrapper (step 1e-4) agrees with grad_L on the
+    largest spline component within 1e-3."""
+    import torch
+    s = _system()
+    P = api.default_potential()
+    spl = spline.fit(P)
+    th0 = _theta0(P, spl)
+    rng = np.random.default_rng(3)
+    with _ctx(s) as g:
+        _params(g, P, spl, th0)
+        _, f0, _, _ = g.adjoint_eval(gradients=False)
+        target = f0 + rng.normal(0.0, 0.05, f0.shape)
+        # theta in the NGRAD layout (chi, J, Z of all five species)
+        th = np.zeros(_abi.NGRAD)
+        th[:3 * NS] = th0[:3 * NS]
+        for sp in range(1, 6):
+            p = P.param[sp - 1]
+            th[3 * NS + 3 * (sp - 1): 3 * NS + 3 * sp] = [p.chi, p.J, p.Z]
+
+        def set_all(theta):
+            g.set_eam_spline(spline.with_coefficients(spl, theta[:3 * NS]))
+            for sp in range(1, 6):
+                chi, J, Z = theta[3 * NS + 3 * (sp - 1): 3 * NS + 3 * sp]
+                g.set_ctip_params(sp, chi, J, Z)
+
+        saved = {}
+
+        class Fn(torch.autograd.Function):
+            @staticmethod
+            def forward(ctx, theta):
+                set_all(theta.detach().numpy())
+                rep, _, gE, gL = g.adjoint_eval(target)
+                saved["gE"], saved["gL"] = gE, gL
+                ctx.save_for_backward(torch.from_numpy(gE), torch.from_numpy(gL))
+                return theta.new_tensor([rep["loss"], rep["E"]])
+
+            @staticmethod
+            def backward(ctx, grad_out):
+                gE, gL = ctx.saved_tensors
+                return grad_out[0] * gL + grad_out[1] * gE
+
+        theta = torch.tensor(th, dtype=torch.float64, requires_grad=True)
+        out = Fn.apply(theta)
+        (out[0] + 0.5 * out[1]).backward()
+        gE, gL = saved["gE"], saved["gL"]
+        ref = gL + 0.5 * gE
+        assert np.linalg.norm(theta.grad.numpy() - ref) <= 1e-12 * np.linalg.norm(ref)
+        # one component by central differences through the wrapper
+        k = int(np.argmax(np.abs(gL[:3 * NS])))
+        q0 = g.get_state()["q"]
+        vals = []
+        for sgn in (1.0, -1.0):
+            t = th.copy()
+            t[k] += sgn * 1e-4
+            g.set_state(q=q0)
+            with torch.no_grad():
+                vals.append(float(Fn.apply(torch.tensor(t))[0]))
+        d = (vals[0] - vals[1]) / 2e-4
+        assert abs(d - gL[k]) <= 1e-3 * abs(gL[k]) + 1e-6 * np.abs(gL).max(), (d, gL[k])
+        set_all(th)
