@@ -78,48 +78,30 @@ int build_cell_tables(simox_ctx* c) {
 
 // ---------------------------------------------------------------------------
 // CELL_SORT kernels
-
-// Counter increment shared by the lanes of a warp with the same key (key < 0:
-// the lane takes no part): one atomic per distinct key instead of one per
-// lane, the lanes' slots numbered in lane order.  Atoms of consecutive indices
-// mostly fall into the same few cells, so this cuts the atomics on the cell
-// counters several-fold.  All 32 lanes must call it.
-__device__ __forceinline__ int warp_agg_add(int* __restrict__ counter, int key) {
-    const int lane = threadIdx.x & 31;
-    const unsigned peers = __match_any_sync(0xffffffffu, key);
-    const int leader = __ffs(peers) - 1;
-    int first = 0;
-    if (lane == leader && key >= 0) first = atomicAdd(counter + key, __popc(peers));
-    first = __shfl_sync(0xffffffffu, first, leader);
-    return first + __popc(peers & ((1u << lane) - 1u));
-}
-
 __global__ void bin_atoms_kernel(int n, const double* __restrict__ x, double3 hbox, double3 lc, int3 nc,
                                  int* __restrict__ cell_of, int* __restrict__ cell_xyz, int* __restrict__ count,
                                  int* __restrict__ status) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int cell = -1;
-    if (i < n) {
-        int id[3];
-        const double hb[3] = {hbox.x, hbox.y, hbox.z};
-        const double l[3] = {lc.x, lc.y, lc.z};
-        const int m[3] = {nc.x, nc.y, nc.z};
-        bool bad = false;
-        for (int d = 0; d < 3; d++) {
-            double xx = __dadd_rn(x[3 * i + d], hb[d]);     // xx = x + hbox   cellsort.f90:69
-            double t = __ddiv_rn(xx, l[d]);                 // xx/Lcell        cellsort.f90:70
-            if (!(fabs(t) < 1.0e9)) { bad = true; id[d] = 0; continue; }
-            int v = __double2int_rz(t);                     // INT(): toward zero
-            v = (v + m[d]) % m[d];                          // MOD(id+Ncell, Ncell) cellsort.f90:71
-            if (v < 0) { bad = true; v = 0; }
-            id[d] = v;
-        }
-        if (bad) atomicOr(status, ST_POSITION);
-        cell = id[0] + id[1] * m[0] + id[2] * m[0] * m[1];
-        cell_of[i] = cell;
-        cell_xyz[i] = id[0] | (id[1] << 10) | (id[2] << 20);   // Ncell <= 1024 per axis (checked at set-up)
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int id[3];
+    const double hb[3] = {hbox.x, hbox.y, hbox.z};
+    const double l[3] = {lc.x, lc.y, lc.z};
+    const int m[3] = {nc.x, nc.y, nc.z};
+    bool bad = false;
+    for (int d = 0; d < 3; d++) {
+        double xx = __dadd_rn(x[3 * i + d], hb[d]);     // xx = x + hbox   cellsort.f90:69
+        double t = __ddiv_rn(xx, l[d]);                 // xx/Lcell        cellsort.f90:70
+        if (!(fabs(t) < 1.0e9)) { bad = true; id[d] = 0; continue; }
+        int v = __double2int_rz(t);                     // INT(): toward zero
+        v = (v + m[d]) % m[d];                          // MOD(id+Ncell, Ncell) cellsort.f90:71
+        if (v < 0) { bad = true; v = 0; }
+        id[d] = v;
     }
-    warp_agg_add(count, cell);
+    if (bad) atomicOr(status, ST_POSITION);
+    int cell = id[0] + id[1] * m[0] + id[2] * m[0] * m[1];
+    cell_of[i] = cell;
+    cell_xyz[i] = id[0] | (id[1] << 10) | (id[2] << 20);   // Ncell <= 1024 per axis (checked at set-up)
+    atomicAdd(count + cell, 1);
 }
 
 // cond: nullptr, or a device flag that must be non-zero for the kernel to run
@@ -155,9 +137,10 @@ __global__ void scan_cells_kernel(const int* __restrict__ count, int* __restrict
 __global__ void scatter_atoms_kernel(int n, const int* __restrict__ cell_of, int* __restrict__ fill,
                                      int* __restrict__ sorted, const int* __restrict__ cond) {
     if (cond && *cond == 0) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int slot = warp_agg_add(fill, i < n ? cell_of[i] : -1);   // order inside a cell: set by the rank sort
-    if (i < n) sorted[slot] = i;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int slot = atomicAdd(fill + cell_of[i], 1);
+    sorted[slot] = i;
 }
 
 // Rank sort inside each cell: ascending original index (= CELL_SORT order).
@@ -510,23 +493,21 @@ __global__ void skin_bin_kernel(int n, const double* __restrict__ x, double3 hbo
                                 const int* __restrict__ cond) {
     if (*cond == 0) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int c = -1;
-    if (i < n) {
-        const double xx[3] = {x[3 * i], x[3 * i + 1], x[3 * i + 2]};
-        const double h[3] = {hbox.x, hbox.y, hbox.z}, il[3] = {ilc.x, ilc.y, ilc.z};
-        const int m[3] = {nc.x, nc.y, nc.z};
-        int id[3];
+    if (i >= n) return;
+    const double xx[3] = {x[3 * i], x[3 * i + 1], x[3 * i + 2]};
+    const double h[3] = {hbox.x, hbox.y, hbox.z}, il[3] = {ilc.x, ilc.y, ilc.z};
+    const int m[3] = {nc.x, nc.y, nc.z};
+    int id[3];
 #pragma unroll
-        for (int d = 0; d < 3; d++) {
-            int v = (int)floor((xx[d] + h[d]) * il[d]);
-            v = v < 0 ? 0 : (v >= m[d] ? m[d] - 1 : v);
-            id[d] = v;
-            x0[3 * i + d] = xx[d];
-        }
-        c = id[0] + id[1] * m[0] + id[2] * m[0] * m[1];
-        cell_of[i] = c;
+    for (int d = 0; d < 3; d++) {
+        int v = (int)floor((xx[d] + h[d]) * il[d]);
+        v = v < 0 ? 0 : (v >= m[d] ? m[d] - 1 : v);
+        id[d] = v;
+        x0[3 * i + d] = xx[d];
     }
-    warp_agg_add(count, c);
+    const int c = id[0] + id[1] * m[0] + id[2] * m[0] * m[1];
+    cell_of[i] = c;
+    atomicAdd(count + c, 1);
 }
 
 // Choose the pair-kernel order for the current state and gather into it.  In
