@@ -443,7 +443,7 @@ def run_adjoint(args):
     line = {"metric": "parameter-gradient snapshots/s (2000-atom Al/O, FP64 adjoint)", "value": len(ctxs) / el,
             "unit": "snapshots/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"{len(ctxs)} seeded snapshots of 2000 atoms, targets = model forces + N(0, 0.05)",
-                       "parameters": "3 x 64 spline coefficients + chi, J, Z of 5 species (207)",
+                       "parameters": "3 x 64 spline coefficients + chi, J, Z, xi of 5 species (212)",
                        "api": "simox_adjoint_eval_many (all snapshots concurrently, one host thread and "
                               "stream per snapshot, up to 16 threads)"},
             "ms_per_snapshot": el / len(ctxs) * 1e3,

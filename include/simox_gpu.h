@@ -250,10 +250,11 @@ int simox_neighbor_stats(simox_ctx* ctx, int* max_nnb, long long* total_nnb);
  * Newton steps on the fixed active set to FP64 precision).  Its forces are
  * FORCE + PME at q* (as-written formulas).  All of it is FP64.
  * Gradient layout (SIMOX_NGRAD doubles): phi[64], dens[64], emb[64], then for
- * species 1..5: d/dchi, d/dJ, d/dZ.  Gradients with respect to xi (zeta) are
- * not provided: the Slater coefficient table fafb depends on xi. */
+ * species 1..5: d/dchi, d/dJ, d/dZ, then d/dxi (zeta) of species 1..5.  The
+ * xi derivatives take the Slater coefficients fafb as the functions of xi
+ * that datafmt.f90:201-220 defines (as simox_set_ctip_xi sets them). */
 #define SIMOX_SPLINE_N 64
-#define SIMOX_NGRAD (3 * SIMOX_SPLINE_N + 3 * SIMOX_NATOM)
+#define SIMOX_NGRAD (3 * SIMOX_SPLINE_N + 4 * SIMOX_NATOM)
 typedef struct {
     int    metal;            /* species id whose EAM functions are splines (1 = Al) */
     double r0, r1;           /* domain (A) of the f and phi splines; pairs beyond r1 add nothing */
@@ -274,6 +275,11 @@ typedef struct {
 int simox_set_eam_spline(simox_ctx* ctx, const simox_eam_spline* s);
 /* CTIP parameters chi, J, Z of species 1..5 (POTN datafmt.f90:54-56). */
 int simox_set_ctip_params(simox_ctx* ctx, int species, double chi, double J, double Z);
+/* Slater exponent xi (zeta) of species 1..5 (POTN datafmt.f90:57); recomputes
+ * the fafb coefficients of every pair involving it (datafmt.f90:201-220).
+ * SIMOX_E_ARG for xi <= 0 or xi equal to another species' xi (the cross
+ * coefficients divide by xi_a - xi_b). */
+int simox_set_ctip_xi(simox_ctx* ctx, int species, double xi);
 /* Charges q*, energy, forces (original order, [n][3], may be NULL) and the
  * gradients of E (grad_E) and of L = sum |F - T|^2 (grad_L; needs f_target
  * [n][3]) with respect to the parameters; either gradient may be NULL.  The

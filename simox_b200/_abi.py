@@ -131,7 +131,8 @@ EXPORTED = [
     "simox_set_tuning", "simox_get_tuning",
     "simox_batch_create", "simox_batch_destroy", "simox_batch_md_run", "simox_batch_autotune",
     "simox_batch_launch_count",
-    "simox_set_eam_spline", "simox_set_ctip_params", "simox_adjoint_eval", "simox_adjoint_eval_many",
+    "simox_set_eam_spline", "simox_set_ctip_params", "simox_set_ctip_xi", "simox_adjoint_eval",
+    "simox_adjoint_eval_many",
 ]
 
 
@@ -141,7 +142,7 @@ class Tuning(C.Structure):
 
 
 SPLINE_N = 64
-NGRAD = 3 * SPLINE_N + 3 * NATOM
+NGRAD = 3 * SPLINE_N + 4 * NATOM
 
 
 class EamSpline(C.Structure):

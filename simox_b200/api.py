@@ -86,6 +86,7 @@ def lib():
         "simox_batch_launch_count": [_vp, C.POINTER(C.c_longlong)],
         "simox_set_eam_spline": [_vp, C.POINTER(EamSpline)],
         "simox_set_ctip_params": [_vp, C.c_int, C.c_double, C.c_double, C.c_double],
+        "simox_set_ctip_xi": [_vp, C.c_int, C.c_double],
         "simox_adjoint_eval": [_vp, _dp, C.POINTER(AdjointReport), _dp, _dp, _dp],
         "simox_adjoint_eval_many": [C.POINTER(_vp), C.c_int, C.POINTER(_dp), C.POINTER(AdjointReport),
                                     C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp), C.c_int],
@@ -360,6 +361,10 @@ class Simox:
         t = _f64(f_target, (self.n, 3))
         _check(lib().simox_adjoint_eval(self._ctx, _d(t), C.byref(rep), _d(f), _d(gE), _d(gL)), "adjoint_eval")
         return rep.as_dict(), f, gE, gL
+
+    def set_ctip_xi(self, species: int, xi: float):
+        """Slater exponent xi of species 1..5 (recomputes the fafb coefficients)."""
+        _check(lib().simox_set_ctip_xi(self._ctx, int(species), float(xi)), "set_ctip_xi")
 
     def set_tuning(self, force_splits: int):
         t = Tuning()

@@ -575,6 +575,132 @@ __global__ void __launch_bounds__(AT)
     }
 }
 
+// Derivatives of one pair table entry's CTIP coefficients with respect to the
+// X exponent field xi_x ([0]) and the Y field xi_y ([1]).  For X == Y the
+// coefficients' whole dependence on the species' xi sits in [0].
+struct XiTab {
+    double dSx[2][4], dSy[2][4], dQx[2][5], dQy[2][5];
+};
+
+// pass 6: xi (zeta) gradients.  Per ordered pair (X, Y) of X's row, with
+// d = d/dxi_x (credited to X's species) and d/dxi_y (to Y's):
+//   dE += q_X Z_Y d asym_XY + 1/2 q_X q_Y d sym_XY          (U at fixed q)
+//   dL += -lambda_X (Z_Y d asym_XY + q_Y d sym_XY)           (through G)
+//       + 1/2 d fs_XY (w_X - w_Y) . d_XY                     (forces, as written)
+// asym and sym are CTIP_SOLVER's (ctip.f90:86-108), fs the CTIP part of the
+// pair force of force.f90:101-140.
+__global__ void __launch_bounds__(AT)
+    adj_xi_grad_kernel(AdjParams P, const PairTab<double>* __restrict__ tab, const XiTab* __restrict__ xit,
+                       const double4* __restrict__ xq, const int* __restrict__ ts, const int2* __restrict__ nn,
+                       const unsigned* __restrict__ nbr, const double* __restrict__ q,
+                       const double* __restrict__ lam, const double* __restrict__ w, double* __restrict__ gE,
+                       double* __restrict__ gL) {
+    __shared__ PairTab<double> st[kSpecies * kSpecies];
+    __shared__ XiTab sx[kSpecies * kSpecies];
+    __shared__ double bE[kSpecies], bL[kSpecies];
+    for (int k = threadIdx.x; k < kSpecies * kSpecies; k += blockDim.x) {
+        st[k] = tab[k];
+        sx[k] = xit[k];
+    }
+    for (int k = threadIdx.x; k < kSpecies; k += blockDim.x) bE[k] = bL[k] = 0.0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    const double kc = P.kc;
+    const bool want_L = lam != nullptr || w != nullptr;
+    for (int X = blockIdx.x * wpb + (threadIdx.x >> 5); X < P.n; X += gridDim.x * wpb) {
+        const int sX = ts[X];
+        if (sX >= kSpecies) continue;
+        const double4 xa = xq[X];
+        const int2 m = nn[X];
+        const unsigned* row = nbr + (size_t)X * P.cap;
+        const double qX = q[X], lX = lam ? lam[X] : 0.0;
+        const double wx = w ? w[3 * X] : 0.0, wy = w ? w[3 * X + 1] : 0.0, wz = w ? w[3 * X + 2] : 0.0;
+        double eX_acc = 0.0, lX_acc = 0.0;                       // d/dxi_x: species sX
+        double eY_acc[kSpecies] = {}, lY_acc[kSpecies] = {};    // d/dxi_y: species sY
+        for (int k = lane; k < m.x + m.y; k += 32) {
+            const int Y = (int)(row[slot(k, P.cap, m.x)] & kIdxMask);
+            const int sY = ts[Y];
+            if (sY >= kSpecies) continue;
+            double dx, dy, dz;
+            sep(xa, xq[Y], P, dx, dy, dz);
+            const double r = sqrt(dx * dx + dy * dy + dz * dz);
+            const double ir = 1.0 / r, ir2 = ir * ir;
+            const PairTab<double>& T = st[sX * kSpecies + sY];
+            const XiTab& D = sx[sX * kSpecies + sY];
+            const double eX = exp(-2.0 * T.xi_x * r), eY = exp(-2.0 * T.xi_y * r);
+            const double qY = q[Y], ZX = T.Z_x, ZY = T.Z_y;
+            // CTIP_SOLVER pair: fifj_s = -(eX SX + eY SY)/r, afb_X = -eX (xi_x + 1/r)
+            const double SX = T.Sx[0] + r * (T.Sx[1] + r * (T.Sx[2] + r * T.Sx[3]));
+            const double SY = T.Sy[0] + r * T.Sy[1];
+            double de[2], dl[2];
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                const double dSX = D.dSx[j][0] + r * (D.dSx[j][1] + r * (D.dSx[j][2] + r * D.dSx[j][3]));
+                const double dSY = D.dSy[j][0] + r * D.dSy[j][1];
+                const double dnum = eX * dSX + eY * dSY + (j == 0 ? -2.0 * r * eX * SX : -2.0 * r * eY * SY);
+                const double dfifj_s = -dnum * ir;
+                const double dafb = j == 0 ? eX * (2.0 * r * T.xi_x + 1.0) : 0.0;
+                const double dasym = kc * (dafb - dfifj_s), dsym = kc * dfifj_s;
+                de[j] = qX * ZY * dasym + 0.5 * qX * qY * dsym;
+                dl[j] = lam ? -lX * (ZY * dasym + qY * dsym) : 0.0;
+            }
+            if (w) {   // as-written CTIP pair force scalar (es_pair) and its xi derivatives
+                const double QX = T.Qx[0] + r * (T.Qx[1] + r * T.Qx[2]) + ir * (T.Qx[3] + ir * T.Qx[4]);
+                const double QY = T.Qy[0] + ir * (T.Qy[3] + ir * T.Qy[4]);
+                const double djfi = eX * (2.0 * T.xi_x * T.xi_x + (1.0 + 2.0 * T.xi_x * r) * ir2);
+                const double difj = eY * (2.0 * T.xi_y * T.xi_y + (1.0 + 2.0 * T.xi_y * r) * ir2);
+                const double wd = (wx - w[3 * Y]) * dx + (wy - w[3 * Y + 1]) * dy + (wz - w[3 * Y + 2]) * dz;
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    const double dQX = D.dQx[j][0] + r * (D.dQx[j][1] + r * D.dQx[j][2]) +
+                                       ir * (D.dQx[j][3] + ir * D.dQx[j][4]);
+                    const double dQY = D.dQy[j][0] + ir * (D.dQy[j][3] + ir * D.dQy[j][4]);
+                    const double ddfifj = eX * dQX + eY * dQY + (j == 0 ? -2.0 * r * eX * QX : -2.0 * r * eY * QY);
+                    const double ddjfi = j == 0 ? -2.0 * r * djfi + eX * (4.0 * T.xi_x + 2.0 * ir) : 0.0;
+                    const double ddifj = j == 1 ? -2.0 * r * difj + eY * (4.0 * T.xi_y + 2.0 * ir) : 0.0;
+                    const double dfs =
+                        kc * ((qX * ZY + qY * ZX - qX * qY) * ddfifj - qX * ZY * ddjfi - qY * ZX * ddifj) * ir;
+                    dl[j] += 0.5 * dfs * wd;
+                }
+            }
+            eX_acc += de[0];
+            lX_acc += dl[0];
+#pragma unroll
+            for (int s = 0; s < kSpecies; s++)
+                if (s == sY) {
+                    eY_acc[s] += de[1];
+                    lY_acc[s] += dl[1];
+                }
+        }
+        eX_acc = warp_sum(eX_acc);
+        lX_acc = warp_sum(lX_acc);
+#pragma unroll
+        for (int s = 0; s < kSpecies; s++) {
+            eY_acc[s] = warp_sum(eY_acc[s]);
+            lY_acc[s] = warp_sum(lY_acc[s]);
+        }
+        if (lane == 0) {
+            atomicAdd(&bE[sX], eX_acc);
+            if (want_L) atomicAdd(&bL[sX], lX_acc);
+            for (int s = 0; s < kSpecies; s++) {
+                atomicAdd(&bE[s], eY_acc[s]);
+                if (want_L) atomicAdd(&bL[s], lY_acc[s]);
+            }
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < kSpecies; k += blockDim.x) {
+        if (bE[k] != 0.0) atomicAdd(gE + 3 * NS + 3 * SIMOX_NATOM + k, bE[k]);
+        if (want_L && bL[k] != 0.0) atomicAdd(gL + 3 * NS + 3 * SIMOX_NATOM + k, bL[k]);
+    }
+}
+
+// charges of the sorted order from xq_s.w
+__global__ void adj_load_q(int n, const double4* __restrict__ xq, double* __restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) out[k] = xq[k].w;
+}
+
 // refined charges back into q (original order) and xq_s.w
 __global__ void adj_store_q(int n, const int* __restrict__ sorted, const double* __restrict__ qs,
                             double* __restrict__ q, double4* __restrict__ xq) {
@@ -596,6 +722,7 @@ struct AdjointState {
     double *r = nullptr, *p = nullptr, *Hp = nullptr, *sr = nullptr, *cc = nullptr, *G = nullptr, *tgt = nullptr;
     double *scal = nullptr, *gE = nullptr, *gL = nullptr;
     double* cg = nullptr;   // scalars of the device-side CG loop (CG_* slots)
+    XiTab* xit = nullptr;   // d/dxi of the CTIP pair coefficients
     int cap = 0;
 };
 
@@ -603,7 +730,7 @@ void adjoint_free(simox_ctx* c) {
     AdjointState* A = c->adj;
     if (!A) return;
     void* b[] = {A->spl, A->d2F, A->w, A->wt, A->gam, A->u, A->lam, A->r, A->p, A->Hp, A->sr, A->cc, A->G, A->tgt,
-                 A->scal, A->gE, A->gL, A->cg};
+                 A->scal, A->gE, A->gL, A->cg, A->xit};
     for (void* x : b)
         if (x) cudaFree(x);
     delete A;
@@ -624,6 +751,7 @@ static int adjoint_alloc(simox_ctx* c) {
          cudaMalloc(&A->tgt, sizeof(double) * 3 * N) == cudaSuccess &&
          cudaMalloc(&A->scal, sizeof(double) * 8) == cudaSuccess &&
          cudaMalloc(&A->cg, sizeof(double) * CG_SLOTS) == cudaSuccess &&
+         cudaMalloc(&A->xit, sizeof(XiTab) * kSpecies * kSpecies) == cudaSuccess &&
          cudaMalloc(&A->gE, sizeof(double) * SIMOX_NGRAD) == cudaSuccess &&
          cudaMalloc(&A->gL, sizeof(double) * SIMOX_NGRAD) == cudaSuccess;
     if (!ok) {
@@ -632,6 +760,46 @@ static int adjoint_alloc(simox_ctx* c) {
     }
     A->cap = c->cap;
     return SIMOX_OK;
+}
+
+// Dual number with two derivative components (forward-mode d/dxi_x, d/dxi_y).
+struct Dual2 {
+    double v, d0, d1;
+    Dual2(double x = 0.0) : v(x), d0(0.0), d1(0.0) {}
+    Dual2(double x, double a, double b) : v(x), d0(a), d1(b) {}
+};
+static inline Dual2 operator+(Dual2 a, Dual2 b) { return {a.v + b.v, a.d0 + b.d0, a.d1 + b.d1}; }
+static inline Dual2 operator-(Dual2 a, Dual2 b) { return {a.v - b.v, a.d0 - b.d0, a.d1 - b.d1}; }
+static inline Dual2 operator*(Dual2 a, Dual2 b) {
+    return {a.v * b.v, a.d0 * b.v + a.v * b.d0, a.d1 * b.v + a.v * b.d1};
+}
+static inline Dual2 operator/(Dual2 a, Dual2 b) {
+    const double q = a.v / b.v;
+    return {q, (a.d0 - q * b.d0) / b.v, (a.d1 - q * b.d1) / b.v};
+}
+
+// d/dxi tables: the coefficient construction of the pair tables (fafb from
+// datafmt.f90:201-220, then the force.f90 / ctip.f90 polynomials) run on dual
+// numbers seeded with d xi_x = (1, 0), d xi_y = (0, 1).
+static void xi_tables(const simox_potential& pot, XiTab* out) {
+    for (int X = 0; X < kSpecies; X++)
+        for (int Y = 0; Y < kSpecies; Y++) {
+            const bool same = X == Y;
+            const Dual2 xx(pot.param[X].xi, 1.0, 0.0);
+            const Dual2 xy = same ? xx : Dual2(pot.param[Y].xi, 0.0, 1.0);
+            Dual2 f[4], Px[5], Py[5], Qx[5], Qy[5], Sx[4], Sy[4];
+            slater_fafb<Dual2>(xx, xy, same, f);
+            ctip_coefs<Dual2>(xx, xy, same, f, Px, Py, Qx, Qy, Sx, Sy);
+            XiTab& t = out[X * kSpecies + Y];
+            for (int k = 0; k < 5; k++) {
+                t.dQx[0][k] = Qx[k].d0; t.dQx[1][k] = Qx[k].d1;
+                t.dQy[0][k] = Qy[k].d0; t.dQy[1][k] = Qy[k].d1;
+            }
+            for (int k = 0; k < 4; k++) {
+                t.dSx[0][k] = Sx[k].d0; t.dSx[1][k] = Sx[k].d1;
+                t.dSy[0][k] = Sy[k].d0; t.dSy[1][k] = Sy[k].d1;
+            }
+        }
 }
 
 static AdjParams adj_params(const simox_ctx* c) {
@@ -837,7 +1005,10 @@ int adjoint_eval(simox_ctx* c, const double* f_target, simox_adjoint_report* rep
     const double V = c->box[0] * c->box[1] * c->box[2];
     const double c_pme = SX_KC * (double)c->fft[0] * (double)c->fft[1] * (double)c->fft[2] / V / SX_PI;
     int st;
-    // charges: the reference's CG, then Newton steps on the fixed active set
+    // charges: the reference's CG, then Newton steps on the fixed active set.
+    // The entry charges (sorted order) are kept in u, free until the loss pass.
+    if ((st = ensure_list(c))) return st;
+    adj_load_q<<<nb, 256, 0, s>>>(n, c->xq_s, A->u);
     simox_ctip_report cr;
     if ((st = ctip_solve(c, 0, &cr))) return st;
     R.n_cg = cr.n_cg;
@@ -864,41 +1035,61 @@ int adjoint_eval(simox_ctx* c, const double* f_target, simox_adjoint_report* rep
     // penalties hold it (J' is smaller than the Coulomb coupling of an
     // alternating charge pattern), so a step is solved on the current active
     // set and accepted (halving up to 4 times) only if it lowers ||P G||.
+    const double abs_tol = 1e-11 * std::sqrt((double)n);
+    auto newton = [&](double& rn, int& steps) -> int {
+        for (int it = 0; it < 8 && rn > abs_tol; it++) {
+            cudaMemsetAsync(A->lam, 0, sizeof(double) * n, s);
+            {
+                double m1 = -1.0;
+                cudaMemcpyAsync(A->scal + 4, &m1, sizeof(double), cudaMemcpyHostToDevice, s);
+                cudaMemsetAsync(A->r, 0, sizeof(double) * n, s);
+                adj_axpy<<<nb, 256, 0, s>>>(n, A->scal, 4, 1.0, A->G, A->r);   // r = -G
+            }
+            int its = 0;
+            double rel = 0.0;
+            if (int e = proj_cg(c, S, c_pme, A->r, A->lam, 1e-13, 2000, &its, &rel)) return e;
+            // trial charges q + t delta; the accepted step stays in qs
+            cudaMemcpyAsync(A->gam, c->qs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);   // saved q
+            bool accepted = false;
+            double t = 1.0;
+            for (int ls = 0; ls < 5 && !accepted; ls++, t *= 0.5) {
+                cudaMemcpyAsync(c->qs, A->gam, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
+                cudaMemcpyAsync(A->scal + 5, &t, sizeof(double), cudaMemcpyHostToDevice, s);
+                adj_axpy<<<nb, 256, 0, s>>>(n, A->scal, 5, 1.0, A->lam, c->qs);
+                if (int e = grad_u(nullptr)) return e;
+                const double rt = resid();
+                if (rt < rn) {
+                    rn = rt;
+                    accepted = true;
+                }
+            }
+            steps = it + 1;
+            if (!accepted) {   // no step lowers the residual: keep the previous charges
+                cudaMemcpyAsync(c->qs, A->gam, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
+                if (int e = grad_u(nullptr)) return e;
+                break;
+            }
+        }
+        return SIMOX_OK;
+    };
     double Uq = 0.0;
     if ((st = grad_u(nullptr))) return st;
     double rn = resid();
-    const double abs_tol = 1e-11 * std::sqrt((double)n);
-    for (int it = 0; it < 8 && rn > abs_tol; it++) {
-        cudaMemsetAsync(A->lam, 0, sizeof(double) * n, s);
-        {
-            double m1 = -1.0;
-            cudaMemcpyAsync(A->scal + 4, &m1, sizeof(double), cudaMemcpyHostToDevice, s);
-            cudaMemsetAsync(A->r, 0, sizeof(double) * n, s);
-            adj_axpy<<<nb, 256, 0, s>>>(n, A->scal, 4, 1.0, A->G, A->r);   // r = -G
-        }
-        int its = 0;
-        double rel = 0.0;
-        if ((st = proj_cg(c, S, c_pme, A->r, A->lam, 1e-13, 2000, &its, &rel))) return st;
-        // trial charges q + t delta; the accepted step stays in qs
-        cudaMemcpyAsync(A->gam, c->qs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);   // saved q (gam is free here)
-        bool accepted = false;
-        double t = 1.0;
-        for (int ls = 0; ls < 5 && !accepted; ls++, t *= 0.5) {
-            cudaMemcpyAsync(c->qs, A->gam, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
-            cudaMemcpyAsync(A->scal + 5, &t, sizeof(double), cudaMemcpyHostToDevice, s);
-            adj_axpy<<<nb, 256, 0, s>>>(n, A->scal, 5, 1.0, A->lam, c->qs);
-            if ((st = grad_u(nullptr))) return st;
-            const double rt = resid();
-            if (rt < rn) {
-                rn = rt;
-                accepted = true;
-            }
-        }
-        R.n_newton = it + 1;
-        if (!accepted) {   // no step lowers the residual: keep the previous charges
-            cudaMemcpyAsync(c->qs, A->gam, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
-            break;
-        }
+    int steps = 0;
+    if ((st = newton(rn, steps))) return st;
+    R.n_newton = steps;
+    if (rn > 1e-9 * std::sqrt((double)n)) {
+        // Stalled: the CG's last line search can leave the charges where the
+        // functional is not convex on the current active set.  Restart the
+        // refinement from the entry charges and keep the smaller residual.
+        cudaMemcpyAsync(A->tgt, c->qs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);   // first result
+        cudaMemcpyAsync(c->qs, A->u, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
+        if ((st = grad_u(nullptr))) return st;
+        double rn2 = resid();
+        int steps2 = 0;
+        if ((st = newton(rn2, steps2))) return st;
+        R.n_newton += steps2;
+        if (!(rn2 < rn)) cudaMemcpyAsync(c->qs, A->tgt, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
     }
     if ((st = grad_u(&Uq))) return st;
     {   // residual ||P G||
@@ -971,6 +1162,15 @@ int adjoint_eval(simox_ctx* c, const double* f_target, simox_adjoint_report* rep
         adj_ctip_grad_kernel<<<g, AT, 0, s>>>(P, c->tab_d, c->xq_s, c->t_s, reinterpret_cast<const int2*>(c->nn),
                                               c->nbr, c->qs, want_L ? A->lam : nullptr, A->gE, A->gL);
     }
+    {
+        XiTab hx[kSpecies * kSpecies];
+        xi_tables(c->pot, hx);
+        cudaMemcpyAsync(A->xit, hx, sizeof(hx), cudaMemcpyHostToDevice, s);
+        Launch L(c, "adjoint_grad_xi");
+        adj_xi_grad_kernel<<<g, AT, 0, s>>>(P, c->tab_d, A->xit, c->xq_s, c->t_s,
+                                            reinterpret_cast<const int2*>(c->nn), c->nbr, c->qs,
+                                            want_L ? A->lam : nullptr, want_L ? A->w : nullptr, A->gE, A->gL);
+    }
     if ((st = check_launch(c))) return st;
     if (grad_E) cudaMemcpyAsync(grad_E, A->gE, sizeof(double) * SIMOX_NGRAD, cudaMemcpyDeviceToHost, s);
     if (grad_L) cudaMemcpyAsync(grad_L, A->gL, sizeof(double) * SIMOX_NGRAD, cudaMemcpyDeviceToHost, s);
@@ -1024,6 +1224,19 @@ extern "C" int simox_set_ctip_params(simox_ctx* c, int species, double chi, doub
     p.J = J;
     p.Z = Z;
     return sx::build_pair_tables(c);   // Z enters the pair tables
+}
+
+extern "C" int simox_set_ctip_xi(simox_ctx* c, int species, double xi) {
+    if (!c || species < 1 || species > SIMOX_NATOM || !(xi > 0.0) || !std::isfinite(xi)) return SIMOX_E_ARG;
+    for (int s = 0; s < SIMOX_NATOM; s++)
+        if (s != species - 1 && c->pot.param[s].xi == xi) return SIMOX_E_ARG;
+    cudaSetDevice(c->device);
+    c->pot.param[species - 1].xi = xi;
+    for (int i = 0; i < SIMOX_NATOM; i++)   // datafmt.f90:201-220 for every pair involving the species
+        for (int j = 0; j < SIMOX_NATOM; j++)
+            if (i == species - 1 || j == species - 1)
+                sx::slater_fafb<double>(c->pot.param[i].xi, c->pot.param[j].xi, i == j, c->pot.param[i].fafb[j]);
+    return sx::build_pair_tables(c);
 }
 
 extern "C" int simox_adjoint_eval(simox_ctx* c, const double* f_target, simox_adjoint_report* rep, double* forces,

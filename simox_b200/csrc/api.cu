@@ -287,21 +287,7 @@ extern "C" int simox_default_potential(simox_potential* P) {
     }
     // Slater 1s Coulomb-integral coefficients (datafmt.f90:201-220)
     for (int i = 0; i < 5; i++)
-        for (int j = 0; j < 5; j++) {
-            double* f = P->param[i].fafb[j];
-            if (i == j) {
-                double x = xi[i];
-                f[0] = 1.0; f[1] = 11.0 * x / 8.0; f[2] = 0.75 * (x * x); f[3] = (x * x * x) / 6.0;
-            } else {
-                double a = xi[i], b = xi[j];
-                double apb = a + b, amb = a - b, bma = b - a;
-                double a2 = a * a, b2 = b * b, a4 = a2 * a2, b4 = b2 * b2;
-                f[0] = a * b4 / (apb * apb) / (amb * amb);
-                f[1] = b * a4 / (apb * apb) / (bma * bma);
-                f[2] = (3.0 * a2 * b4 - b4 * b2) / (apb * apb * apb) / (amb * amb * amb);
-                f[3] = (3.0 * b2 * a4 - a4 * a2) / (apb * apb * apb) / (bma * bma * bma);
-            }
-        }
+        for (int j = 0; j < 5; j++) sx::slater_fafb<double>(xi[i], xi[j], i == j, P->param[i].fafb[j]);
     simox_oxid& o = P->oxygn;
     const double ore[5] = {2.98520, 2.95732, 3.07992, 3.64857, 1.0};
     const double oal[5] = {8.49741, 7.96528, 7.52309, 5.44072, 0.0};

@@ -62,28 +62,12 @@ static void fill_tab(const simox_potential& P, PairTab<R>* T) {
             const simox_potn& pX = P.param[X];
             const simox_potn& pY = P.param[Y];
             t.xi_x = (R)pX.xi; t.xi_y = (R)pY.xi; t.Z_x = (R)pX.Z; t.Z_y = (R)pY.Z;
-            const double* f = pX.fafb[Y];
-            if (X == Y) {
-                double xi = pX.xi;
-                // fifj = -e (1 + f2 r + f3 r^2 + f4 r^3)              force.f90:107-110
-                t.Px[0] = 1; t.Px[1] = (R)f[1]; t.Px[2] = (R)f[2]; t.Px[3] = (R)f[3]; t.Px[4] = 0;
-                // dfifj = e((2xi r+1)(1/r^2+f2/r+f3+f4 r) - (f2/r+2f3+3f4 r)) force.f90:111-118
-                t.Qx[0] = (R)(2 * xi * f[1] - f[2]); t.Qx[1] = (R)(2 * xi * f[2] - 2 * f[3]);
-                t.Qx[2] = (R)(2 * xi * f[3]); t.Qx[3] = (R)(2 * xi); t.Qx[4] = 1;
-                // CTIP_SOLVER: -e (1 + xr(f2 + xr(f3 + xr f4)))/r, xr = xi r  ctip.f90:91-93
-                t.Sx[0] = 1; t.Sx[1] = (R)(f[1] * xi); t.Sx[2] = (R)(f[2] * xi * xi); t.Sx[3] = (R)(f[3] * xi * xi * xi);
-            } else {
-                double xx = pX.xi, xy = pY.xi;
-                // fifj = -f1 eX - f2 eY - f3 eX/r - f4 eY/r            force.f90:126-129
-                t.Px[0] = (R)f[0]; t.Px[4] = (R)f[2];
-                t.Py[0] = (R)f[1]; t.Py[4] = (R)f[3];
-                // dfifj = 2xX f1 eX + 2xY f2 eY + f3 eX(1+2xX r)/r^2 + f4 eY(1+2xY r)/r^2  force.f90:130-133
-                t.Qx[0] = (R)(2 * xx * f[0]); t.Qx[3] = (R)(2 * xx * f[2]); t.Qx[4] = (R)f[2];
-                t.Qy[0] = (R)(2 * xy * f[1]); t.Qy[3] = (R)(2 * xy * f[3]); t.Qy[4] = (R)f[3];
-                // CTIP_SOLVER: -eX(f1 + f3/r) - eY(f2 + f4/r)          ctip.f90:97-100
-                t.Sx[0] = (R)f[2]; t.Sx[1] = (R)f[0];
-                t.Sy[0] = (R)f[3]; t.Sy[1] = (R)f[1];
+            double cPx[5], cPy[5], cQx[5], cQy[5], cSx[4], cSy[4];
+            ctip_coefs<double>(pX.xi, pY.xi, X == Y, pX.fafb[Y], cPx, cPy, cQx, cQy, cSx, cSy);
+            for (int k = 0; k < 5; k++) {
+                t.Px[k] = (R)cPx[k]; t.Py[k] = (R)cPy[k]; t.Qx[k] = (R)cQx[k]; t.Qy[k] = (R)cQy[k];
             }
+            for (int k = 0; k < 4; k++) { t.Sx[k] = (R)cSx[k]; t.Sy[k] = (R)cSy[k]; }
             T[X * kSpecies + Y] = t;
         }
 }

@@ -70,6 +70,55 @@ struct PairTab {
     int pad_;
 };
 
+// Slater 1s Coulomb-integral coefficients fafb(a,b,1..4) (datafmt.f90:201-220)
+// for the exponents xa of the row species and xb of the column species; same:
+// the diagonal form.  T = double, or a dual number for d/dxi.
+template <typename T>
+inline void slater_fafb(T xa, T xb, bool same, T f[4]) {
+    if (same) {
+        f[0] = T(1.0);
+        f[1] = 11.0 * xa / 8.0;
+        f[2] = 0.75 * (xa * xa);
+        f[3] = (xa * xa * xa) / 6.0;
+    } else {
+        const T apb = xa + xb, amb = xa - xb, bma = xb - xa;
+        const T a2 = xa * xa, b2 = xb * xb, a4 = a2 * a2, b4 = b2 * b2;
+        f[0] = xa * b4 / (apb * apb) / (amb * amb);
+        f[1] = xb * a4 / (apb * apb) / (bma * bma);
+        f[2] = (3.0 * a2 * b4 - b4 * b2) / (apb * apb * apb) / (amb * amb * amb);
+        f[3] = (3.0 * b2 * a4 - a4 * a2) / (apb * apb * apb) / (bma * bma * bma);
+    }
+}
+
+// CTIP coefficient polynomials of one pair table entry (PairTab Px..Sy) from
+// the exponents xx (X), xy (Y) and X's fafb row entry f for Y.  T as above.
+template <typename T>
+inline void ctip_coefs(T xx, T xy, bool same, const T f[4], T Px[5], T Py[5], T Qx[5], T Qy[5], T Sx[4],
+                       T Sy[4]) {
+    for (int k = 0; k < 5; k++) Px[k] = Py[k] = Qx[k] = Qy[k] = T(0.0);
+    for (int k = 0; k < 4; k++) Sx[k] = Sy[k] = T(0.0);
+    if (same) {
+        const T xi = xx;
+        // fifj = -e (1 + f2 r + f3 r^2 + f4 r^3)              force.f90:107-110
+        Px[0] = T(1.0); Px[1] = f[1]; Px[2] = f[2]; Px[3] = f[3];
+        // dfifj = e((2xi r+1)(1/r^2+f2/r+f3+f4 r) - (f2/r+2f3+3f4 r)) force.f90:111-118
+        Qx[0] = 2.0 * xi * f[1] - f[2]; Qx[1] = 2.0 * xi * f[2] - 2.0 * f[3];
+        Qx[2] = 2.0 * xi * f[3]; Qx[3] = 2.0 * xi; Qx[4] = T(1.0);
+        // CTIP_SOLVER: -e (1 + xr(f2 + xr(f3 + xr f4)))/r, xr = xi r  ctip.f90:91-93
+        Sx[0] = T(1.0); Sx[1] = f[1] * xi; Sx[2] = f[2] * xi * xi; Sx[3] = f[3] * xi * xi * xi;
+    } else {
+        // fifj = -f1 eX - f2 eY - f3 eX/r - f4 eY/r            force.f90:126-129
+        Px[0] = f[0]; Px[4] = f[2];
+        Py[0] = f[1]; Py[4] = f[3];
+        // dfifj = 2xX f1 eX + 2xY f2 eY + f3 eX(1+2xX r)/r^2 + f4 eY(1+2xY r)/r^2  force.f90:130-133
+        Qx[0] = 2.0 * xx * f[0]; Qx[3] = 2.0 * xx * f[2]; Qx[4] = f[2];
+        Qy[0] = 2.0 * xy * f[1]; Qy[3] = 2.0 * xy * f[3]; Qy[4] = f[3];
+        // CTIP_SOLVER: -eX(f1 + f3/r) - eY(f2 + f4/r)          ctip.f90:97-100
+        Sx[0] = f[2]; Sx[1] = f[0];
+        Sy[0] = f[3]; Sy[1] = f[1];
+    }
+}
+
 // Device resources of one PME precision (grid, half spectrum, G/N, plans).
 struct PmeRes {
     bool dbl = false, ready = false;

@@ -56,11 +56,12 @@ def test_spline_model_reproduces_analytic_forces():
 
 
 def _params(g, P, spl, theta):
-    """theta = (192 spline coefficients, chi/J/Z of Al and O)"""
+    """theta = (192 spline coefficients, chi/J/Z of Al and O, xi of Al and O)"""
     g.set_eam_spline(spline.with_coefficients(spl, theta[:3 * NS]))
     for k, sp in enumerate((1, 4)):
         chi, J, Z = theta[3 * NS + 3 * k: 3 * NS + 3 * k + 3]
         g.set_ctip_params(sp, chi, J, Z)
+        g.set_ctip_xi(sp, theta[3 * NS + 6 + k])
 
 
 def _theta0(P, spl):
@@ -68,7 +69,8 @@ def _theta0(P, spl):
     for sp in (1, 4):
         p = P.param[sp - 1]
         c.append([p.chi, p.J, p.Z])
-    return np.concatenate([c[0], np.array(c[1]), np.array(c[2])])
+    xi = [P.param[0].xi, P.param[3].xi]
+    return np.concatenate([c[0], np.array(c[1]), np.array(c[2]), np.array(xi)])
 
 
 def _grad_index(k):
@@ -76,6 +78,8 @@ def _grad_index(k):
     if k < 3 * NS:
         return k
     j = k - 3 * NS
+    if j >= 6:                      # xi of Al, O: after chi/J/Z of all five species
+        return 3 * NS + 3 * _abi.NATOM + (0, 3)[j - 6]
     sp = (1, 4)[j // 3]
     return 3 * NS + 3 * (sp - 1) + j % 3
 
@@ -98,7 +102,7 @@ def test_energy_and_loss_gradients_match_finite_differences():
         for fn in range(3):
             block = np.abs(gL[fn * NS:(fn + 1) * NS]) + np.abs(gE[fn * NS:(fn + 1) * NS])
             picks += list(fn * NS + np.argsort(block)[-3:])
-        picks += [3 * NS + j for j in range(6)]
+        picks += [3 * NS + j for j in range(8)]   # chi, J, Z, xi of Al and O
         h = 1e-4
         for k in picks:
             vals = []
@@ -151,7 +155,7 @@ def test_adjoint_eval_many_matches_one_by_one():
 
 
 def test_adjoint_as_autograd_function():
-    """The adjoint wrapped as a torch.autograd.Function of the 207 parameters
+    """The adjoint wrapped as a torch.autograd.Function of the 212 parameters
     (test harness only; the library exposes it through the C ABI):
     backward() of loss + 0.5 E returns grad_L + 0.5 grad_E, and a central
     difference through the wrapper (step 1e-4) agrees with grad_L on the
@@ -169,15 +173,19 @@ def test_adjoint_as_autograd_function():
         # theta in the NGRAD layout (chi, J, Z of all five species)
         th = np.zeros(_abi.NGRAD)
         th[:3 * NS] = th0[:3 * NS]
+        x0 = 3 * NS + 3 * _abi.NATOM
         for sp in range(1, 6):
             p = P.param[sp - 1]
             th[3 * NS + 3 * (sp - 1): 3 * NS + 3 * sp] = [p.chi, p.J, p.Z]
+            th[x0 + sp - 1] = p.xi
 
         def set_all(theta):
             g.set_eam_spline(spline.with_coefficients(spl, theta[:3 * NS]))
             for sp in range(1, 6):
                 chi, J, Z = theta[3 * NS + 3 * (sp - 1): 3 * NS + 3 * sp]
                 g.set_ctip_params(sp, chi, J, Z)
+                if sp < 5:                                   # H (xi 0) is not on the device path
+                    g.set_ctip_xi(sp, theta[x0 + sp - 1])
 
         saved = {}
 
