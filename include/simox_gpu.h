@@ -139,6 +139,12 @@ typedef struct {
     int    accumulate_rdf;    /* 1 = accumulate the RDF histogram in FORCE        */
     int    freq_stat;         /* energies (FP64) on steps with MOD(step, freq_stat)
                                  == 0 (TAG_SET's status rule); <= 0: every step  */
+    int    thermo_stoch;      /* with thermostat = 1: 1 = the stochastic pair
+                                 VV_NVT1_STOCH / VV_NVT2_STOCH (tag%thermo_stoch)
+                                 instead of VV_NVE1 / VV_NVT2_BEREND; such steps
+                                 run without CUDA graphs                         */
+    double alpha;             /* friction of the stochastic thermostat (Nset%alpha) */
+    unsigned long long seed;  /* seed of its random forces (see simox_vinit)      */
 } simox_md_opts;
 
 typedef struct simox_ctx simox_ctx;
@@ -210,6 +216,29 @@ int simox_vv_nve1(simox_ctx* ctx, double dt);                      /* vverlet.f9
 int simox_vv_nve1_reflect(simox_ctx* ctx, double dt);              /* vverlet.f90:100-129 */
 int simox_vv_nve2(simox_ctx* ctx, double dt, double* mv2);         /* vverlet.f90:132-157 */
 int simox_vv_nvt2_berend(simox_ctx* ctx, double dt, double T_given, double* mv2); /* vverlet.f90:160-208 */
+
+/* ---- VINIT and the stochastic thermostat --------------------------------
+ * The reference draws its random numbers from Fortran's RANDOM_NUMBER after
+ * RANDOM_SEED (main.f90:28), a stream no other program reproduces.  Here every
+ * draw is a pure function of (seed, stream, counter) -- the SplitMix64 output
+ * mix applied twice, 53 bits scaled into [0, 1) -- so a run is reproducible
+ * from its seed on any device and the CPU oracle draws the same numbers.
+ * Streams: VINIT (1 << 62 | atom), counter = component; the thermostat at step
+ * s (s << 32 | atom), counters 2 (256 d + k), 2 (256 d + k) + 1 for attempt k
+ * of component d (atom = index in the caller's order). */
+/* VINIT (vverlet.f90:2-71): velocities U[-0.5, 0.5) per component, mean
+ * removed, scaled per species to T_given (eV); then FORCE + PME at x - dt v
+ * (VV_NVE1 with -dt and zero forces) into f, with x and v restored.  Needs
+ * PME_SELF and CELL_SORT first, like the reference.  e (may be NULL): the
+ * energies of that FORCE + PME; mv2 (may be NULL): VINIT's as-written sum,
+ * every atom's v^2 times the last atom's mass (vverlet.f90:64-69). */
+int simox_vinit(simox_ctx* ctx, unsigned long long seed, double T_given, double dt, simox_energies* e,
+                double* mv2);
+int simox_vv_nvt1_stoch(simox_ctx* ctx, double dt, double alpha);   /* vverlet.f90:237-260 */
+/* f += fluct * sqrt(2 alpha T_given / dt) (util.f90:84-101, draws of step
+ * `step`), then the damped half kick; mv2 = sum m v^2 */
+int simox_vv_nvt2_stoch(simox_ctx* ctx, double dt, double alpha, double T_given,
+                        unsigned long long seed, unsigned long long step, double* mv2); /* vverlet.f90:263-296 */
 
 /* ---- device-resident main loop (main.f90:40-84) -------------------------
  * Runs steps first_step .. first_step+nsteps-1 of the reference loop on the

@@ -68,6 +68,17 @@ def lib():
         L.or_vv_nvt2_berend.argtypes = [C.c_int, C.POINTER(_abi.Potential), _ip, _dp, _dp,
                                         C.c_double, C.c_double]
         L.or_vv_nvt2_berend.restype = C.c_double
+        L.or_rng_uniform.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64]
+        L.or_rng_uniform.restype = C.c_double
+        L.or_fluct.argtypes = [C.c_uint64, C.c_uint64, C.c_int, C.c_int, C.c_double, _ip]
+        L.or_fluct.restype = C.c_double
+        L.or_vinit_velocities.argtypes = [C.c_int, C.POINTER(_abi.Potential), _ip, _dp, C.c_uint64, C.c_double]
+        L.or_vinit_velocities.restype = C.c_double
+        L.or_vv_nvt1_stoch.argtypes = [C.c_int, _dp, C.POINTER(_abi.Potential), _ip, _dp, _dp, _dp,
+                                       C.c_double, C.c_double]
+        L.or_vv_nvt2_stoch.argtypes = [C.c_int, C.POINTER(_abi.Potential), _ip, _dp, _dp, C.c_double,
+                                       C.c_double, C.c_double, C.c_uint64, C.c_uint64, _ip]
+        L.or_vv_nvt2_stoch.restype = C.c_double
         L.or_set_spread_round.argtypes = [C.c_int]
         _lib = L
     return _lib
@@ -245,6 +256,41 @@ class System:
         mv2 = lib().or_vv_nvt2_berend(self.n, C.byref(self.pot), _i(self.ids), _d(v), _d(_c64(f)),
                                       float(dt), float(T_given))
         return v, mv2
+
+    # -- VINIT and the stochastic thermostat (seeded counter-based draws) --
+    def vinit_velocities(self, seed, T_given):
+        """VINIT's velocities (vverlet.f90:19-55) and its as-written mv2."""
+        v = np.zeros((self.n, 3))
+        mv2 = lib().or_vinit_velocities(self.n, C.byref(self.pot), _i(self.ids), _d(v), int(seed), float(T_given))
+        return v, mv2
+
+    def vv_nvt1_stoch(self, v, f, dt, alpha):
+        """VV_NVT1_STOCH (vverlet.f90:237-260): moves self.x, returns v."""
+        v = _c64(v).copy()
+        lib().or_vv_nvt1_stoch(self.n, _d(self.box), C.byref(self.pot), _i(self.ids), _d(self.x), _d(v),
+                               _d(_c64(f)), float(dt), float(alpha))
+        return v
+
+    def vv_nvt2_stoch(self, v, f, dt, alpha, T_given, seed, step):
+        """VV_NVT2_STOCH (vverlet.f90:263-296): returns (v, f with the random
+        force added, mv2)."""
+        v = _c64(v).copy()
+        f = _c64(f).copy()
+        bad = np.zeros(1, np.int32)
+        mv2 = lib().or_vv_nvt2_stoch(self.n, C.byref(self.pot), _i(self.ids), _d(v), _d(f), float(dt),
+                                     float(alpha), float(T_given), int(seed), int(step), _i(bad))
+        if bad[0]:
+            raise OracleError(_abi.SIMOX_E_ARG)
+        return v, f, mv2
+
+
+def rng_uniform(seed: int, a: int, b: int) -> float:
+    return lib().or_rng_uniform(int(seed), int(a), int(b))
+
+
+def fluct(seed: int, step: int, i: int, d: int, x: float = 1.0) -> float:
+    bad = np.zeros(1, np.int32)
+    return lib().or_fluct(int(seed), int(step), int(i), int(d), float(x), _i(bad))
 
 
 def zfft3d(a: np.ndarray, iopt: int) -> np.ndarray:

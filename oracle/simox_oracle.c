@@ -1262,3 +1262,111 @@ double or_vv_nvt2_berend(int n, const simox_potential* P, const int* id, double*
     }
     return mv2;
 }
+
+/* ---------------------------------------------------------------------- */
+/* Random numbers of VINIT and the stochastic thermostat.  The reference  */
+/* draws from Fortran's RANDOM_NUMBER after RANDOM_SEED (main.f90:28),    */
+/* which no other program can reproduce; both this oracle and the GPU     */
+/* library use the same seeded counter-based generator instead: the       */
+/* SplitMix64 output mix (Steele, Lea & Flood, OOPSLA 2014) applied to    */
+/* (seed, stream a, counter b), 53 bits scaled into [0, 1).               */
+/* ---------------------------------------------------------------------- */
+static uint64_t or_mix64(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+double or_rng_uniform(uint64_t seed, uint64_t a, uint64_t b)
+{
+    const uint64_t g = 0x9E3779B97F4A7C15ULL;
+    uint64_t z = or_mix64(or_mix64(seed + g * (a + 1)) + g * (b + 1));
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+/* fluct (util.f90:84-101): Marsaglia's polar method, v1 kept.  The draw of
+ * component d of atom i at step `step` uses stream (step << 32 | i) and
+ * counters 2 (256 d + k) and 2 (256 d + k) + 1 for attempt k < 100; after 100
+ * rejected attempts (probability (1 - pi/4)^100) it returns 0 and sets *bad. */
+double or_fluct(uint64_t seed, uint64_t step, int i, int d, double x, int* bad)
+{
+    const uint64_t a = (step << 32) | (uint64_t)(uint32_t)i;
+    for (int k = 0; k < 100; k++) {
+        const uint64_t b = 2 * (uint64_t)(256 * d + k);
+        double v1 = 2.0 * or_rng_uniform(seed, a, b) - 1.0;
+        double v2 = 2.0 * or_rng_uniform(seed, a, b + 1) - 1.0;
+        double r = v1 * v1 + v2 * v2;
+        if (r < 1.0 && r > 0.0) return v1 * sqrt(-2.0 * log(r) / r) * x;
+    }
+    *bad = 1;
+    return 0.0;
+}
+
+/* VINIT velocities (vverlet.f90:19-55; VINIT is vverlet.f90:2-71): uniform in [-0.5, 0.5) from stream
+ * (1 << 62 | i), counter d; the mean removed; scaled per species to T_given.
+ * Returns the as-written mv2 of vverlet.f90:64-69, which multiplies every
+ * atom's v^2 by the mass left in xm by the previous loop (the last atom's). */
+double or_vinit_velocities(int n, const simox_potential* P, const int* id, double* v, uint64_t seed,
+                           double T_given)
+{
+    double sumv[3] = {0.0, 0.0, 0.0}, mv2[SIMOX_NATOM] = {0}, lambda[SIMOX_NATOM] = {0};
+    int Npt[SIMOX_NATOM] = {0};
+    for (int i = 0; i < n; i++)
+        for (int d = 0; d < 3; d++) {
+            v[3 * i + d] = or_rng_uniform(seed, (1ULL << 62) | (uint64_t)(uint32_t)i, (uint64_t)d) - 0.5;
+            sumv[d] = sumv[d] + v[3 * i + d];
+        }
+    for (int d = 0; d < 3; d++) sumv[d] = sumv[d] / (double)n;
+    double xm = 0.0;
+    for (int i = 0; i < n; i++) {
+        for (int d = 0; d < 3; d++) v[3 * i + d] = v[3 * i + d] - sumv[d];
+        xm = P->param[id[i] - 1].xm;
+        mv2[id[i] - 1] += xm * (v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2]);
+        Npt[id[i] - 1]++;
+    }
+    for (int s = 0; s < SIMOX_NATOM; s++)
+        if (Npt[s] > 0) {
+            double T0 = mv2[s] / (double)(Npt[s] * 3);
+            lambda[s] = sqrt(T_given / T0);
+        }
+    double out = 0.0;
+    for (int i = 0; i < n; i++) {
+        for (int d = 0; d < 3; d++) v[3 * i + d] = v[3 * i + d] * lambda[id[i] - 1];
+        out = out + xm * (v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2]);
+    }
+    return out;
+}
+
+/* VV_NVT1_STOCH vverlet.f90:237-260 */
+void or_vv_nvt1_stoch(int n, const double box[3], const simox_potential* P, const int* id,
+                      double* x, double* v, const double* f, double dt, double alpha)
+{
+    for (int i = 0; i < n; i++) {
+        double xm = P->param[id[i] - 1].xm;
+        for (int d = 0; d < 3; d++) {
+            v[3 * i + d] = v[3 * i + d] * (1.0 - 0.5 * alpha * dt / xm) + 0.5 * dt * f[3 * i + d] / xm;
+            double xx = x[3 * i + d] + dt * v[3 * i + d];
+            x[3 * i + d] = xx - box[d] * round(xx / box[d]);
+        }
+    }
+}
+
+/* VV_NVT2_STOCH vverlet.f90:263-296 (sigma 1): f gains the random force;
+ * returns mv2, *bad as or_fluct */
+double or_vv_nvt2_stoch(int n, const simox_potential* P, const int* id, double* v, double* f, double dt,
+                        double alpha, double T_given, uint64_t seed, uint64_t step, int* bad)
+{
+    double beta = sqrt(2.0 * alpha * T_given / dt), mv2 = 0.0;
+    for (int i = 0; i < n; i++) {
+        double xm = P->param[id[i] - 1].xm, t = 0.0;
+        for (int d = 0; d < 3; d++) {
+            double eta = or_fluct(seed, step, i, d, 1.0, bad);
+            f[3 * i + d] = f[3 * i + d] + eta * beta;
+            v[3 * i + d] = (v[3 * i + d] + 0.5 * dt * f[3 * i + d] / xm) / (1.0 + 0.5 * alpha * dt / xm);
+            t = t + xm * (v[3 * i + d] * v[3 * i + d]);
+        }
+        mv2 = mv2 + t;
+    }
+    return mv2;
+}

@@ -111,7 +111,8 @@ class CtipReport(C.Structure):
 class MdOpts(C.Structure):
     _fields_ = [("dt", C.c_double), ("thermostat", C.c_int), ("T_given", C.c_double),
                 ("freq_new", C.c_int), ("freq_sort", C.c_int), ("reflect", C.c_int),
-                ("charge_every_step", C.c_int), ("accumulate_rdf", C.c_int), ("freq_stat", C.c_int)]
+                ("charge_every_step", C.c_int), ("accumulate_rdf", C.c_int), ("freq_stat", C.c_int),
+                ("thermo_stoch", C.c_int), ("alpha", C.c_double), ("seed", C.c_ulonglong)]
 
 
 def potential_to_bytes(p: Potential) -> bytes:
@@ -125,6 +126,7 @@ EXPORTED = [
     "simox_cell_hierarchy", "simox_cell_sort", "simox_get_cells",
     "simox_pme_self", "simox_get_psi", "simox_ctip_solve", "simox_force", "simox_pme", "simox_get_eam",
     "simox_vv_nve1", "simox_vv_nve1_reflect", "simox_vv_nve2", "simox_vv_nvt2_berend",
+    "simox_vinit", "simox_vv_nvt1_stoch", "simox_vv_nvt2_stoch",
     "simox_md_run", "simox_timer_begin", "simox_timer_end", "simox_profile_enable",
     "simox_profile_read", "simox_profile_reset", "simox_launch_count", "simox_sync",
     "simox_neighbor_stats", "simox_cell_sort_noalloc",

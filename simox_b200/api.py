@@ -67,6 +67,9 @@ def lib():
         "simox_vv_nve1_reflect": [_vp, C.c_double],
         "simox_vv_nve2": [_vp, C.c_double, _dp],
         "simox_vv_nvt2_berend": [_vp, C.c_double, C.c_double, _dp],
+        "simox_vinit": [_vp, C.c_ulonglong, C.c_double, C.c_double, C.POINTER(Energies), _dp],
+        "simox_vv_nvt1_stoch": [_vp, C.c_double, C.c_double],
+        "simox_vv_nvt2_stoch": [_vp, C.c_double, C.c_double, C.c_double, C.c_ulonglong, C.c_ulonglong, _dp],
         "simox_md_run": [_vp, C.POINTER(MdOpts), C.c_int, C.c_int, C.POINTER(Energies), _ip],
         "simox_timer_begin": [_vp],
         "simox_timer_end": [_vp, C.POINTER(C.c_float)],
@@ -285,14 +288,35 @@ class Simox:
         _check(lib().simox_vv_nvt2_berend(self._ctx, float(dt), float(T_given), C.byref(mv2)), "VV_NVT2_BEREND")
         return mv2.value
 
+    def vinit(self, seed: int, T_given: float, dt: float):
+        """VINIT: seeded velocities at T_given, forces at x - dt v (x, v kept).
+        Returns (energies of that FORCE + PME, VINIT's as-written mv2)."""
+        e = Energies()
+        mv2 = C.c_double(0.0)
+        _check(lib().simox_vinit(self._ctx, int(seed), float(T_given), float(dt), C.byref(e), C.byref(mv2)),
+               "VINIT")
+        return e.as_dict(), mv2.value
+
+    def vv_nvt1_stoch(self, dt: float, alpha: float):
+        _check(lib().simox_vv_nvt1_stoch(self._ctx, float(dt), float(alpha)), "VV_NVT1_STOCH")
+
+    def vv_nvt2_stoch(self, dt: float, alpha: float, T_given: float, seed: int, step: int) -> float:
+        mv2 = C.c_double(0.0)
+        _check(lib().simox_vv_nvt2_stoch(self._ctx, float(dt), float(alpha), float(T_given), int(seed), int(step),
+                                         C.byref(mv2)), "VV_NVT2_STOCH")
+        return mv2.value
+
     # -- main loop ----------------------------------------------------------
     def md_run(self, nsteps: int, dt: float, first_step: int = 1, thermostat: bool = False,
                T_given: float = 0.0, freq_new: int = 0, freq_sort: int = 1, reflect: bool = False,
-               charge_every_step: bool = False, rdf: np.ndarray | None = None, freq_stat: int = 0):
+               charge_every_step: bool = False, rdf: np.ndarray | None = None, freq_stat: int = 0,
+               thermo_stoch: bool = False, alpha: float = 0.0, seed: int = 0):
         """Steps first_step..first_step+nsteps-1 of main.f90:40-84 on the device.
         Energies (FP64) are evaluated on steps with MOD(step, freq_stat) == 0,
         TAG_SET's status rule (every step with freq_stat <= 0); the returned
-        energies are those of the last such step, mv2 that of the final step."""
+        energies are those of the last such step, mv2 that of the final step.
+        thermostat with thermo_stoch: the stochastic pair VV_NVT1_STOCH /
+        VV_NVT2_STOCH with friction alpha and random forces from seed."""
         o = MdOpts()
         o.dt = float(dt)
         o.thermostat = 1 if thermostat else 0
@@ -303,6 +327,9 @@ class Simox:
         o.charge_every_step = 1 if charge_every_step else 0
         o.accumulate_rdf = 1 if rdf is not None else 0
         o.freq_stat = int(freq_stat)
+        o.thermo_stoch = 1 if thermo_stoch else 0
+        o.alpha = float(alpha)
+        o.seed = int(seed)
         e = Energies()
         _check(lib().simox_md_run(self._ctx, C.byref(o), int(first_step), int(nsteps), C.byref(e), _i(rdf)),
                "md_run")

@@ -117,14 +117,15 @@ static int pme_fork(simox_ctx* c, bool estep) {
     return SIMOX_OK;
 }
 
-// One step without CTIP: VV_NVE1, CELL_SORT, FORCE (+ PME on the side
-// stream), VV_NVE2 / VV_NVT2_BEREND.  Every launch goes to c->stream or, for
+// One step without CTIP: VV_NVE1 (or VV_NVT1_STOCH), CELL_SORT, FORCE (+ PME
+// on the side stream), VV_NVE2 / VV_NVT2_BEREND / VV_NVT2_STOCH.  Every launch goes to c->stream or, for
 // PME, to c->side forked from and joined back to it, so the whole step can be
 // captured into one CUDA graph.
 int md_step(simox_ctx* c, const simox_md_opts* o, bool sort, bool estep, bool want_rdf) {
     int st;
     if (estep) cudaMemsetAsync(c->acc, 0, sizeof(double) * (A_EREC + 1), c->stream);
-    if ((st = vv1(c, o->dt, o->reflect != 0))) return st;
+    const bool stoch = o->thermostat && o->thermo_stoch;
+    if ((st = stoch ? nvt1_stoch(c, o->dt, o->alpha) : vv1(c, o->dt, o->reflect != 0))) return st;
     if (sort && (st = cell_sort(c))) return st;
     // PME (positions and charges only) runs on the side stream while the
     // pair passes run; its forces land in f_rec and the second half kick
@@ -135,7 +136,8 @@ int md_step(simox_ctx* c, const simox_md_opts* o, bool sort, bool estep, bool wa
     if ((st = eam_density(c, estep))) return st;
     if ((st = pair_forces(c, estep, want_rdf))) return st;
     cudaStreamWaitEvent(c->stream, c->ev_join, 0);
-    if (o->thermostat) st = nvt2_berend(c, o->dt, o->T_given, true, c->f_rec);
+    if (stoch) st = nvt2_stoch(c, o->dt, o->alpha, o->T_given, o->seed, c->md_step_no, true, c->f_rec);
+    else if (o->thermostat) st = nvt2_berend(c, o->dt, o->T_given, true, c->f_rec);
     else st = vv2(c, o->dt, true, c->f_rec);
     return st;
 }
@@ -199,13 +201,15 @@ int md_run(simox_ctx* c, const simox_md_opts* o, int first, int nsteps, simox_en
     if (want_rdf) cudaMemsetAsync(c->rdf, 0, sizeof(int) * SIMOX_RDF_LEN, c->stream);
     int st = SIMOX_OK;
     for (int step = first; step < first + nsteps; step++) {
+        c->md_step_no = (unsigned long long)step;
         const bool new_charge = o->freq_new > 0 && (o->charge_every_step || step % o->freq_new == 1);
         const bool sort = o->freq_sort > 0 && step % o->freq_sort == 0;
         const bool estep = o->freq_stat <= 0 || step % o->freq_stat == 0;   // TAG_SET status rule
         if (new_charge) {
             // CTIP_SOLVER between CELL_SORT and FORCE: eager (host-driven CG)
             if (estep) cudaMemsetAsync(c->acc, 0, sizeof(double) * (A_EREC + 1), c->stream);
-            if ((st = vv1(c, o->dt, o->reflect != 0))) return st;
+            const bool stoch = o->thermostat && o->thermo_stoch;
+            if ((st = stoch ? nvt1_stoch(c, o->dt, o->alpha) : vv1(c, o->dt, o->reflect != 0))) return st;
             if (sort && (st = cell_sort(c))) return st;
             simox_ctip_report rep;
             if ((st = ctip_solve(c, 0, &rep))) return st;
@@ -217,14 +221,17 @@ int md_run(simox_ctx* c, const simox_md_opts* o, int first, int nsteps, simox_en
             if ((st = eam_density(c, estep))) return st;
             if ((st = pair_forces(c, estep, want_rdf))) return st;
             cudaStreamWaitEvent(c->stream, c->ev_join, 0);
-            if (o2.thermostat) st = nvt2_berend(c, o2.dt, o2.T_given, true, c->f_rec);
+            if (stoch) st = nvt2_stoch(c, o2.dt, o2.alpha, o2.T_given, o2.seed, c->md_step_no, true, c->f_rec);
+            else if (o2.thermostat) st = nvt2_berend(c, o2.dt, o2.T_given, true, c->f_rec);
             else st = vv2(c, o2.dt, true, c->f_rec);
             if (st) return st;
             continue;
         }
         // a graph replays only the launches it captured: the first step after
         // a new atom set (skin list seeded from the host) runs eagerly
-        const bool graph_ok = c->graphs_on && !c->profiling && (!c->skin_mode || c->skin_valid);
+        // stochastic steps stay eager too: their draws depend on the step number
+        const bool graph_ok = c->graphs_on && !c->profiling && (!c->skin_mode || c->skin_valid) &&
+                              !(o->thermostat && o->thermo_stoch);
         st = graph_ok ? md_step_graph(c, o, sort, estep, want_rdf) : md_step(c, o, sort, estep, want_rdf);
         if (st) return st;
     }
@@ -713,6 +720,66 @@ extern "C" int simox_vv_nvt2_berend(simox_ctx* c, double dt, double T_given, dou
     cudaSetDevice(c->device);
     int st = nvt2_berend(c, dt, T_given, false);
     return st ? st : read_mv2(c, mv2);
+}
+
+extern "C" int simox_vv_nvt1_stoch(simox_ctx* c, double dt, double alpha) {
+    if (!c) return SIMOX_E_ARG;
+    cudaSetDevice(c->device);
+    int st = nvt1_stoch(c, dt, alpha);
+    return st ? st : cuda_status(cudaStreamSynchronize(c->stream));
+}
+
+extern "C" int simox_vv_nvt2_stoch(simox_ctx* c, double dt, double alpha, double T_given, unsigned long long seed,
+                                   unsigned long long step, double* mv2) {
+    if (!c || !(dt != 0.0) || !(alpha >= 0.0) || !(T_given >= 0.0)) return SIMOX_E_ARG;
+    cudaSetDevice(c->device);
+    int st = nvt2_stoch(c, dt, alpha, T_given, seed, step, false, nullptr);
+    return st ? st : read_mv2(c, mv2);
+}
+
+// VINIT vverlet.f90:2-71
+extern "C" int simox_vinit(simox_ctx* c, unsigned long long seed, double T_given, double dt, simox_energies* e,
+                           double* mv2) {
+    if (!c || !(T_given >= 0.0)) return SIMOX_E_ARG;
+    cudaSetDevice(c->device);
+    if (!c->cells_valid || !c->psi_valid) return SIMOX_E_STATE;
+    const int n = c->n;
+    double mv2_v = 0.0;
+    int st = vinit_velocities(c, seed, T_given);
+    if (st || (st = read_mv2(c, &mv2_v))) return st;
+    if (mv2) *mv2 = mv2_v;
+    if (n == 0) return SIMOX_OK;
+    // forces at x - dt v (VV_NVE1 with -dt and zero forces), then x and v
+    // back (vverlet.f90:57-70); v is unchanged by the zero-force kick
+    double* x0 = nullptr;
+    if (cudaMalloc(&x0, sizeof(double) * 3 * n) != cudaSuccess) {
+        cudaGetLastError();
+        return SIMOX_E_NOMEM;
+    }
+    const bool in_box = c->in_box;
+    cudaMemcpyAsync(x0, c->x, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, c->stream);
+    cudaMemsetAsync(c->f, 0, sizeof(double) * 3 * n, c->stream);
+    simox_energies ef{}, ep{};
+    st = vv1(c, -dt, false);
+    if (!st) st = simox_force(c, e ? &ef : nullptr, nullptr);
+    if (!st) st = simox_pme(c, e ? &ep : nullptr);
+    cudaMemcpyAsync(c->x, x0, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, c->stream);
+    const cudaError_t se = cudaStreamSynchronize(c->stream);
+    cudaFree(x0);
+    c->gathered = false;
+    c->list_valid = false;
+    c->eam_valid = false;
+    c->cells_fresh = false;
+    c->in_box = in_box;
+    if (st) return st;
+    if (se != cudaSuccess) return cuda_status(se);
+    if (e) {
+        *e = ef;
+        e->Erec = ep.Erec;
+        e->Eself = c->eself;
+        e->mv2 = mv2_v;
+    }
+    return SIMOX_OK;
 }
 
 extern "C" int simox_md_run(simox_ctx* c, const simox_md_opts* o, int first_step, int nsteps, simox_energies* e,

@@ -49,6 +49,7 @@ int check_opts(const simox_batch* b, const simox_md_opts* o) {
         if (o[k].freq_new != 0 || o[k].charge_every_step) return SIMOX_E_ARG;
         if (o[k].freq_sort != o[0].freq_sort || o[k].freq_stat != o[0].freq_stat) return SIMOX_E_ARG;
         if (o[k].accumulate_rdf) return SIMOX_E_ARG;
+        if (o[k].thermostat && o[k].thermo_stoch) return SIMOX_E_ARG;   // per-step draws: not graph-replayable
         if (!b->ctx[k]->psi_valid || !b->ctx[k]->cells_valid) return SIMOX_E_STATE;
     }
     return SIMOX_OK;

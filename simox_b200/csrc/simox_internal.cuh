@@ -160,6 +160,7 @@ struct simox_ctx {
     size_t ngrid = 0, nhalf = 0;
     int npt_max = SIMOX_NPT_MAX, nnb_cap = 1024;
     int force_splits = 2;       // CTAs per skin cell of the mixed force pass (simox_set_tuning)
+    unsigned long long md_step_no = 0;   // md_run's current step: the stochastic thermostat's draw counter
     sx::AdjointState* adj = nullptr;   // parameter-adjoint model (simox_set_eam_spline)
     bool spline_on = false;
 
@@ -348,6 +349,10 @@ int update_masses(simox_ctx* c);
 int md_run(simox_ctx* c, const simox_md_opts* o, int first, int nsteps, simox_energies* e, int* rdf);
 void drop_graphs(simox_ctx* c);
 int md_step(simox_ctx* c, const simox_md_opts* o, bool sort, bool estep, bool want_rdf);
+int vinit_velocities(simox_ctx* c, unsigned long long seed, double T_given);
+int nvt1_stoch(simox_ctx* c, double dt, double alpha);
+int nvt2_stoch(simox_ctx* c, double dt, double alpha, double T_given, unsigned long long seed,
+               unsigned long long step, bool subtract_mean, const double* f_add);
 
 // device helpers -------------------------------------------------------------
 __device__ __forceinline__ double warp_sum(double v) {

@@ -201,3 +201,65 @@ def test_ctip_oracle_keeps_total_charge_and_converges():
     assert abs(o.q.sum() - q0) < 1e-10
     al, ox = o.q[s.ids == 1], o.q[s.ids == 4]
     assert al.mean() > 0 > ox.mean()       # charge transfer Al -> O
+
+
+# -- VINIT and the stochastic thermostat: the seeded counter-based draws ------
+
+_M64 = (1 << 64) - 1
+
+
+def _mix64(z):
+    """SplitMix64 output mix (Steele, Lea & Flood 2014), in Python integers."""
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & _M64
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & _M64
+    return z ^ (z >> 31)
+
+
+def _uniform(seed, a, b):
+    g = 0x9E3779B97F4A7C15
+    z = _mix64((_mix64((seed + g * (a + 1)) & _M64) + g * (b + 1)) & _M64)
+    return (z >> 11) * (1.0 / 9007199254740992.0)
+
+
+def test_rng_is_the_stated_splitmix_construction():
+    """The C oracle's draws equal an independent Python statement of the same
+    construction, bit for bit (streams of VINIT and of the thermostat)."""
+    for seed in (0, 1, 12345, (1 << 63) + 17):
+        for a in (0, 5, (1 << 62) | 7, (3 << 32) | 11):
+            for b in (0, 1, 2, 513):
+                assert O.rng_uniform(seed, a, b) == _uniform(seed, a, b)
+
+
+def test_rng_uniform_and_fluct_statistics():
+    """20,000 draws: uniforms in [0, 1) with mean 1/2 and variance 1/12; the
+    polar-method normals (util.f90 fluct) with mean 0 and variance 1, each
+    within 5 standard errors."""
+    u = np.array([O.rng_uniform(99, k >> 2, k & 3) for k in range(20000)])
+    assert u.min() >= 0.0 and u.max() < 1.0
+    assert abs(u.mean() - 0.5) < 5 * np.sqrt(1 / 12 / u.size)
+    assert abs(u.var() - 1 / 12) < 5 * np.sqrt(1 / 180 / u.size)
+    g = np.array([O.fluct(7, 3, i, d) for i in range(6667) for d in range(3)])
+    assert abs(g.mean()) < 5 / np.sqrt(g.size)
+    assert abs(g.var() - 1.0) < 5 * np.sqrt(2.0 / g.size)
+    assert abs(np.mean(g ** 4) / g.var() ** 2 - 3.0) < 0.3   # Gaussian kurtosis
+
+
+def test_vinit_velocities_species_temperature():
+    """VINIT (vverlet.f90:19-55): reproducible from the seed, each species'
+    mean m v^2 / 3 equals T_given after the per-species rescale, and the
+    returned mv2 is the as-written sum with the last atom's mass.  (The mean
+    removal before the rescale leaves sum v = 0 only for a single species.)"""
+    s = S.small_alo(seed=3, n=400, o_frac=0.4)
+    o = O.System(s.ids, s.x, s.q, s.box, s.rcut, s.fft, order=s.order)
+    T = 600.0 * S.KB
+    v, mv2 = o.vinit_velocities(11, T)
+    v2, _ = o.vinit_velocities(11, T)
+    assert np.array_equal(v, v2)                                  # reproducible from the seed
+    assert not np.array_equal(v, o.vinit_velocities(12, T)[0])
+    pot = O.potential_setup()
+    xm = np.array([pot.param[i - 1].xm for i in s.ids])
+    for sp in (1, 4):
+        sel = s.ids == sp
+        Tsp = np.sum(xm[sel, None] * v[sel] ** 2) / (3 * sel.sum())
+        assert abs(Tsp - T) <= 1e-12 * T
+    assert abs(mv2 - xm[-1] * np.sum(v ** 2)) <= 1e-12 * mv2
