@@ -61,6 +61,10 @@ extern "C" {
                                        eam.f90:38-168) are not on the GPU path */
 #define SIMOX_E_SCRATCH_LIMIT  -17  /* simox_cell_sort_noalloc: more than 65,536 cells
                                        or a link stride above 4,096 */
+#define SIMOX_E_IO             -18  /* checkpoint file cannot be opened, read or written,
+                                       is not a checkpoint, or its box differs */
+#define SIMOX_E_RNG            -19  /* VV_NVT2_STOCH: a random-force draw rejected 100
+                                       polar-method attempts (probability 3e-67) */
 
 /* ---- precision modes --------------------------------------------------- */
 #define SIMOX_FP64   0   /* every term in FP64 (the FP64 GPU oracle path) */
@@ -239,6 +243,25 @@ int simox_vv_nvt1_stoch(simox_ctx* ctx, double dt, double alpha);   /* vverlet.f
  * `step`), then the damped half kick; mv2 = sum m v^2 */
 int simox_vv_nvt2_stoch(simox_ctx* ctx, double dt, double alpha, double T_given,
                         unsigned long long seed, unsigned long long step, double* mv2); /* vverlet.f90:263-296 */
+
+/* ---- checkpoint and status output -----------------------------------------
+ * The reference restarts from restart.xyz, written by PRINT_SNAPSHOT
+ * (util.f90:22-81) with ES13.6 positions and ES11.4 velocities and forces, so
+ * a restarted run does not continue the original trajectory.  The checkpoint
+ * keeps every bit of the state: a little-endian file of the 8 bytes
+ * "SIMOXCK1", int32 version (1), int32 n, int64 step, double box[3], then
+ * int32 id[n], double x[n][3], v[n][3], f[n][3], q[n] (original order). */
+int simox_checkpoint_write(simox_ctx* ctx, const char* path, long long step);
+/* Reads a checkpoint into the context (as simox_set_state with ids); the box
+ * must equal the context's, n its capacity or less.  *step (may be NULL)
+ * receives the stored step.  SIMOX_E_IO for a missing, short or foreign file. */
+int simox_checkpoint_read(simox_ctx* ctx, const char* path, long long* step);
+/* PRINT_STAT's line (util.f90:3-19), host only: time (fs) = step TFM dt,
+ * T (K) = mv2 / (3 n) / kB, E_total = E_es + E_eam + mv2 / 2, E_es = Eself +
+ * Edir + Erec + Ectip, E_eam, Epair, Egroup, in the reference's
+ * FORMAT (ES11.4, 1X, F6.1, 5(1X, ES11.4)) ("******" where F6.1 overflows).
+ * buf receives the line without newline (len >= 80). */
+int simox_format_status(const simox_energies* e, int n_atoms, int step, double dt, char* buf, int len);
 
 /* ---- device-resident main loop (main.f90:40-84) -------------------------
  * Runs steps first_step .. first_step+nsteps-1 of the reference loop on the

@@ -32,6 +32,8 @@ SIMOX_E_STATE = -14
 SIMOX_E_NO_DEVICE = -15
 SIMOX_E_UNSUPPORTED = -16
 SIMOX_E_SCRATCH_LIMIT = -17
+SIMOX_E_IO = -18
+SIMOX_E_RNG = -19
 
 SIMOX_FP64 = 0
 SIMOX_MIXED = 1
@@ -59,6 +61,8 @@ _STATUS = {
     SIMOX_E_NO_DEVICE: "no CUDA device",
     SIMOX_E_UNSUPPORTED: "hetero-metal pair form not implemented on the GPU path",
     SIMOX_E_SCRATCH_LIMIT: "size beyond the fixed scratch of simox_cell_sort_noalloc (65536 cells, stride 4096)",
+    SIMOX_E_IO: "=== cannot open checkpoint, or not a checkpoint of this box ===",
+    SIMOX_E_RNG: "random-force draw rejected 100 polar-method attempts",
 }
 
 
@@ -127,6 +131,7 @@ EXPORTED = [
     "simox_pme_self", "simox_get_psi", "simox_ctip_solve", "simox_force", "simox_pme", "simox_get_eam",
     "simox_vv_nve1", "simox_vv_nve1_reflect", "simox_vv_nve2", "simox_vv_nvt2_berend",
     "simox_vinit", "simox_vv_nvt1_stoch", "simox_vv_nvt2_stoch",
+    "simox_checkpoint_write", "simox_checkpoint_read", "simox_format_status",
     "simox_md_run", "simox_timer_begin", "simox_timer_end", "simox_profile_enable",
     "simox_profile_read", "simox_profile_reset", "simox_launch_count", "simox_sync",
     "simox_neighbor_stats", "simox_cell_sort_noalloc",

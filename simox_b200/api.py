@@ -68,6 +68,9 @@ def lib():
         "simox_vv_nve2": [_vp, C.c_double, _dp],
         "simox_vv_nvt2_berend": [_vp, C.c_double, C.c_double, _dp],
         "simox_vinit": [_vp, C.c_ulonglong, C.c_double, C.c_double, C.POINTER(Energies), _dp],
+        "simox_checkpoint_write": [_vp, C.c_char_p, C.c_longlong],
+        "simox_checkpoint_read": [_vp, C.c_char_p, C.POINTER(C.c_longlong)],
+        "simox_format_status": [C.POINTER(Energies), C.c_int, C.c_int, C.c_double, C.c_char_p, C.c_int],
         "simox_vv_nvt1_stoch": [_vp, C.c_double, C.c_double],
         "simox_vv_nvt2_stoch": [_vp, C.c_double, C.c_double, C.c_double, C.c_ulonglong, C.c_ulonglong, _dp],
         "simox_md_run": [_vp, C.POINTER(MdOpts), C.c_int, C.c_int, C.POINTER(Energies), _ip],
@@ -297,6 +300,19 @@ class Simox:
                "VINIT")
         return e.as_dict(), mv2.value
 
+    def checkpoint_write(self, path: str, step: int = 0):
+        """Every bit of ids, x, v, f, q (simox_checkpoint_write)."""
+        _check(lib().simox_checkpoint_write(self._ctx, os.fsencode(path), int(step)), "checkpoint_write")
+
+    def checkpoint_read(self, path: str) -> int:
+        """Loads a checkpoint of this box into the context; returns its step."""
+        step = C.c_longlong(0)
+        _check(lib().simox_checkpoint_read(self._ctx, os.fsencode(path), C.byref(step)), "checkpoint_read")
+        n = C.c_int(0)
+        _check(lib().simox_get_natoms(self._ctx, C.byref(n)), "get_natoms")
+        self.n = n.value
+        return step.value
+
     def vv_nvt1_stoch(self, dt: float, alpha: float):
         _check(lib().simox_vv_nvt1_stoch(self._ctx, float(dt), float(alpha)), "VV_NVT1_STOCH")
 
@@ -414,6 +430,17 @@ def from_system(sys_, precision="fp64", **kw) -> Simox:
     """Context for a :class:`simox_b200.systems.AtomSystem`."""
     return Simox(sys_.ids, sys_.x, sys_.box, sys_.fft, rcut=sys_.rcut, q=sys_.q, v=sys_.v,
                  order=sys_.order, precision=precision, **kw)
+
+
+def format_status(e: dict, n_atoms: int, step: int, dt: float) -> str:
+    """PRINT_STAT's line (util.f90:3-19) for energies e (a simox_energies
+    dict), host only."""
+    en = Energies()
+    for k in ("Eself", "Edir", "Erec", "Ectip", "Epair", "Egroup", "mv2"):
+        setattr(en, k, float(e.get(k, 0.0)))
+    buf = C.create_string_buffer(128)
+    _check(lib().simox_format_status(C.byref(en), int(n_atoms), int(step), float(dt), buf, 128), "format_status")
+    return buf.value.decode()
 
 
 def md_opts(dt: float, thermostat: bool = False, T_given: float = 0.0, freq_new: int = 0, freq_sort: int = 1,

@@ -33,6 +33,7 @@ int read_status(simox_ctx* c) {
     if (s & ST_UNKNOWN_ELEMENT) return SIMOX_E_UNKNOWN_ELEMENT;
     if (s & ST_UNSUPPORTED) return SIMOX_E_UNSUPPORTED;
     if (s & ST_LINE_NOBRACKET) return SIMOX_E_BRENT;
+    if (s & ST_RNG) return SIMOX_E_RNG;
     return SIMOX_OK;
 }
 
@@ -342,6 +343,8 @@ extern "C" const char* simox_status_string(int s) {
         case SIMOX_E_NO_DEVICE: return "no CUDA device";
         case SIMOX_E_UNSUPPORTED: return "hetero-metal pair form not implemented on the GPU path";
         case SIMOX_E_SCRATCH_LIMIT: return "size beyond the fixed scratch of simox_cell_sort_noalloc (65536 cells, stride 4096)";
+        case SIMOX_E_IO: return "=== cannot open checkpoint, or not a checkpoint of this box ===";
+        case SIMOX_E_RNG: return "random-force draw rejected 100 polar-method attempts";
         default: return "unknown status";
     }
 }
@@ -735,6 +738,84 @@ extern "C" int simox_vv_nvt2_stoch(simox_ctx* c, double dt, double alpha, double
     cudaSetDevice(c->device);
     int st = nvt2_stoch(c, dt, alpha, T_given, seed, step, false, nullptr);
     return st ? st : read_mv2(c, mv2);
+}
+
+// ---- binary FP64 checkpoint ------------------------------------------------
+static const char kCkMagic[8] = {'S', 'I', 'M', 'O', 'X', 'C', 'K', '1'};
+
+extern "C" int simox_checkpoint_write(simox_ctx* c, const char* path, long long step) {
+    if (!c || !path) return SIMOX_E_ARG;
+    if (!c->have_ids) return SIMOX_E_STATE;
+    const int n = c->n;
+    const size_t m = (size_t)std::max(n, 1);
+    std::vector<int> id(m);
+    std::vector<double> x(3 * m), v(3 * m), f(3 * m), q(m);
+    int st = simox_get_state(c, n, id.data(), x.data(), v.data(), f.data(), q.data());
+    if (st) return st;
+    FILE* fp = std::fopen(path, "wb");
+    if (!fp) return SIMOX_E_IO;
+    const int32_t version = 1, nn = n;
+    const int64_t s64 = step;
+    bool ok = std::fwrite(kCkMagic, 1, 8, fp) == 8 && std::fwrite(&version, 4, 1, fp) == 1 &&
+              std::fwrite(&nn, 4, 1, fp) == 1 && std::fwrite(&s64, 8, 1, fp) == 1 &&
+              std::fwrite(c->box, 8, 3, fp) == 3;
+    if (n > 0) {
+        ok = ok && std::fwrite(id.data(), 4, (size_t)n, fp) == (size_t)n &&
+             std::fwrite(x.data(), 8, 3 * (size_t)n, fp) == 3 * (size_t)n &&
+             std::fwrite(v.data(), 8, 3 * (size_t)n, fp) == 3 * (size_t)n &&
+             std::fwrite(f.data(), 8, 3 * (size_t)n, fp) == 3 * (size_t)n &&
+             std::fwrite(q.data(), 8, (size_t)n, fp) == (size_t)n;
+    }
+    ok = (std::fclose(fp) == 0) && ok;
+    return ok ? SIMOX_OK : SIMOX_E_IO;
+}
+
+extern "C" int simox_checkpoint_read(simox_ctx* c, const char* path, long long* step) {
+    if (!c || !path) return SIMOX_E_ARG;
+    FILE* fp = std::fopen(path, "rb");
+    if (!fp) return SIMOX_E_IO;
+    char magic[8];
+    int32_t version = 0, nn = -1;
+    int64_t s64 = 0;
+    double box[3];
+    bool ok = std::fread(magic, 1, 8, fp) == 8 && std::memcmp(magic, kCkMagic, 8) == 0 &&
+              std::fread(&version, 4, 1, fp) == 1 && version == 1 && std::fread(&nn, 4, 1, fp) == 1 && nn >= 0 &&
+              std::fread(&s64, 8, 1, fp) == 1 && std::fread(box, 8, 3, fp) == 3;
+    ok = ok && box[0] == c->box[0] && box[1] == c->box[1] && box[2] == c->box[2];
+    if (ok && nn > c->cap) {
+        std::fclose(fp);
+        return SIMOX_E_CAPACITY;
+    }
+    const size_t n = ok ? (size_t)nn : 0, m = std::max<size_t>(n, 1);
+    std::vector<int> id(m);
+    std::vector<double> x(3 * m), v(3 * m), f(3 * m), q(m);
+    if (ok && n > 0) {
+        ok = std::fread(id.data(), 4, n, fp) == n && std::fread(x.data(), 8, 3 * n, fp) == 3 * n &&
+             std::fread(v.data(), 8, 3 * n, fp) == 3 * n && std::fread(f.data(), 8, 3 * n, fp) == 3 * n &&
+             std::fread(q.data(), 8, n, fp) == n;
+    }
+    std::fclose(fp);
+    if (!ok) return SIMOX_E_IO;
+    const int st = simox_set_state(c, (int)n, id.data(), x.data(), v.data(), f.data(), q.data());
+    if (st) return st;
+    if (step) *step = (long long)s64;
+    return SIMOX_OK;
+}
+
+// PRINT_STAT util.f90:3-19, FORMAT (ES11.4, 1X, F6.1, 5(1X, ES11.4))
+extern "C" int simox_format_status(const simox_energies* e, int n_atoms, int step, double dt, char* buf, int len) {
+    if (!e || !buf || len < 80 || n_atoms <= 0) return SIMOX_E_ARG;
+    const double kB = 8.617343e-5;                                      // datafmt.f90:27
+    const double E_es = e->Eself + e->Edir + e->Erec + e->Ectip;
+    const double E_eam = e->Epair + e->Egroup;
+    const double E_total = E_es + E_eam + e->mv2 / 2.0;
+    const double T = e->mv2 / (double)(n_atoms * 3) / kB;
+    char tf[32];
+    std::snprintf(tf, sizeof(tf), "%6.1f", T);
+    if (std::strlen(tf) > 6 || !std::isfinite(T)) std::snprintf(tf, sizeof(tf), "******");   // F6.1 overflow
+    std::snprintf(buf, (size_t)len, "%11.4E %s %11.4E %11.4E %11.4E %11.4E %11.4E", (double)step * SX_TFM * dt, tf,
+                  E_total, E_es, E_eam, e->Epair, e->Egroup);
+    return SIMOX_OK;
 }
 
 // VINIT vverlet.f90:2-71

@@ -290,7 +290,7 @@ __global__ void __launch_bounds__(256)
         }
         mv2 = t;
     }
-    if (bad) atomicOr(status, ST_UNSUPPORTED);   // 100 rejected polar-method attempts
+    if (bad) atomicOr(status, ST_RNG);   // 100 rejected polar-method attempts
     block_add<256>(mv2, acc, A_MV2, red);
 }
 

@@ -34,7 +34,8 @@ constexpr unsigned kCodeMask = 31u;
 // Device status bits (OR-ed by kernels, read by the host after a call).
 enum : int {
     ST_CELL_OVERFLOW = 1, ST_NBR_OVERFLOW = 2, ST_UNKNOWN_PAIR = 4, ST_UNKNOWN_ELEMENT = 8,
-    ST_POSITION = 16, ST_UNSUPPORTED = 32, ST_LINE_NOBRACKET = 64   // Brent: 100 steps without convergence
+    ST_POSITION = 16, ST_UNSUPPORTED = 32, ST_LINE_NOBRACKET = 64,  // Brent: 100 steps without convergence
+    ST_RNG = 128                                                     // thermostat: 100 rejected draws
 };
 
 // Slots of the FP64 accumulator array (energies and reductions).

@@ -11,7 +11,10 @@
   solve reproduces U to ~1e-11 relative between evaluations; L, through the
   forces, carries ~1e-7 relative noise from it, so loss differences at small
   steps measure that noise (in isolated runs they agree with the adjoint to
-  ~1e-8 at steps 1e-3 and 1e-4).
+  ~1e-8 at steps 1e-3 and 1e-4).  The CTIP functional is not convex, and now
+  and then the two solves of one difference settle in different local minima
+  (1e-6 eV apart, observed once in ~40 differences): a component whose
+  difference misses the bar is retried with steps 2e-4 and 5e-5.
 """
 import numpy as np
 import pytest
@@ -97,28 +100,34 @@ def test_energy_and_loss_gradients_match_finite_differences():
         rep, _, gE, gL = g.adjoint_eval(target)
         q0 = g.get_state()["q"]
         assert rep["adj_residual"] <= 1e-10
-        # components: the largest spline-coefficient gradients of each function, and chi, J, Z of Al and O
+        # components: the largest spline-coefficient gradients of each function, and chi, J, Z, xi of Al and O
         picks = []
         for fn in range(3):
             block = np.abs(gL[fn * NS:(fn + 1) * NS]) + np.abs(gE[fn * NS:(fn + 1) * NS])
             picks += list(fn * NS + np.argsort(block)[-3:])
         picks += [3 * NS + j for j in range(8)]   # chi, J, Z, xi of Al and O
-        h = 1e-4
         for k in picks:
-            vals = []
-            for sgn in (1.0, -1.0):
-                th = th0.copy()
-                th[k] += sgn * h
-                _params(g, P, spl, th)
-                g.set_state(q=q0)
-                r, _, _, _ = g.adjoint_eval(target, gradients=False)
-                assert r["residual"] <= 1e-8 * np.sqrt(s.n), r
-                vals.append((r["E"], r["loss"]))
-            dE = (vals[0][0] - vals[1][0]) / (2 * h)
-            dL = (vals[0][1] - vals[1][1]) / (2 * h)
             j = _grad_index(k)
-            assert abs(dE - gE[j]) <= 1e-4 * abs(gE[j]) + 1e-6 * np.abs(gE).max(), (k, dE, gE[j])
-            assert abs(dL - gL[j]) <= 1e-3 * abs(gL[j]) + 1e-6 * np.abs(gL).max(), (k, dL, gL[j])
+            tolE = 1e-4 * abs(gE[j]) + 1e-6 * np.abs(gE).max()
+            tolL = 1e-3 * abs(gL[j]) + 1e-6 * np.abs(gL).max()
+            tried = []
+            for h in (1e-4, 2e-4, 5e-5):   # a step whose two solves land on different local minima is retried
+                vals = []
+                for sgn in (1.0, -1.0):
+                    th = th0.copy()
+                    th[k] += sgn * h
+                    _params(g, P, spl, th)
+                    g.set_state(q=q0)
+                    r, _, _, _ = g.adjoint_eval(target, gradients=False)
+                    assert r["residual"] <= 1e-8 * np.sqrt(s.n), r
+                    vals.append((r["E"], r["loss"]))
+                dE = (vals[0][0] - vals[1][0]) / (2 * h)
+                dL = (vals[0][1] - vals[1][1]) / (2 * h)
+                tried.append((h, dE, dL))
+                if abs(dE - gE[j]) <= tolE and abs(dL - gL[j]) <= tolL:
+                    break
+            assert abs(dE - gE[j]) <= tolE, (k, tried, gE[j])
+            assert abs(dL - gL[j]) <= tolL, (k, tried, gL[j])
         _params(g, P, spl, th0)
 
 
