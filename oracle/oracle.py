@@ -79,6 +79,9 @@ def lib():
         L.or_vv_nvt2_stoch.argtypes = [C.c_int, C.POINTER(_abi.Potential), _ip, _dp, _dp, C.c_double,
                                        C.c_double, C.c_double, C.c_uint64, C.c_uint64, _ip]
         L.or_vv_nvt2_stoch.restype = C.c_double
+        L.or_remove_rigid_motion.argtypes = [C.c_int, _dp, _dp]
+        L.or_oxide_check.argtypes = [C.c_int, _ip, _dp, _dp, C.c_int, C.c_double]
+        L.or_random_position_o2.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_uint64, C.c_uint64, _dp]
         L.or_set_spread_round.argtypes = [C.c_int]
         _lib = L
     return _lib
@@ -315,3 +318,23 @@ def bspline_gen(p: int, u: float):
     dw = np.zeros(16)
     lib().or_bspline_gen(int(p), float(u), _d(w), _d(dw))
     return w[:p].copy(), dw[:p].copy()
+
+
+# -- oxidation-mode host steps (main.f90:62-84) --
+def remove_rigid_motion(x, v):
+    x = _c64(x).copy()
+    v = _c64(v).copy()
+    lib().or_remove_rigid_motion(x.shape[0], _d(x), _d(v))
+    return x, v
+
+
+def oxide_check(ids, x, q, n_o2, q_crit) -> bool:
+    ids = np.ascontiguousarray(ids, dtype=np.int32)
+    return bool(lib().or_oxide_check(ids.size, _i(ids), _d(_c64(x)), _d(_c64(q)), int(n_o2), float(q_crit)))
+
+
+def random_position_o2(n_o, z_new, Lx, Ly, seed, event):
+    xx = np.zeros((2 * (n_o // 2), 3))
+    if lib().or_random_position_o2(int(n_o), float(z_new), float(Lx), float(Ly), int(seed), int(event), _d(xx)):
+        raise OracleError(_abi.SIMOX_E_ARG)
+    return xx

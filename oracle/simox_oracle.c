@@ -1370,3 +1370,82 @@ double or_vv_nvt2_stoch(int n, const simox_potential* P, const int* id, double* 
     }
     return mv2;
 }
+
+/* ====================================================================== */
+/* Oxidation-mode host steps (main.f90:62-84)                             */
+/* ====================================================================== */
+/* REMOVE_RIGID_MOTION vverlet.f90:211-234 */
+void or_remove_rigid_motion(int n, double* x, double* v)
+{
+    double sumv[3] = {0.0, 0.0, 0.0}, avg_z = 0.0;
+    if (n <= 0) return;
+    for (int i = 0; i < n; i++) {
+        for (int d = 0; d < 3; d++) sumv[d] = sumv[d] + v[3 * i + d];
+        avg_z = avg_z + x[3 * i + 2];
+    }
+    for (int d = 0; d < 3; d++) sumv[d] = sumv[d] / (double)n;
+    avg_z = avg_z / (double)n;
+    for (int i = 0; i < n; i++) {
+        for (int d = 0; d < 3; d++) v[3 * i + d] = v[3 * i + d] - sumv[d];
+        x[3 * i + 2] = x[3 * i + 2] - avg_z;
+    }
+}
+
+/* OXIDE_CHECK util.f90:152-188; returns 1 when a new dimer is due */
+int or_oxide_check(int n, const int* id, const double* x, const double* q, int n_o2, double q_crit)
+{
+    double m_height = 0.0, o_height = 0.0, q_max = -10.0;
+    for (int i = 0; i < n; i++)
+        if (id[i] == 1) m_height = fmax(x[3 * i + 2], m_height);
+    for (int i = n - 1; i >= n - 2 * n_o2 && i >= 0; i--)
+        if (id[i] == 4) {
+            o_height = fmax(x[3 * i + 2], o_height);
+            q_max = fmax(q[i], q_max);
+        }
+    return ((m_height + 0.0) > o_height || q_max < q_crit) ? 1 : 0;
+}
+
+/* RANDOM_POSITION_O2 util.f90:104-148 with the seeded draws of stream
+ * (1 << 63 | event), counter = draw number in the reference's order.
+ * Returns 0, or -1 for "=== Too many new oxygens ===" / no room. */
+int or_random_position_o2(int n_o, double z_new, double Lx, double Ly, uint64_t seed, uint64_t event,
+                          double* xx)
+{
+    const double L0 = 2.0;
+    int n_o2 = n_o / 2;
+    if (n_o2 <= 0) return 0;
+    double Rcut = sqrt(Lx * Ly / (double)n_o2) * 0.5;
+    if (Rcut < L0) return -1;
+    double Rcut2 = Rcut * Rcut;
+    uint64_t a = (1ULL << 63) | event, k = 0;
+    double* cx = (double*)calloc((size_t)n_o2 * 3, sizeof(double));
+    if (!cx) return -1;
+    cx[0] = (or_rng_uniform(seed, a, k++) - 0.5) * Lx;
+    cx[1] = (or_rng_uniform(seed, a, k++) - 0.5) * Ly;
+    for (int i = 1; i < n_o2; i++) {
+        int placed = 0;
+        for (int t = 0; t < 100000 && !placed; t++) {
+            cx[3 * i] = (or_rng_uniform(seed, a, k++) - 0.5) * Lx;
+            cx[3 * i + 1] = (or_rng_uniform(seed, a, k++) - 0.5) * Ly;
+            placed = 1;
+            for (int j = 0; j < i; j++) {
+                double dx = cx[3 * i] - cx[3 * j], dy = cx[3 * i + 1] - cx[3 * j + 1];
+                double r2 = dx * dx + dy * dy;
+                if (r2 < Rcut2) placed = 0;
+            }
+        }
+        if (!placed) { free(cx); return -1; }
+    }
+    for (int i = 0; i < n_o2; i++) cx[3 * i + 2] = z_new;
+    for (int i = 0; i < n_o2; i++) {
+        double phi = or_rng_uniform(seed, a, k++) * M_PI * 2.0;
+        double theta = or_rng_uniform(seed, a, k++) * M_PI;
+        double d[3] = {L0 * sin(theta) * cos(phi), L0 * sin(theta) * cos(phi), L0 * cos(theta)};
+        for (int c = 0; c < 3; c++) {
+            xx[3 * (2 * i) + c] = d[c] + cx[3 * i + c];
+            xx[3 * (2 * i + 1) + c] = -d[c] + cx[3 * i + c];
+        }
+    }
+    free(cx);
+    return 0;
+}
