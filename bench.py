@@ -297,13 +297,11 @@ def cpu_baseline_sample(s, timeout_s=120.0):
     return el
 
 
-def run_reference(args):
-    """--impl reference: the reference's path on host cores.  The Fortran
-    reference cannot be compiled here (no Fortran compiler), so this times
-    the oracle port of it (FP64, single thread, as the serial reference)."""
-    rank, world, _ = dist_info()
-    if rank != 0:
-        return 0
+def _reference_worker(nsteps, warm, barrier, out):
+    """One copy of the reference's step (the oracle port, one thread): set-up
+    and warm-up, then `nsteps` timed steps started together with the other
+    copies (barrier); puts (timed seconds, peak RSS in bytes) on `out`."""
+    import resource
     s = build_system()
     from oracle import oracle as O
     from simox_b200 import systems as S
@@ -314,8 +312,6 @@ def run_reference(args):
     f, _ = o.pme(f)
     dt = 1.0 / S.TFM
     v = s.v.copy()
-    nsteps = max(1, min(args.steps, 3))
-    warm = 1 if args.warmup > 0 else 0
 
     def step(v, f):
         v = o.vv_nve1(v, f, dt)
@@ -327,20 +323,67 @@ def run_reference(args):
 
     for _ in range(warm):
         v, f = step(v, f)
+    barrier.wait()
     t0 = time.perf_counter()
     for _ in range(nsteps):
         v, f = step(v, f)
     el = time.perf_counter() - t0
-    val = s.n * nsteps / el
+    out.put((el, resource.getrusage(resource.RUSAGE_SELF).ru_maxrss * 1024))
+
+
+def reference_processes(requested=0):
+    """Copies of the serial reference that this host runs side by side: one
+    per core, at most one per 3 GiB of available memory (a 128,000-atom copy
+    peaks near 2.2 GiB), at most 64."""
+    if requested > 0:
+        return requested
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    try:
+        import psutil
+        mem = int(psutil.virtual_memory().available // (3 << 30))
+    except Exception:
+        mem = cores
+    return max(1, min(cores, mem, 64))
+
+
+def run_reference(args):
+    """--impl reference: the reference's path on the host's cores.  The
+    Fortran reference cannot be compiled here (no Fortran compiler), so this
+    times the oracle port of it (FP64, statement by statement).  The reference
+    is serial, so it uses the host's threads the only way it can: one copy of
+    the same 128,000-atom step per core, all started together; the value is
+    the copies' total atom-steps over the slowest copy's time."""
+    import multiprocessing as mp
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return 0
+    from simox_b200 import systems as S
+    n_atoms = build_system().n
+    nsteps = max(1, min(args.steps, 3))
+    warm = 1 if args.warmup > 0 else 0
+    procs = reference_processes(args.ref_procs)
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(procs)
+    out = ctx.Queue()
+    workers = [ctx.Process(target=_reference_worker, args=(nsteps, warm, barrier, out)) for _ in range(procs)]
+    for w in workers:
+        w.start()
+    res = [out.get() for _ in workers]
+    for w in workers:
+        w.join()
+    el = max(r[0] for r in res)
+    val = procs * n_atoms * nsteps / el
     sample = (f"{nsteps} timed step(s) after {warm} warm-up of the full 128,000-atom step "
-              f"(VV_NVE1, CELL_SORT, FORCE, PME, VV_NVT2_BEREND) on 1 host thread; "
-              f"oracle port of the Fortran (no Fortran compiler on this image)")
+              f"(VV_NVE1, CELL_SORT, FORCE, PME, VV_NVT2_BEREND), {procs} copies side by side, one thread "
+              f"each (the reference is serial); oracle port of the Fortran (no Fortran compiler on this image); "
+              f"slowest copy {el / nsteps:.2f} s per step, peak memory "
+              f"{max(r[1] for r in res) / 2 ** 30:.2f} GiB per copy")
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
         "steps": nsteps, "warmup": warm, "ms_per_step": el / nsteps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n_atoms": s.n},
-        "cpu_baseline": {"value": val, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+        "config": {"workload": WORKLOAD, "n_atoms": n_atoms, "copies": procs},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": procs, "kind": "port", "sample": sample},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -467,6 +510,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ref-procs", type=int, default=0,
+                    help="copies of the serial reference run side by side by --impl reference "
+                         "(default: one per core, memory permitting)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the all-FP64 comparison run")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--ncu", action="store_true",
