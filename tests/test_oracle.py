@@ -8,7 +8,10 @@ Fortran compiler), so these published / mathematical facts pin the oracle:
   * EAM: the Al parameter set's fitted lattice constant (4.05 A) and
     equilibrium density rho_e (datafmt.f90:155-157);
   * forces = -grad E by central differences for EAM and Ewald/PME; the
-    same-species CTIP terms are inconsistent as written (force.f90:107-118).
+    same-species CTIP terms are inconsistent as written (force.f90:107-118);
+  * the seeded draws of VINIT and the stochastic thermostat: an independent
+    Python statement of the SplitMix64 construction, bit for bit, and the
+    uniform / polar-method normal moments; VINIT's per-species temperature.
 """
 import numpy as np
 import pytest
