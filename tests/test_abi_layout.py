@@ -55,3 +55,19 @@ def test_struct_layout_matches_header(c_layout, cname, cls):
     assert C.sizeof(cls) == c_layout[(cname, "size")], cname
     for fname, _ in cls._fields_:
         assert getattr(cls, fname).offset == c_layout[(cname, fname)], (cname, fname)
+
+
+@pytest.mark.parametrize("lang", ["c99", "c++11"])
+def test_header_compiles_strict(tmp_path, lang):
+    """include/simox_gpu.h is plain C (and C++) for any caller: no warnings
+    under -std=c99 / -std=c++11 -Wall -Wextra -pedantic."""
+    cc = shutil.which("gcc" if lang == "c99" else "g++")
+    if cc is None:
+        pytest.skip("no compiler")
+    src = tmp_path / "h.c"
+    src.write_text('#include "simox_gpu.h"\nint main(void) { return 0; }\n')
+    cmd = [cc, f"-std={lang}", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.join(ROOT, "include"),
+           "-c", str(src), "-o", str(tmp_path / "h.o")]
+    if lang != "c99":
+        cmd[1:1] = ["-x", "c++"]
+    subprocess.run(cmd, check=True, capture_output=True)
