@@ -444,8 +444,10 @@ def format_status(e: dict, n_atoms: int, step: int, dt: float) -> str:
 
 
 def md_opts(dt: float, thermostat: bool = False, T_given: float = 0.0, freq_new: int = 0, freq_sort: int = 1,
-            reflect: bool = False, freq_stat: int = 0) -> MdOpts:
-    """simox_md_opts for one system (see Simox.md_run)."""
+            reflect: bool = False, freq_stat: int = 0, thermo_stoch: bool = False, alpha: float = 0.0,
+            seed: int = 0) -> MdOpts:
+    """simox_md_opts for one system (see Simox.md_run; batches reject the
+    stochastic thermostat)."""
     o = MdOpts()
     o.dt = float(dt)
     o.thermostat = 1 if thermostat else 0
@@ -456,6 +458,9 @@ def md_opts(dt: float, thermostat: bool = False, T_given: float = 0.0, freq_new:
     o.charge_every_step = 0
     o.accumulate_rdf = 0
     o.freq_stat = int(freq_stat)
+    o.thermo_stoch = 1 if thermo_stoch else 0
+    o.alpha = float(alpha)
+    o.seed = int(seed)
     return o
 
 
