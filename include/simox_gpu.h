@@ -401,7 +401,9 @@ int simox_batch_launch_count(simox_batch* b, long long* n);
  *   link_stride per-cell row length, 1..4,096 (500 in the reference)
  *   stream      cudaStream_t as void* (NULL: the legacy default stream)
  * Returns SIMOX_E_SCRATCH_LIMIT beyond 65,536 cells or a stride above 4,096,
- * SIMOX_E_CELL_OVERFLOW when a cell holds more than link_stride atoms.
+ * SIMOX_E_CELL_OVERFLOW when a cell holds more than link_stride atoms, and
+ * SIMOX_E_CELL_TOO_SMALL for the cell grids simox_create rejects (fewer than
+ * 2 cells on an axis, or fewer than 3 on every axis).
  * The call synchronises the stream.  The first call on a device looks up the
  * scratch array's device address with that device current; make that first
  * call before any stream capture.  All calls share the one scratch array, so

@@ -9,6 +9,7 @@ import numpy as np
 
 MAGIC = b"SIMOXCK1"
 VERSION = 1
+HEADER = 48          # magic 8 + version, n 2 x 4 + step 8 + box 24
 
 
 def write(path: str, ids, x, v, f, q, box, step: int = 0) -> None:
@@ -29,18 +30,18 @@ def write(path: str, ids, x, v, f, q, box, step: int = 0) -> None:
 def read(path: str) -> dict:
     with open(path, "rb") as fh:
         data = fh.read()
-    if len(data) < 40 or data[:8] != MAGIC:
+    if len(data) < HEADER or data[:8] != MAGIC:
         raise ValueError(f"{path}: not a checkpoint")
     version, n = np.frombuffer(data, "<i4", 2, 8)
     if version != VERSION or n < 0:
         raise ValueError(f"{path}: unsupported version {version} or n {n}")
     n = int(n)
-    need = 40 + 4 * n + 8 * 10 * n
+    need = HEADER + 4 * n + 8 * 10 * n
     if len(data) < need:
         raise ValueError(f"{path}: short file ({len(data)} of {need} bytes)")
     step = int(np.frombuffer(data, "<i8", 1, 16)[0])
     box = np.frombuffer(data, "<f8", 3, 24).copy()
-    off = 48
+    off = HEADER
     ids = np.frombuffer(data, "<i4", n, off).copy()
     off += 4 * n
     out = {"n": n, "step": step, "box": box, "ids": ids}

@@ -144,6 +144,7 @@ int md_step(simox_ctx* c, const simox_md_opts* o, bool sort, bool estep, bool wa
 }
 
 void drop_graphs(simox_ctx* c) {
+    c->graph_gen++;   // graphs of a batch that hold this context's launches are stale too
     for (auto& g : c->graphs) {
         if (g.exec) cudaGraphExecDestroy(g.exec);
         g = simox_ctx::StepGraph{};

@@ -29,6 +29,11 @@ struct simox_batch {
         unsigned key = 0;
         cudaGraphExec_t exec = nullptr;
         long long kernels = 0;
+        // what the captured launches baked in: each member's step options
+        // (dt, thermostat, T_given, reflect) and its graph generation (bumped
+        // by tuning changes and new atom sets)
+        std::vector<simox_md_opts> opts;
+        std::vector<unsigned long long> gens;
     };
     G graphs[2];
     long long launches = 0;
@@ -68,11 +73,23 @@ int step_all(simox_batch* b, const simox_md_opts* o, bool sort, bool estep) {
     return sx::cuda_status(cudaGetLastError());
 }
 
+// The options a captured step reads as kernel arguments.
+bool same_step_opts(const simox_md_opts& a, const simox_md_opts& b) {
+    return a.dt == b.dt && a.thermostat == b.thermostat && a.T_given == b.T_given && a.reflect == b.reflect;
+}
+
+bool graph_current(const simox_batch* b, const simox_batch::G& g, const simox_md_opts* o) {
+    if (g.opts.size() != b->ctx.size() || g.gens.size() != b->ctx.size()) return false;
+    for (size_t k = 0; k < b->ctx.size(); k++)
+        if (g.gens[k] != b->ctx[k]->graph_gen || !same_step_opts(g.opts[k], o[k])) return false;
+    return true;
+}
+
 int graph_step(simox_batch* b, const simox_md_opts* o, bool sort, bool estep) {
     const unsigned key = 1u | (sort ? 2u : 0u) | (estep ? 4u : 0u);
     simox_batch::G* hit = nullptr;
     for (auto& g : b->graphs)
-        if (g.exec && g.key == key) hit = &g;
+        if (g.exec && g.key == key && graph_current(b, g, o)) hit = &g;
     if (!hit) {
         long long l0 = 0;
         for (auto* c : b->ctx) l0 += c->launches;
@@ -96,6 +113,9 @@ int graph_step(simox_batch* b, const simox_md_opts* o, bool sort, bool estep) {
         g.key = key;
         g.exec = exec;
         g.kernels = l1 - l0;
+        g.opts.assign(o, o + b->ctx.size());
+        g.gens.clear();
+        for (auto* c : b->ctx) g.gens.push_back(c->graph_gen);
         hit = &g;
     }
     b->launches += hit->kernels;
@@ -107,7 +127,11 @@ int run(simox_batch* b, const simox_md_opts* o, int first, int nsteps) {
         const bool sort = o[0].freq_sort > 0 && step % o[0].freq_sort == 0;
         const bool estep = o[0].freq_stat <= 0 || step % o[0].freq_stat == 0;
         int st;
-        if (!b->primed) {
+        // a member whose skin list must be seeded from the host (new atom set)
+        // cannot be captured: that step runs eagerly, as in simox_md_run
+        bool seed = false;
+        for (auto* c : b->ctx) seed |= c->skin_mode && !c->skin_valid;
+        if (!b->primed || seed) {
             // the first step after set-up seeds each skin list: eager
             long long l0 = 0, l1 = 0;
             for (auto* c : b->ctx) l0 += c->launches;

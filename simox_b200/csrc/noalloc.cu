@@ -104,7 +104,9 @@ extern "C" int simox_cell_sort_noalloc(const double* x_dev, int n, const double*
     for (int d = 0; d < 3; d++) {
         if (!(box[d] > 0.0)) return SIMOX_E_ARG;
         nc[d] = (int)(box[d] / rcut);                  // main.f90:269-270
-        if (nc[d] < 1) return SIMOX_E_CELL_TOO_SMALL;
+        // simox_create's rule: a dimension below 2 cells pairs an atom with
+        // itself at r = 0 in FORCE, so neither entry point accepts it
+        if (nc[d] < 2) return SIMOX_E_CELL_TOO_SMALL;
         lc[d] = box[d] / (double)nc[d];
         hbox[d] = 0.5 * box[d];
     }

@@ -279,6 +279,7 @@ struct simox_ctx {
     StepGraph graphs[4];
     int graph_next = 0;
     bool graphs_on = true;
+    unsigned long long graph_gen = 0;   // bumped whenever captured launches go stale (drop_graphs)
     double eself = 0.0;         // sys%Eself of the last PME_SELF or CTIP_SOLVER
     int last_max_nnb = 0;
     long long last_tot_nnb = 0;

@@ -94,3 +94,35 @@ def test_batch_autotune_picks_a_rule_and_keeps_running():
     finally:
         for g in members:
             g.close()
+
+
+def test_batch_follows_changed_step_options():
+    """A batch whose members' dt and T_given change between md_run calls
+    (an annealing schedule) must step with the new values, as each context's
+    own simox_md_run does -- not replay the graph captured with the old ones."""
+    systems = _members()[:3]
+    plan = [(DT, 1.0), (0.5 * DT, 1.6), (DT, 0.7)]     # (dt, T scale) per md_run call
+    alone = []
+    for s in systems:
+        with _prepared(s, "fp64") as g:
+            step = 1
+            for dt, ts in plan:
+                g.md_run(4, dt, first_step=step, thermostat=True, T_given=ts * s.meta["T"] * S.KB, freq_stat=4)
+                step += 4
+            alone.append(g.get_state()["x"])
+    members = [_prepared(s, "fp64") for s in systems]
+    try:
+        with api.Batch(members) as b:
+            step = 1
+            for dt, ts in plan:
+                opts = [api.md_opts(dt, thermostat=True, T_given=ts * s.meta["T"] * S.KB, freq_stat=4)
+                        for s in systems]
+                b.md_run(opts, 4, first_step=step)
+                step += 4
+        for k, g in enumerate(members):
+            d = g.get_state()["x"] - alone[k]
+            d -= systems[k].box * np.round(d / systems[k].box)
+            assert np.abs(d).max() <= 1e-9, (k, np.abs(d).max())
+    finally:
+        for g in members:
+            g.close()

@@ -60,3 +60,22 @@ def test_checkpoint_file_round_trip(tmp_path):
         fh.write(b"NOTACKPT")
     with pytest.raises(ValueError):
         checkpoint.read(p)
+
+
+@pytest.mark.parametrize("cut", [1, 5, 8, 47])
+def test_checkpoint_truncated_by_a_few_bytes_is_refused(tmp_path, cut):
+    """A file missing its last bytes fails the explicit length check with a
+    clear message, not later inside numpy."""
+    s = S.small_alo(seed=6, n=40)
+    p = os.fspath(tmp_path / "state.ck")
+    checkpoint.write(p, s.ids, s.x, s.x, s.x, s.q, s.box, step=3)
+    with open(p, "rb") as fh:
+        data = fh.read()
+    with open(p, "wb") as fh:
+        fh.write(data[:-cut])
+    with pytest.raises(ValueError, match="short file"):
+        checkpoint.read(p)
+    with open(p, "wb") as fh:          # a bare header shorter than 48 bytes
+        fh.write(data[:44])
+    with pytest.raises(ValueError, match="not a checkpoint"):
+        checkpoint.read(p)

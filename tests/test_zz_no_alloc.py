@@ -62,9 +62,36 @@ def test_noalloc_matches_cell_sort_on_two_calls(simox_lib):
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch(simox_lib):
+    import torch
+    # small real device buffers: if a later change reordered the argument
+    # checks after the launches, a wrong status would show, not a bad address
+    npt = torch.zeros(1, dtype=torch.int32, device="cuda")
+    link = torch.zeros(1, dtype=torch.int32, device="cuda")
+    p_npt, p_link = C.c_void_p(npt.data_ptr()), C.c_void_p(link.data_ptr())
     box = (C.c_double * 3)(1000.0, 1000.0, 1000.0)     # 100^3 cells > 65,536
-    st = simox_lib.simox_cell_sort_noalloc(None, 0, box, 10.0, C.c_void_p(1), C.c_void_p(1), 500, None)
+    st = simox_lib.simox_cell_sort_noalloc(None, 0, box, 10.0, p_npt, p_link, 500, None)
     assert st == _abi.SIMOX_E_SCRATCH_LIMIT
     box = (C.c_double * 3)(40.0, 40.0, 40.0)
-    st = simox_lib.simox_cell_sort_noalloc(None, 0, box, 10.0, C.c_void_p(1), C.c_void_p(1), 5000, None)
+    st = simox_lib.simox_cell_sort_noalloc(None, 0, box, 10.0, p_npt, p_link, 5000, None)
     assert st == _abi.SIMOX_E_SCRATCH_LIMIT
+    torch.cuda.synchronize()
+    assert int(npt.item()) == 0 and int(link.item()) == 0
+
+
+def test_noalloc_grid_rule_agrees_with_create(simox_lib):
+    """Both entry points reject a cell grid with one cell on an axis."""
+    import torch
+    from simox_b200 import api
+    s = S.small_alo(seed=8, n=200, box=(41.0, 31.5, 52.0), fft=(16, 16, 16))
+    s.box = np.array([41.0, 31.5, 15.0])                      # 4 x 3 x 1 cells
+    s.x[:, 2] = np.clip(s.x[:, 2], -7.4, 7.4)
+    with pytest.raises(api.SimoxError) as ei:
+        api.from_system(s)
+    assert ei.value.code == _abi.SIMOX_E_CELL_TOO_SMALL
+    npt = torch.zeros(12, dtype=torch.int32, device="cuda")
+    link = torch.zeros((12, 500), dtype=torch.int32, device="cuda")
+    x = torch.from_numpy(np.ascontiguousarray(s.x)).cuda()
+    box = (C.c_double * 3)(*[float(b) for b in s.box])
+    st = simox_lib.simox_cell_sort_noalloc(C.c_void_p(x.data_ptr()), s.n, box, float(s.rcut),
+                                           C.c_void_p(npt.data_ptr()), C.c_void_p(link.data_ptr()), 500, None)
+    assert st == _abi.SIMOX_E_CELL_TOO_SMALL
