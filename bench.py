@@ -131,45 +131,39 @@ def measured_peaks():
         return 6650.0, "of fallback"
 
 
-def profile_traffic(kernel):
-    """DRAM bytes per launch of ``kernel`` from the committed ncu summary."""
+def profile_figure(kernel, key):
+    """A figure recorded in the committed ncu summary of ``kernel``
+    (profiles/<kernel>_corundum128k.md, a line "key: value")."""
     path = os.path.join(ROOT, "profiles", f"{kernel}_corundum128k.md")
     try:
         for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
+            if line.startswith(key + ":"):
                 return float(line.split(":")[1])
-    except OSError:
+    except (OSError, ValueError):
         pass
     return None
 
 
-# Algorithmic bytes per launch of each kernel family (unique bytes a launch
-# must move: per-atom state in and out plus its neighbour-list row).  n atoms,
-# nnb mean neighbours, K grid points, p spline order.  The skin list's mean
-# row length is taken as nnb ((Rcut + skin) / Rcut)^3 (uniform density).
-SKIN = 1.0
-
-
-def algorithmic_bytes(name, n, nnb, K, prec, rcut=10.0):
-    r = 8 if prec == "fp64" else 4
-    nnb_s = nnb * ((rcut + SKIN) / rcut) ** 3
-    if name == "neighbor_filter_density":
-        # xq 32, type 4, cell 4, index 4, skin count 8, skin row 4*nnb_s in;
-        # exact row 4*nnb, count 8, rho 8, F' 8 + 4 out
-        return n * (32 + 4 + 4 + 4 + 8 + 4 * nnb_s + 4 * nnb + 8 + 8 + 12)
-    if name == "pair_force":      # xq 32, type 4, count 4, F' 8, list 4*nnb in; force 24 out
-        return n * (32 + 4 + 4 + 8 + 4 * nnb + 24)
-    if name == "eam_density":     # xq 32, type 4, count 4, list 4*nnb in; rho, F' 16 out
-        return n * (32 + 4 + 4 + 4 * nnb + 16)
-    if name == "neighbor_list":   # positions 32 in, list 4*nnb + count 4 out
-        return n * (32 + 4 * nnb + 4)
-    if name == "pme_spread":      # xq 32 in, grid K r out
-        return n * 32 + K * r
-    if name == "pme_gather_force":
-        return n * (32 + 4 + 48) + K * r
-    if name in ("pme_fft_r2c", "pme_fft_c2r"):
-        return 2 * K * r * 2
-    return None
+# Algorithmic bytes per atom-step of each kernel family: the path's cost model
+# (FP64 sizes, the mixed path's FP32 grids halved; K grid points amortised over
+# the N atoms).  integrate-1 124 B, integrate-2 72 B (+ 48 B for the Berendsen
+# rescale's second sweep over v), cell binning 104 B in all, EAM pass 1 44 B,
+# pair/force pass 2 68 B, spread 32 B + K grid values, FFT R2C + C2R two
+# read+write sweeps of the real and the half-complex grid each, influence
+# multiply 40 B per half-spectrum point (20 B in FP32), gather 56 B + K grid
+# values.  The skin-list upkeep, the gather into pair order and the exact-list
+# rows are this implementation's own traffic, not algorithmic.
+def algorithmic_bytes(name, n, K, prec):
+    g = 8 if prec == "fp64" else 4          # bytes per real grid value
+    table = {
+        "vv_nve1": 124 * n, "vv_nvt2_kick": 72 * n, "vv_nvt2_scale": 48 * n,
+        "cell_bin": 104 * n,                  # the whole binning (bin, scan, scatter, order)
+        "neighbor_filter_density": 44 * n, "pair_force": 68 * n,
+        "pme_spread": 32 * n + g * K, "pme_gather_force": 56 * n + g * K,
+        "pme_fft_r2c": 4 * g * K, "pme_fft_c2r": 4 * g * K,
+        "pme_influence": 5 * g * (K // 2),
+    }
+    return table.get(name)
 
 
 # --------------------------------------------------------------------------
@@ -193,21 +187,34 @@ def equilibrated_context(s, precision, device=0):
 def force_error(s, device=0):
     """Mixed-precision FORCE + PME forces against the all-FP64 path on the
     same input: ||F_mixed - F_fp64|| / ||F_fp64|| over all components, and
-    the largest per-atom |dF| relative to the RMS atom force."""
+    the largest per-atom |dF| relative to the RMS atom force; the same two
+    figures for FORCE alone and PME alone (each relative to the total force's
+    RMS), which locate the error."""
     from simox_b200 import api
-    out = {}
+    out, pair, rec = {}, {}, {}
     for prec in ("fp64", "mixed"):
         with api.from_system(s, precision=prec, device=device) as g:
             g.pme_self()
             g.cell_sort()
             g.force(energies=False)
+            pair[prec] = g.get_state()["f"]
             g.pme(energies=False)
             out[prec] = g.get_state()["f"]
-    d = out["mixed"] - out["fp64"]
+            g.set_state(f=np.zeros((s.n, 3)))
+            g.pme(energies=False)
+            rec[prec] = g.get_state()["f"]
     nrm = np.linalg.norm(out["fp64"])
     frms = nrm / np.sqrt(s.n)
-    return {"rel_norm": float(np.linalg.norm(d) / nrm),
-            "max_atom_rel_rms": float(np.linalg.norm(d, axis=1).max() / frms)}
+
+    def fig(a):
+        d = a["mixed"] - a["fp64"]
+        return {"rel_norm": float(np.linalg.norm(d) / nrm),
+                "max_atom_rel_rms": float(np.linalg.norm(d, axis=1).max() / frms)}
+
+    res = fig(out)
+    res["force_only"] = fig(pair)
+    res["pme_only"] = fig(rec)
+    return res
 
 
 def run_md(g, s, first, nsteps, rdf):
@@ -390,17 +397,15 @@ def run_reference(args):
     return 0
 
 
-def run_batch(args):
-    """--batch: the batched-replica workload (256 independent Al/O systems,
-    500-8000 atoms each, O fraction 0-0.6, 300-1200 K, own box and PME grid
-    32^3-64^3, order 6), mixed precision, NVT Berendsen at each system's
+def batch_object(nsys, steps, sequential=True):
+    """The batched-replica workload (independent Al/O systems of 500-8000
+    atoms, O fraction 0-0.6, 300-1200 K, own box and PME grid 32^3-64^3,
+    order 6; seed 7), mixed precision, NVT Berendsen at each system's
     temperature, energies every 10th step.  All systems advance together (one
-    CUDA graph launch per step); the force pass's CTA split is autotuned on
-    the batch first.  Reported beside the same systems stepped one after
-    another.  Not the headline metric."""
-    from simox_b200 import api, build, systems as S
-    build.build()
-    systems = S.replica_batch(seed=7, nsys=args.batch)
+    CUDA graph launch per step) after the force pass's CTA split is autotuned
+    on the batch.  Reported beside the same systems stepped one after another."""
+    from simox_b200 import api, systems as S
+    systems = S.replica_batch(seed=7, nsys=nsys)
     natoms = sum(s.n for s in systems)
     dt = 1.0 / S.TFM
     members = []
@@ -418,48 +423,62 @@ def run_batch(args):
     step = 3 + 5 * 6
     b.md_run(opts, 20, first_step=step)          # both step graphs captured again
     step += 20
-    n = max(args.steps, 20)
+    n = max(steps, 20)
+    l0 = b.launch_count()
     t0 = time.perf_counter()
     b.md_run(opts, n, first_step=step)
     el = time.perf_counter() - t0
+    launches = (b.launch_count() - l0) / n
     step += n
-    t1 = time.perf_counter()
-    for k, g in enumerate(members):
-        g.md_run(10, dt, first_step=step, thermostat=True, T_given=systems[k].meta["T"] * S.KB, freq_stat=10)
-        g.sync()
-    el_seq = time.perf_counter() - t1
-    line = {"metric": "atom-steps/s, batched independent Al/O systems", "value": natoms * n / el,
-            "unit": UNIT, "n_gpus": 1, "steps": n, "ms_per_step": el / n * 1e3, "higher_is_better": True,
-            "dtype": "f32+f64", "data": "synthetic",
-            "config": {"workload": f"{args.batch} systems of 500-8000 atoms (seed 7), {natoms} atoms in total",
-                       "precision": "mixed", "energies": "every 10th step",
-                       "timing": "wall clock around one batch md_run call (ends with a device sync)"},
-            "autotune_ms_per_step": [round(t, 3) for t in times], "autotune_best_rule": int(best),
-            "sequential": {"value": natoms * 10 / el_seq, "unit": UNIT, "ms_per_step": el_seq / 10 * 1e3,
-                           "how": "each system's own md_run (its step graphs), one after another"},
-            "gpu_launches_per_step": b.launch_count()}
+    out = {"metric": "atom-steps/s, batched independent Al/O systems", "value": natoms * n / el,
+           "unit": UNIT, "steps": n, "ms_per_step": el / n * 1e3,
+           "workload": f"{nsys} systems of 500-8000 atoms (seed 7), {natoms} atoms in total, mixed precision, "
+                       f"energies every 10th step",
+           "timing": "wall clock around one batch md_run call (ends with a device sync)",
+           "autotune_ms_per_step": [round(t, 3) for t in times], "autotune_best_rule": int(best),
+           "gpu_launches_per_step": launches}
+    if sequential:
+        t1 = time.perf_counter()
+        for k, g in enumerate(members):
+            g.md_run(10, dt, first_step=step, thermostat=True, T_given=systems[k].meta["T"] * S.KB, freq_stat=10)
+            g.sync()
+        el_seq = time.perf_counter() - t1
+        out["sequential"] = {"value": natoms * 10 / el_seq, "unit": UNIT, "ms_per_step": el_seq / 10 * 1e3,
+                             "how": "each system's own md_run (its step graphs), one after another"}
     b.close()
     for g in members:
         g.close()
+    return out
+
+
+def run_batch(args):
+    """--batch N: the batched-replica workload alone (256 systems in its
+    configuration).  Not the headline metric."""
+    from simox_b200 import build
+    build.build()
+    o = batch_object(args.batch, args.steps)
+    line = {"metric": o.pop("metric"), "value": o.pop("value"), "unit": UNIT, "n_gpus": 1,
+            "steps": o.pop("steps"), "higher_is_better": True, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": o.pop("workload"), "timing": o.pop("timing")}}
+    line.update(o)
     print(json.dumps(line), flush=True)
     return 0
 
 
-def run_adjoint(args):
-    """--adjoint: the parameter-gradient workload -- seeded snapshots of
-    2000-atom Al/O systems (O fraction 0.1-0.5, 300-1000 K), synthetic
-    targets = the FP64 model forces plus Gaussian noise (0.05 eV/A); per
-    snapshot the charges, forces and the gradients of the energy and of the
-    force-matching loss with respect to 3 x 64 spline coefficients and chi, J,
-    Z (FP64, one adjoint CG through the charge solve).  Reports snapshots/s
-    and the summed loss gradient's size.  Not the headline metric."""
-    from simox_b200 import api, build, spline, systems as S
-    build.build()
+def adjoint_object(nsnap, sequential=True):
+    """The parameter-gradient workload: seeded snapshots of 2000-atom Al/O
+    systems (O fraction 0.1-0.5, 300-1000 K), synthetic targets = the FP64
+    model forces plus Gaussian noise (0.05 eV/A); per snapshot the charges,
+    forces and the gradients of the energy and of the force-matching loss with
+    respect to 3 x 64 spline coefficients and chi, J, Z, xi (FP64, one adjoint
+    CG through the charge solve), all snapshots at once through
+    simox_adjoint_eval_many."""
+    from simox_b200 import api, spline, systems as S
     rng = np.random.default_rng(11)
     P = api.default_potential()
     spl = spline.fit(P)
     ctxs, targets = [], []
-    for k in range(args.adjoint):
+    for k in range(nsnap):
         s = S.replica(int(rng.integers(1 << 30)), 2000, float(rng.uniform(0.1, 0.5)), float(rng.uniform(300, 1000)))
         g = api.from_system(s, precision="fp64")
         g.pme_self()
@@ -468,40 +487,111 @@ def run_adjoint(args):
         _, f0, _, _ = g.adjoint_eval(gradients=False)
         targets.append(f0 + rng.normal(0.0, 0.05, f0.shape))
         ctxs.append(g)
-    for g, t in zip(ctxs, targets):      # warm-up: charges converged at these parameters
-        g.adjoint_eval(t)
-    # one snapshot after another through simox_adjoint_eval
-    t0 = time.perf_counter()
-    seq = [g.adjoint_eval(t) for g, t in zip(ctxs, targets)]
-    el_seq = time.perf_counter() - t0
-    # all snapshots at once through simox_adjoint_eval_many (host threads, a stream each)
-    api.adjoint_eval_many(ctxs, targets)   # warm-up of the threaded path
+    api.adjoint_eval_many(ctxs, targets)   # warm-up: charges converged at these parameters, threads started
+    seq = None
+    if sequential:
+        t0 = time.perf_counter()
+        seq = [g.adjoint_eval(t) for g, t in zip(ctxs, targets)]
+        el_seq = time.perf_counter() - t0
     t0 = time.perf_counter()
     out = api.adjoint_eval_many(ctxs, targets)
     el = time.perf_counter() - t0
     reps = [o[0] for o in out]
     gE = np.sum([o[2] for o in out], axis=0)
     gL = np.sum([o[3] for o in out], axis=0)
-    gL_seq = np.sum([o[3] for o in seq], axis=0)
-    line = {"metric": "parameter-gradient snapshots/s (2000-atom Al/O, FP64 adjoint)", "value": len(ctxs) / el,
-            "unit": "snapshots/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{len(ctxs)} seeded snapshots of 2000 atoms, targets = model forces + N(0, 0.05)",
-                       "parameters": "3 x 64 spline coefficients + chi, J, Z, xi of 5 species (212)",
-                       "api": "simox_adjoint_eval_many (all snapshots concurrently, one host thread and "
-                              "stream per snapshot, up to 16 threads)"},
-            "ms_per_snapshot": el / len(ctxs) * 1e3,
-            "sequential": {"value": len(ctxs) / el_seq, "unit": "snapshots/s",
-                           "api": "simox_adjoint_eval, one snapshot after another"},
-            "grad_L_rel_diff_concurrent_vs_sequential": float(np.linalg.norm(gL - gL_seq) / np.linalg.norm(gL_seq)),
-            "mean_adjoint_cg_iterations": float(np.mean([r["n_adjoint"] for r in reps])),
-            "mean_newton_steps": float(np.mean([r["n_newton"] for r in reps])),
-            "max_charge_residual": float(max(r["residual"] for r in reps)),
-            "loss_total": float(sum(r["loss"] for r in reps)),
-            "grad_L_norm": float(np.linalg.norm(gL)), "grad_E_norm": float(np.linalg.norm(gE))}
+    res = {"metric": "parameter-gradient snapshots/s (2000-atom Al/O, FP64 adjoint)", "value": len(ctxs) / el,
+           "unit": "snapshots/s",
+           "workload": f"{len(ctxs)} seeded snapshots of 2000 atoms, targets = model forces + N(0, 0.05)",
+           "parameters": "3 x 64 spline coefficients + chi, J, Z, xi of 5 species (212)",
+           "api": "simox_adjoint_eval_many (all snapshots concurrently, one host thread and stream per "
+                  "snapshot, up to 16 threads)",
+           "ms_per_snapshot": el / len(ctxs) * 1e3,
+           "mean_adjoint_cg_iterations": float(np.mean([r["n_adjoint"] for r in reps])),
+           "mean_newton_steps": float(np.mean([r["n_newton"] for r in reps])),
+           "max_charge_residual": float(max(r["residual"] for r in reps)),
+           "loss_total": float(sum(r["loss"] for r in reps)),
+           "grad_L_norm": float(np.linalg.norm(gL)), "grad_E_norm": float(np.linalg.norm(gE))}
+    if seq is not None:
+        gL_seq = np.sum([o[3] for o in seq], axis=0)
+        res["sequential"] = {"value": len(ctxs) / el_seq, "unit": "snapshots/s",
+                             "api": "simox_adjoint_eval, one snapshot after another"}
+        res["grad_L_rel_diff_concurrent_vs_sequential"] = float(np.linalg.norm(gL - gL_seq) / np.linalg.norm(gL_seq))
     for g in ctxs:
         g.close()
+    return res
+
+
+def run_adjoint(args):
+    """--adjoint N: the parameter-gradient workload alone (32 snapshots in its
+    configuration).  Not the headline metric."""
+    from simox_b200 import build
+    build.build()
+    o = adjoint_object(args.adjoint)
+    line = {"metric": o.pop("metric"), "value": o.pop("value"), "unit": o.pop("unit"), "n_gpus": 1,
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": o.pop("workload"), "parameters": o.pop("parameters"), "api": o.pop("api")}}
+    line.update(o)
     print(json.dumps(line), flush=True)
     return 0
+
+
+def ctip_object(g, label):
+    """One CTIP_SOLVER re-solve at the context's current positions (charges
+    from the last solve), timed with CUDA events on the context's stream:
+    CG iterations, line evaluations, ms per solve and per CG iteration; then
+    the per-kernel split from up to 20 host-driven iterations from the same
+    starting charges with every launch bracketed by events."""
+    q0 = g.get_state()["q"]
+    g.sync()
+    g.timer_begin()
+    _, rep = g.ctip_solver()
+    ms = g.timer_end()
+    q1 = g.get_state()["q"]
+    out = {"precision": label, "n_cg": rep["n_cg"], "n_line": rep["n_line"], "ms_per_solve": ms,
+           "ms_per_cg_iteration": ms / max(rep["n_cg"], 1), "final_error": rep["error"],
+           "total_charge_change_e": float(abs(q1.sum() - q0.sum()))}
+    g.set_state(q=q0)
+    g.profile(True)
+    g.profile_reset()
+    _, rep2 = g.ctip_solver(max_cg=20)
+    prof = g.profile_read()
+    g.profile(False)
+    it = max(rep2["n_cg"], 1)
+    out["kernels_ms_per_cg_iteration"] = {k: round(v[0] / it, 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
+    out["kernels_note"] = f"host-driven loop, {it} iterations, event span per launch family"
+    g.set_state(q=q1)
+    return out
+
+
+def c3_object(steps=2, device=0):
+    """The oxidation slab (fcc Al 60x60x30 = 432,000 atoms plus 40,000 O at
+    0.02 A^-3 above, PME 256x256x384, order 6), mixed precision, NVE at
+    dt = 0.5 fs with CTIP_SOLVER on every step (the driver flag): one charge
+    solve from zero charges first (untimed), then `steps` timed loop steps,
+    each VV_NVE1, CELL_SORT, CTIP_SOLVER, FORCE, PME, VV_NVE2."""
+    from simox_b200 import api, systems as S
+    s = S.oxidation_slab()
+    g = api.from_system(s, precision="mixed", device=device)
+    g.pme_self()
+    g.cell_sort()
+    t0 = time.perf_counter()
+    _, rep0 = g.ctip_solver()
+    first_s = time.perf_counter() - t0
+    g.force(energies=False)
+    g.pme(energies=False)
+    q0 = g.get_state()["q"].sum()
+    g.sync()
+    g.timer_begin()
+    e = g.md_run(steps, 0.5 / S.TFM, first_step=2, thermostat=False, freq_new=1000, charge_every_step=True,
+                 freq_stat=1)
+    ms = g.timer_end()
+    q = g.get_state()["q"]
+    g.close()
+    return {"metric": "atom-steps/s, oxidation slab with CTIP_SOLVER every step", "value": s.n * steps / (ms / 1e3),
+            "unit": UNIT, "n_atoms": s.n, "steps": steps, "ms_per_step": ms / steps,
+            "first_solve": {"n_cg": rep0["n_cg"], "seconds": first_s, "from": "zero charges"},
+            "total_charge_change_e": float(abs(q.sum() - q0)),
+            "energies_last_step": e}
 
 
 def main():
@@ -525,6 +615,11 @@ def main():
                     help="run the batched-replica workload with this many systems (256 in its configuration)")
     ap.add_argument("--adjoint", type=int, default=0,
                     help="run the parameter-gradient workload with this many snapshots (32 in its configuration)")
+    ap.add_argument("--no-ctip", action="store_true", help="skip the timed CTIP re-solves")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the 32-system batch and 32-snapshot adjoint objects of the default line")
+    ap.add_argument("--c3", action="store_true",
+                    help="add the 472k oxidation slab with the charge solve on every step")
     args = ap.parse_args()
     if args.adjoint:
         return run_adjoint(args)
@@ -564,6 +659,7 @@ def main():
     value = world * s.n * args.steps / (ms_max / 1e3)
     mx_nnb, tot_nnb = g.neighbor_stats()
     nnb = tot_nnb / s.n
+    half = g.get_tuning().get("half_list", 0) == 1
 
     # e2e through the C ABI with host buffers
     e2e_s, nbytes = time_e2e(g, s, max(3, args.steps // 2), args.warmup + args.steps + 1)
@@ -571,22 +667,57 @@ def main():
     e2e_val = world * s.n * max(3, args.steps // 2) / e2e_s
 
     # per-kernel profile (separate pass; event-bracketed launches)
-    prof = profile_steps(g, s, min(args.steps, 5), args.warmup + args.steps + 100)
+    nprof = min(args.steps, 5)
+    prof = profile_steps(g, s, nprof, args.warmup + args.steps + 100)
+    ctip_mixed = ctip_object(g, "mixed") if not args.no_ctip else None
     g.close()
-    dom = max((k for k in prof if algorithmic_bytes(k, 1, 1, 1, "mixed") is not None),
-              key=lambda k: prof[k][0])
     K = int(np.prod(s.fft))
-    dom_ms = prof[dom][0] / max(prof[dom][1], 1)
-    dom_bytes = algorithmic_bytes(dom, s.n, nnb, K, "mixed", s.rcut)
+    fam = {k: [v[0] / nprof, v[1] / nprof] for k, v in prof.items()}
+    cell = [k for k in fam if k in ("cell_bin", "cell_scan", "cell_scatter", "cell_order")]
+    if cell:   # the binning's cost model covers its four kernels together
+        fam["cell_bin"] = [sum(fam[k][0] for k in cell), 1.0]
+        for k in cell:
+            if k != "cell_bin":
+                fam.pop(k)
     peak, peak_kind = measured_peaks()
+    per_kernel = {}
+    for k, (ms_k, nl) in fam.items():
+        by = algorithmic_bytes(k, s.n, K, "mixed")
+        if by is None or ms_k <= 0:
+            continue
+        per_launch = ms_k / max(nl, 1)
+        gbs = by / (per_launch / 1e3) / 1e9
+        per_kernel[k] = {"ms_per_step": round(ms_k, 4), "algorithmic_mb_per_launch": round(by / 1e6, 2),
+                         "achieved_gbs": round(gbs, 1), "frac": round(gbs / peak, 4)}
+    dom = max(per_kernel, key=lambda k: per_kernel[k]["ms_per_step"])
+    dom_ms = fam[dom][0] / max(fam[dom][1], 1)
+    dom_bytes = algorithmic_bytes(dom, s.n, K, "mixed")
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
-    traffic = profile_traffic(dom)
+    traffic = profile_figure(dom, "traffic_bytes_per_launch")
+    step_bytes = sum(algorithmic_bytes(k, s.n, K, "mixed") or 0 for k in
+                     ("vv_nve1", "vv_nvt2_kick", "vv_nvt2_scale", "cell_bin", "neighbor_filter_density",
+                      "pair_force", "pme_spread", "pme_gather_force", "pme_fft_r2c", "pme_fft_c2r", "pme_influence"))
+    # the pair passes are bound by instruction issue and the SFU, not by
+    # memory: their rate in pair evaluations per second beside the issue
+    # utilisation ncu measured
+    evals = tot_nnb * (0.5 if half else 1.0)
+    pair_rate = {}
+    for k in ("neighbor_filter_density", "pair_force"):
+        if k in fam:
+            t = fam[k][0] / max(fam[k][1], 1)
+            pair_rate[k] = {"pairs_per_launch": int(tot_nnb // 2), "evaluations_per_launch": int(evals),
+                            "pair_evaluations_per_s": evals / (t / 1e3), "ms_per_launch": round(t, 4),
+                            "issue_active_pct_ncu": profile_figure(k, "issue_active_pct"),
+                            "sfu_pipe_pct_ncu": profile_figure(k, "xu_pipe_pct")}
 
     # all-FP64 path, same input
     fp64 = None
+    ctip_fp64 = None
     if not args.no_fp64:
         g64 = equilibrated_context(s, "fp64", device=local)
         ms64, _, _, _ = time_device(g64, s, args.steps, args.warmup, dist, device)
+        if not args.no_ctip:
+            ctip_fp64 = ctip_object(g64, "fp64")
         g64.close()
         ms64 = reduce_max(dist, ms64, device)
         fp64 = {"value": world * s.n * args.steps / (ms64 / 1e3), "unit": UNIT, "ms_per_step": ms64 / args.steps}
@@ -600,6 +731,13 @@ def main():
                "sample": "one full 128,000-atom step (VV_NVE1, CELL_SORT, FORCE, PME, VV_NVT2_BEREND) "
                          "of the oracle port on 1 host thread"}
 
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        extras["batch"] = batch_object(32, 20, sequential=True)
+        extras["adjoint"] = adjoint_object(32, sequential=False)
+        if args.c3:
+            extras["slab_charges_every_step"] = c3_object(steps=2, device=local)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -608,7 +746,7 @@ def main():
             "config": {"workload": WORKLOAD, "n_atoms": s.n, "per_rank_replicas": 1,
                        "parallelism": "replicas" if world > 1 else "single",
                        "precision": "mixed: FP32 pair/PME terms, FP64 sums, energies, CG",
-                       "charges": "CTIP at step 1 (warm-up), freq_new > run length",
+                       "charges": "CTIP at step 1 (warm-up), freq_new > run length; re-solve timed separately (ctip)",
                        "energies": "FP64 energies on every 10th step (status rule) and the last; RDF every step",
                        "l2": "inputs larger than L2 (neighbour list %.0f MB rebuilt every step)" % (tot_nnb * 4 / 1e6),
                        "mean_neighbours": round(nnb, 1), "max_neighbours": mx_nnb},
@@ -619,16 +757,25 @@ def main():
             "gpu_launches": launches,
             "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
-                         "avg_launch_ms": dom_ms, "algorithmic_bytes_per_launch": dom_bytes},
+                         "traffic_over_algorithmic": (traffic / dom_bytes) if traffic else None,
+                         "avg_launch_ms": dom_ms, "algorithmic_bytes_per_launch": dom_bytes,
+                         "bytes_model": "per-atom cost model of the path (EAM pass 1 44 B, pair pass 2 68 B, ...)"},
+            "step_roofline": {"algorithmic_mb_per_step": round(step_bytes / 1e6, 1),
+                              "achieved_gbs": step_bytes / (ms_max / args.steps / 1e3) / 1e9,
+                              "frac": step_bytes / (ms_max / args.steps / 1e3) / 1e9 / peak},
+            "kernel_roofline": per_kernel,
+            "pair_rate": pair_rate,
             "kernels_note": "event spans per launch family from a separate eager pass with PME on the main "
                             "stream (the timed steps run it on a side stream, overlapped with the pair passes)",
-            "kernels_ms_per_step": {k: round(v[0] / max(min(args.steps, 5), 1), 4) for k, v in
+            "kernels_ms_per_step": {k: round(v[0] / max(nprof, 1), 4) for k, v in
                                     sorted(prof.items(), key=lambda kv: -kv[1][0])},
+            "ctip": {"mixed": ctip_mixed, "fp64": ctip_fp64},
             "cpu_baseline": cpu,
             "clocks": clk,
             "energies_last_step": e,
             "warmup_seconds": warm_s,
         }
+        line.update(extras)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
