@@ -151,6 +151,18 @@ typedef struct {
     unsigned long long seed;  /* seed of its random forces (see simox_vinit)      */
 } simox_md_opts;
 
+/* Oxidation-mode charge events (main.f90:63-84, Nset%N_o2, z_new, q_crit of
+ * config.prm lines 19-21): on every charge step REMOVE_RIGID_MOTION,
+ * OXIDE_CHECK and, when it is due, NEW_O2 run between CELL_SORT and
+ * CTIP_SOLVER.  The reference draws the new dimers from RANDOM_NUMBER; here
+ * from the seeded generator of simox_vinit, stream (1 << 63 | step). */
+typedef struct {
+    int    n_o2;         /* O2 dimers per insertion (Nset%N_o2); 2 n_o2 atoms     */
+    double z_new;        /* height of the new dimers' centres (Nset%z_new), A     */
+    double q_crit;       /* OXIDE_CHECK charge threshold (Nset%q_crit), e         */
+    unsigned long long seed;  /* seed of the dimer positions                      */
+} simox_oxidation;
+
 typedef struct simox_ctx simox_ctx;
 
 /* ---- parameter tables --------------------------------------------------- */
@@ -351,7 +363,10 @@ int simox_adjoint_eval_many(simox_ctx* const* ctxs, int m, const double* const* 
  * depend on it: every atom's force is summed by one warp in the same order
  * whatever the CTA split. */
 typedef struct {
-    int force_splits;    /* CTAs per skin cell in the mixed force pass, 1..16 (default 2) */
+    int force_splits;    /* CTAs per skin cell in the mixed pair passes, 1..16 (default 2) */
+    int half_list;       /* get only: 1 when the current pair order keeps each pair once (mixed
+                            precision, skin list, one metal species plus oxygen); the neighbour
+                            statistics then count pairs, not list entries of both atoms      */
 } simox_tuning;
 int simox_set_tuning(simox_ctx* ctx, const simox_tuning* t);
 int simox_get_tuning(simox_ctx* ctx, simox_tuning* t);
@@ -383,6 +398,38 @@ int simox_batch_autotune(simox_batch* b, const simox_md_opts* opts, int first_st
                          double* times_ms, int* best);
 /* Kernels launched by the batch (graph kernel nodes counted per replay). */
 int simox_batch_launch_count(simox_batch* b, long long* n);
+
+/* ---- oxidation mode (main.f90:63-84), device-resident ------------------
+ * The atom arrays hold the context's capacity, so NEW_O2 appends in place
+ * (the reference reallocates, ADD_PTCL datafmt.f90:84-95); an insertion
+ * beyond the capacity returns SIMOX_E_CAPACITY.  The only host transfer of a
+ * charge event is OXIDE_CHECK's flag. */
+/* REMOVE_RIGID_MOTION vverlet.f90:211-234: v -= mean v, z -= mean z (unit
+ * masses); FP64 block sums in a fixed order. */
+int simox_remove_rigid_motion(simox_ctx* ctx);
+/* OXIDE_CHECK util.f90:152-188: *due = 1 when the highest Al atom lies above
+ * the highest O atom among the last 2 n_o2 atoms (heights floored at 0) or the
+ * largest charge of those O atoms is below q_crit (floored at -10). */
+int simox_oxide_check(simox_ctx* ctx, int n_o2, double q_crit, int* due);
+/* NEW_O2 datafmt.f90:98-139 with RANDOM_POSITION_O2 util.f90:104-148:
+ * appends n_o2 O2 dimers (2 n_o2 atoms of species 4) with centres at height
+ * z_new at least sqrt(Lx Ly / n_o2)/2 apart in (x, y), bond 2 A, the y offset
+ * as written (equal to the x offset, util.f90:138), v = (0, 0,
+ * -sqrt(3 T_given / 16)), f = 0, q = 0.  Draws: stream (1 << 63 | event).
+ * SIMOX_E_ARG for "=== Too many new oxygens ===" or no room after 100,000
+ * tries; SIMOX_E_CAPACITY beyond the context's capacity.  The new atom set
+ * needs simox_cell_sort before FORCE (the reference keeps the new atoms out
+ * of its cell lists until its next CELL_SORT). */
+int simox_new_o2(simox_ctx* ctx, int n_o2, double z_new, double T_given, unsigned long long seed,
+                 unsigned long long event);
+/* The oxidation-mode loop main.f90:63-84 (opts->reflect = 1 for
+ * VV_NVE1_REFLECT): on each charge step (TAG_SET's freq_new rule, or every
+ * step with charge_every_step) REMOVE_RIGID_MOTION, OXIDE_CHECK, NEW_O2 when
+ * due (event = step), a CELL_SORT of the moved and new atoms, CTIP_SOLVER;
+ * then FORCE, PME and VV_NVE2 / VV_NVT2_BEREND.  *n_inserted (may be NULL)
+ * receives the atoms added; simox_get_natoms gives the new count. */
+int simox_md_run_oxidation(simox_ctx* ctx, const simox_md_opts* opts, const simox_oxidation* ox,
+                           int first_step, int nsteps, simox_energies* last, int* rdf, int* n_inserted);
 
 /* ---- allocation-free cell binning ---------------------------------------
  * No counterpart in the reference.  For callers that cannot let a library

@@ -119,6 +119,11 @@ class MdOpts(C.Structure):
                 ("thermo_stoch", C.c_int), ("alpha", C.c_double), ("seed", C.c_ulonglong)]
 
 
+class Oxidation(C.Structure):
+    """simox_oxidation: the oxidation loop's insertion settings."""
+    _fields_ = [("n_o2", C.c_int), ("z_new", C.c_double), ("q_crit", C.c_double), ("seed", C.c_ulonglong)]
+
+
 def potential_to_bytes(p: Potential) -> bytes:
     return bytes(C.string_at(C.addressof(p), C.sizeof(p)))
 
@@ -140,12 +145,14 @@ EXPORTED = [
     "simox_batch_launch_count",
     "simox_set_eam_spline", "simox_set_ctip_params", "simox_set_ctip_xi", "simox_adjoint_eval",
     "simox_adjoint_eval_many",
+    "simox_remove_rigid_motion", "simox_oxide_check", "simox_new_o2", "simox_md_run_oxidation",
 ]
 
 
 class Tuning(C.Structure):
-    """simox_tuning: launch-shape choices (results do not depend on them)."""
-    _fields_ = [("force_splits", C.c_int)]
+    """simox_tuning: launch-shape choices (results do not depend on them),
+    and whether the current pair order keeps each pair once (get only)."""
+    _fields_ = [("force_splits", C.c_int), ("half_list", C.c_int)]
 
 
 SPLINE_N = 64

@@ -19,8 +19,8 @@ import os
 import numpy as np
 
 from . import _abi
-from ._abi import (AdjointReport, CtipReport, EamSpline, Energies, MdOpts, NGRAD, Potential, Setup, SIMOX_FP64,
-                   SIMOX_MIXED, Tuning, status_text)
+from ._abi import (AdjointReport, CtipReport, EamSpline, Energies, MdOpts, NGRAD, Oxidation, Potential, Setup,
+                   SIMOX_FP64, SIMOX_MIXED, Tuning, status_text)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libsimox_b200.so")
@@ -96,6 +96,11 @@ def lib():
         "simox_adjoint_eval": [_vp, _dp, C.POINTER(AdjointReport), _dp, _dp, _dp],
         "simox_adjoint_eval_many": [C.POINTER(_vp), C.c_int, C.POINTER(_dp), C.POINTER(AdjointReport),
                                     C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp), C.c_int],
+        "simox_remove_rigid_motion": [_vp],
+        "simox_oxide_check": [_vp, C.c_int, C.c_double, _ip],
+        "simox_new_o2": [_vp, C.c_int, C.c_double, C.c_double, C.c_ulonglong, C.c_ulonglong],
+        "simox_md_run_oxidation": [_vp, C.POINTER(MdOpts), C.POINTER(Oxidation), C.c_int, C.c_int,
+                                   C.POINTER(Energies), _ip, _ip],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -351,6 +356,52 @@ class Simox:
                "md_run")
         return e.as_dict()
 
+    # -- oxidation mode (main.f90:63-84), device-resident ----------------------
+    def remove_rigid_motion(self):
+        """REMOVE_RIGID_MOTION (vverlet.f90:211-234) on the device."""
+        _check(lib().simox_remove_rigid_motion(self._ctx), "remove_rigid_motion")
+
+    def oxide_check(self, n_o2: int, q_crit: float) -> bool:
+        """OXIDE_CHECK (util.f90:152-188) on the device: is a new dimer due?"""
+        due = C.c_int(0)
+        _check(lib().simox_oxide_check(self._ctx, int(n_o2), float(q_crit), C.byref(due)), "oxide_check")
+        return bool(due.value)
+
+    def new_o2(self, n_o2: int, z_new: float, T_given: float, seed: int, event: int):
+        """NEW_O2 (datafmt.f90:98-139) on the device: appends 2 n_o2 O atoms;
+        the atom count grows (a CELL_SORT is needed before FORCE)."""
+        _check(lib().simox_new_o2(self._ctx, int(n_o2), float(z_new), float(T_given), int(seed), int(event)),
+               "new_o2")
+        n = C.c_int(0)
+        _check(lib().simox_get_natoms(self._ctx, C.byref(n)), "get_natoms")
+        self.n = n.value
+
+    def md_run_oxidation(self, nsteps: int, dt: float, n_o2: int, z_new: float, q_crit: float, seed: int,
+                         first_step: int = 1, thermostat: bool = False, T_given: float = 0.0,
+                         freq_new: int = 0, freq_sort: int = 1, charge_every_step: bool = False,
+                         rdf: np.ndarray | None = None, freq_stat: int = 0):
+        """The oxidation-mode loop (main.f90:63-84) on the device: VV_NVE1_REFLECT,
+        CELL_SORT, and on charge steps REMOVE_RIGID_MOTION, OXIDE_CHECK, NEW_O2
+        when due, CTIP_SOLVER; FORCE, PME, VV_NVE2 / VV_NVT2_BEREND.  Returns
+        (energies of the last energy step, atoms inserted)."""
+        o = md_opts(dt, thermostat=thermostat, T_given=T_given, freq_new=freq_new, freq_sort=freq_sort,
+                    reflect=True, freq_stat=freq_stat)
+        o.charge_every_step = 1 if charge_every_step else 0
+        o.accumulate_rdf = 1 if rdf is not None else 0
+        ox = Oxidation()
+        ox.n_o2 = int(n_o2)
+        ox.z_new = float(z_new)
+        ox.q_crit = float(q_crit)
+        ox.seed = int(seed)
+        e = Energies()
+        ins = C.c_int(0)
+        _check(lib().simox_md_run_oxidation(self._ctx, C.byref(o), C.byref(ox), int(first_step), int(nsteps),
+                                            C.byref(e), _i(rdf), C.byref(ins)), "md_run_oxidation")
+        n = C.c_int(0)
+        _check(lib().simox_get_natoms(self._ctx, C.byref(n)), "get_natoms")
+        self.n = n.value
+        return e.as_dict(), ins.value
+
     # -- timing ---------------------------------------------------------------
     def timer_begin(self):
         _check(lib().simox_timer_begin(self._ctx), "timer_begin")
@@ -417,9 +468,11 @@ class Simox:
     def get_tuning(self) -> dict:
         t = Tuning()
         _check(lib().simox_get_tuning(self._ctx, C.byref(t)), "get_tuning")
-        return {"force_splits": t.force_splits}
+        return {"force_splits": t.force_splits, "half_list": t.half_list}
 
     def neighbor_stats(self):
+        """(longest exact-list row, total exact-list entries).  With the half
+        list (get_tuning()["half_list"]) each pair is one entry of one row."""
         mx = C.c_int(0)
         tot = C.c_longlong(0)
         _check(lib().simox_neighbor_stats(self._ctx, C.byref(mx), C.byref(tot)), "neighbor_stats")

@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 OUT = os.path.join(HERE, "libsimox_b200.so")
 OBJDIR = os.path.join(ROOT, "_build", "obj")
-SOURCES = ["api.cu", "cells.cu", "pair.cu", "pme.cu", "ctip.cu", "integrate.cu", "noalloc.cu", "batch.cu", "adjoint.cu"]
+SOURCES = ["api.cu", "cells.cu", "pair.cu", "pair_half.cu", "pme.cu", "ctip.cu", "integrate.cu", "noalloc.cu", "batch.cu", "adjoint.cu", "oxidation.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

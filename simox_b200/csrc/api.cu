@@ -197,7 +197,8 @@ static int md_step_graph(simox_ctx* c, const simox_md_opts* o, bool sort, bool e
     return cuda_status(cudaGraphLaunch(hit->exec, c->stream));
 }
 
-int md_run(simox_ctx* c, const simox_md_opts* o, int first, int nsteps, simox_energies* e, int* rdf) {
+int md_run(simox_ctx* c, const simox_md_opts* o, int first, int nsteps, simox_energies* e, int* rdf,
+           const simox_oxidation* ox, int* n_inserted) {
     if (!c->psi_valid || !c->cells_valid) return SIMOX_E_STATE;
     const bool want_rdf = rdf != nullptr || o->accumulate_rdf;
     if (want_rdf) cudaMemsetAsync(c->rdf, 0, sizeof(int) * SIMOX_RDF_LEN, c->stream);
@@ -213,6 +214,20 @@ int md_run(simox_ctx* c, const simox_md_opts* o, int first, int nsteps, simox_en
             const bool stoch = o->thermostat && o->thermo_stoch;
             if ((st = stoch ? nvt1_stoch(c, o->dt, o->alpha) : vv1(c, o->dt, o->reflect != 0))) return st;
             if (sort && (st = cell_sort(c))) return st;
+            if (ox) {
+                // oxidation mode (main.f90:69-74): REMOVE_RIGID_MOTION, OXIDE_CHECK
+                // and, when due, NEW_O2, all on the device; the moved and the new
+                // atoms are binned again before the charge solve
+                if ((st = remove_rigid_motion(c))) return st;
+                int due = 0;
+                if ((st = oxide_check(c, ox->n_o2, ox->q_crit, &due))) return st;
+                if (due && ox->n_o2 > 0) {
+                    if ((st = new_o2(c, ox->n_o2, ox->z_new, o->T_given, ox->seed, (unsigned long long)step)))
+                        return st;
+                    if (n_inserted) *n_inserted += 2 * ox->n_o2;
+                }
+                if ((st = cell_sort(c))) return st;
+            }
             simox_ctip_report rep;
             if ((st = ctip_solve(c, 0, &rep))) return st;
             simox_md_opts o2 = *o;
@@ -364,7 +379,7 @@ static void free_ctx(simox_ctx* c) {
                     c->sorted, c->pair13, c->entries, c->xq_s, c->t_s, c->rec_s, c->frec_s, c->nn, c->nbr, c->nn_max, c->nn_tot,
                     c->cs_count, c->cs_start, c->cs_fill, c->cs_cell_of, c->cs_entries, c->perm, c->x0,
                     c->skin_flag, c->nn_s, c->nbr_s, c->rho_s, c->dF_s, c->dF_f, c->tab_d, c->tab_f, c->c_const, c->g, c->pv, c->Ap, c->qs, c->jp,
-                    c->act, c->line, c->acc, c->status, c->rdf, c->f_rec};
+                    c->act, c->line, c->acc, c->status, c->rdf, c->f_rec, c->rho_fx, c->fx_acc};
     for (void* p : bufs)
         if (p) cudaFree(p);
     if (c->h_acc) cudaFreeHost(c->h_acc);
@@ -462,7 +477,8 @@ extern "C" int simox_create(const simox_setup* s, const simox_potential* pot, si
               dalloc(&c->pair13, (size_t)c->ncell * 13) && dalloc(&c->entries, (size_t)c->ncell * kEntries) &&
               dalloc(&c->xq_s, N) && dalloc(&c->t_s, N) && dalloc(&c->rec_s, N) && dalloc(&c->frec_s, N) && dalloc(&c->nn, 2 * N) &&
               dalloc(&c->nbr, N * (size_t)c->nnb_cap) && dalloc(&c->nn_max, 1) && dalloc(&c->nn_tot, 1) &&
-              dalloc(&c->rho_s, N) && dalloc(&c->dF_s, N) && dalloc(&c->dF_f, N) && dalloc(&c->tab_d, kSpecies * kSpecies) &&
+              dalloc(&c->rho_s, N) && dalloc(&c->dF_s, N) && dalloc(&c->dF_f, N) && dalloc(&c->rho_fx, N) &&
+              dalloc(&c->fx_acc, 3 * N) && dalloc(&c->tab_d, kSpecies * kSpecies) &&
               dalloc(&c->tab_f, kSpecies * kSpecies) && dalloc(&c->line, 64) && dalloc(&c->acc, A_COUNT) &&
               dalloc(&c->status, 1) && dalloc(&c->rdf, SIMOX_RDF_LEN);
     if (!ok) { free_ctx(c); return SIMOX_E_NOMEM; }
@@ -871,6 +887,16 @@ extern "C" int simox_md_run(simox_ctx* c, const simox_md_opts* o, int first_step
     return md_run(c, o, first_step, nsteps, e, rdf);
 }
 
+// main.f90:63-84: the oxidation-mode loop
+extern "C" int simox_md_run_oxidation(simox_ctx* c, const simox_md_opts* o, const simox_oxidation* ox,
+                                      int first_step, int nsteps, simox_energies* e, int* rdf, int* n_inserted) {
+    if (!c || !o || !ox || nsteps < 0 || ox->n_o2 < 0) return SIMOX_E_ARG;
+    if (o->thermo_stoch) return SIMOX_E_ARG;   // the oxidation loop has no stochastic thermostat (main.f90:65-79)
+    cudaSetDevice(c->device);
+    if (n_inserted) *n_inserted = 0;
+    return md_run(c, o, first_step, nsteps, e, rdf, ox, n_inserted);
+}
+
 extern "C" int simox_set_tuning(simox_ctx* c, const simox_tuning* t) {
     if (!c || !t) return SIMOX_E_ARG;
     if (t->force_splits < 1 || t->force_splits > 16) return SIMOX_E_ARG;
@@ -884,6 +910,7 @@ extern "C" int simox_set_tuning(simox_ctx* c, const simox_tuning* t) {
 extern "C" int simox_get_tuning(simox_ctx* c, simox_tuning* t) {
     if (!c || !t) return SIMOX_E_ARG;
     t->force_splits = c->force_splits;
+    t->half_list = c->using_skin && c->skin_half ? 1 : 0;
     return SIMOX_OK;
 }
 

@@ -271,7 +271,15 @@ struct LBParams {
     float r2lo, r2hi, hlx, hly, hlz;
     int cap, npt_max;
     int skin;   // skin list: entries carry the stencil code instead of "is i"
+    int half;   // skin list: keep a pair once (forward stencil positions, or the own cell and j > h)
 };
+
+// half skin list: partner j of home atom h in stencil position e is kept by h
+// when e is one of the 13 forward positions, or e is h's own cell and j > h
+__device__ __forceinline__ bool half_keep(const LBParams& P, unsigned tag, int j, int h) {
+    const int e = (int)(tag >> kSkinCodeShift);
+    return !P.half || e > 13 || (e == 13 && j > h);
+}
 
 // reference r2 (force.f90:51-53): rx = dx - box*DNINT(dx/box), no FMA
 __device__ __forceinline__ double exact_r2(double4 a, double4 b, double3 box) {
@@ -375,7 +383,7 @@ __global__ void __launch_bounds__(LB_THREADS)
                         const int j = (int)(tag & (P.skin ? kSkinIdxMask : 0x3fffffffu));
                         bool acc = r2 < P.r2lo;
                         if (!acc) acc = exact_r2(xh, xq[j], P.box) < P.rcut2;
-                        if (acc && j != h) {
+                        if (acc && j != h && (!P.skin || half_keep(P, tag, j, h))) {
                             const unsigned dir = tag >> 30;
                             const unsigned isa = dir == 0 ? (unsigned)(h < j) : (unsigned)(dir == 1);
                             list_append(row, my, P.cap, P.skin ? tag : (unsigned)j | (isa << 31), __float_as_int(cp.w));
@@ -386,7 +394,7 @@ __global__ void __launch_bounds__(LB_THREADS)
                 for (int k = 0; k < tn; k++) {
                     const unsigned tag = ctag[k];
                     const int j = (int)(tag & (P.skin ? kSkinIdxMask : 0x3fffffffu));
-                    if (j == h) continue;
+                    if (j == h || (P.skin && !half_keep(P, tag, j, h))) continue;
                     if (exact_r2(xh, xq[j], P.box) < P.rcut2) {
                         const unsigned dir = tag >> 30;
                         const unsigned isa = dir == 0 ? (unsigned)(h < j) : (unsigned)(dir == 1);
@@ -429,6 +437,7 @@ int build_list(simox_ctx* c) {
     P.ibox = make_double3(c->inv_box[0], c->inv_box[1], c->inv_box[2]);
     P.origin = make_double3(-c->hbox[0], -c->hbox[1], -c->hbox[2]);
     P.skin = 0;
+    P.half = 0;
     P.lc = make_double3(c->lc[0], c->lc[1], c->lc[2]);
     P.nc = make_int3(c->nc[0], c->nc[1], c->nc[2]);
     P.rcut2 = c->rcut2;
@@ -524,6 +533,10 @@ static int prepare_order(simox_ctx* c) {
     }
     c->pair_order = c->perm;
     c->using_skin = true;
+    // the half list needs one metal species plus oxygen (the packed pair
+    // kernels' tables); a new atom set invalidates the skin list, so the
+    // choice holds for the list's whole life
+    c->skin_half = c->precision != SIMOX_FP64 && c->g0_species >= 0;
     int* flag = c->skin_flag;
     if (!c->skin_valid) {
         const int one = 1;
@@ -580,6 +593,7 @@ static int prepare_order(simox_ctx* c) {
     P.cap = c->cap_s;
     P.npt_max = c->npt_max_s;
     P.skin = 1;
+    P.half = c->skin_half ? 1 : 0;
     const size_t smem = LB_TILE * (sizeof(float4) + sizeof(unsigned)) + sizeof(int2) * c->npt_max_s;
     {
         Launch L(c, "skin_list");

@@ -399,6 +399,10 @@ static void launch_ctip_pair(simox_ctx* c, const PairTab<R>* tab, const double* 
 
 void ctip_pair(simox_ctx* c, const double* vin, double* out, double* cconst, const CtipSpecies& S) {
     Launch L(c, cconst ? "ctip_setup_pairs" : "ctip_matvec_pairs");
+    if (c->precision == SIMOX_MIXED && half_path(c)) {   // a launch error surfaces at the next check
+        ctip_pair_half(c, vin, out, cconst, S);
+        return;
+    }
     if (c->precision == SIMOX_MIXED) launch_ctip_pair<float>(c, c->tab_f, vin, out, cconst, S);
     else launch_ctip_pair<double>(c, c->tab_d, vin, out, cconst, S);
 }

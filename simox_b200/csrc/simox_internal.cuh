@@ -193,6 +193,8 @@ struct simox_ctx {
     bool skin_mode = false;     // the box admits the skin list
     bool skin_valid = false;    // perm / x0 / skin list belong to this atom set
     bool using_skin = false;    // the current order is the skin order
+    bool skin_half = false;     // the skin list (and the exact list filtered from it) holds each pair once:
+                                // mixed precision with one metal species plus oxygen (pair_half.cu)
     bool cells_fresh = false;   // reference cells binned after the last move
     bool in_box = false;        // every coordinate in [-L/2, L/2]
     double skin = 1.0;
@@ -222,6 +224,10 @@ struct simox_ctx {
     unsigned* nbr = nullptr;    // [cap*nnb_cap]; metal partners from the front, oxygen from the back
     int* nn_max = nullptr;      // device max
     unsigned long long* nn_tot = nullptr;
+
+    // fixed-point accumulators of the half-list passes (pair_half.cu)
+    unsigned long long* rho_fx = nullptr;   // [cap] densities, 2^40
+    unsigned long long* fx_acc = nullptr;   // [3][cap] forces 2^32, or two charge-solver sums 2^40
 
     // EAM
     double* rho_s = nullptr;
@@ -321,6 +327,11 @@ int build_pair_tables(simox_ctx* c);
 int eam_density(simox_ctx* c, bool eflag);
 int filter_density(simox_ctx* c);
 int pair_forces(simox_ctx* c, bool eflag, bool rdf);
+// pair_half.cu
+bool half_path(const simox_ctx* c);
+int filter_density_half(simox_ctx* c);
+int force_half(simox_ctx* c, bool rdf);
+int energy_half(simox_ctx* c);
 // pme.cu
 int pme_setup(simox_ctx* c);
 int pme_free(simox_ctx* c);
@@ -341,6 +352,7 @@ int ctip_solve(simox_ctx* c, int max_cg, simox_ctip_report* rep, double tol = 1.
 CtipSpecies ctip_species(const simox_ctx* c);
 // out = sum_Y sym_XY vin_Y (sorted order); cconst (may be null) = chi + sum_Y Z_Y asym_XY
 void ctip_pair(simox_ctx* c, const double* vin, double* out, double* cconst, const CtipSpecies& S);
+int ctip_pair_half(simox_ctx* c, const double* vin, double* out, double* cconst, const CtipSpecies& S);
 int ctip_alloc(simox_ctx* c);
 // integrate.cu
 int vv1(simox_ctx* c, double dt, bool reflect);
@@ -348,7 +360,12 @@ int vv2(simox_ctx* c, double dt, bool subtract_mean, const double* f_add = nullp
 int nvt2_berend(simox_ctx* c, double dt, double T_given, bool subtract_mean, const double* f_add = nullptr);
 int update_masses(simox_ctx* c);
 // md
-int md_run(simox_ctx* c, const simox_md_opts* o, int first, int nsteps, simox_energies* e, int* rdf);
+int md_run(simox_ctx* c, const simox_md_opts* o, int first, int nsteps, simox_energies* e, int* rdf,
+           const simox_oxidation* ox = nullptr, int* n_inserted = nullptr);
+// oxidation.cu
+int remove_rigid_motion(simox_ctx* c);
+int oxide_check(simox_ctx* c, int n_o2, double q_crit, int* due);
+int new_o2(simox_ctx* c, int n_o2, double z_new, double T_given, unsigned long long seed, unsigned long long event);
 void drop_graphs(simox_ctx* c);
 int md_step(simox_ctx* c, const simox_md_opts* o, bool sort, bool estep, bool want_rdf);
 int vinit_velocities(simox_ctx* c, unsigned long long seed, double T_given);

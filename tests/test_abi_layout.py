@@ -16,7 +16,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PAIRS = [("simox_metl", _abi.Metl), ("simox_potn", _abi.Potn), ("simox_oxid", _abi.Oxid),
          ("simox_potential", _abi.Potential), ("simox_setup", _abi.Setup), ("simox_energies", _abi.Energies),
          ("simox_ctip_report", _abi.CtipReport), ("simox_md_opts", _abi.MdOpts), ("simox_tuning", _abi.Tuning),
-         ("simox_eam_spline", _abi.EamSpline), ("simox_adjoint_report", _abi.AdjointReport)]
+         ("simox_eam_spline", _abi.EamSpline), ("simox_adjoint_report", _abi.AdjointReport),
+         ("simox_oxidation", _abi.Oxidation)]
 
 # ctypes names that differ from the C member (Python keywords)
 RENAME = {("simox_metl", "lambda_"): "lambda"}

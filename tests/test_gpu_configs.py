@@ -97,6 +97,34 @@ def test_c1_slab_order6_fp64_vs_oracle():
     assert abs(e["mv2"] - mv2_o) <= 1e-9 * mv2_o
 
 
+def test_c1_slab_mixed_half_list_vs_oracle():
+    """The same slab in mixed precision runs the half-list kernels (each pair
+    once, partner shares in fixed-point sums): the charge solve must take the
+    oracle's CG iteration count and land within 1e-6 e of its charges, and
+    FORCE + PME must be within 1e-5 (relative norm) of the oracle's forces."""
+    s = _c1()
+    gold = _c1_golden(s)
+    o = oracle_system(s)
+    o.pme_self()
+    o.cell_sort()
+    o.q = np.array(gold["q"])
+    f_o, *_ = o.force()
+    f_o, _ = o.pme(f_o)
+    with gpu_context(s, precision="mixed") as g:
+        g.pme_self()
+        g.cell_sort()
+        _, rep = g.ctip_solver()
+        assert g.get_tuning()["half_list"] == 1
+        q = g.get_state()["q"]
+        assert rep["n_cg"] == int(gold["n_cg"]), (rep, int(gold["n_cg"]))
+        assert np.abs(q - gold["q"]).max() <= 1e-6, np.abs(q - gold["q"]).max()
+        g.set_state(q=o.q)
+        g.force(energies=False)
+        g.pme(energies=False)
+        f = g.get_state()["f"]
+    assert rel_err(f, f_o) <= 1e-5, rel_err(f, f_o)
+
+
 @pytest.fixture(scope="module")
 def corundum():
     return S.corundum(seed=2)
