@@ -344,6 +344,13 @@ int simox_set_ctip_params(simox_ctx* ctx, int species, double chi, double J, dou
  * SIMOX_E_ARG for xi <= 0 or xi equal to another species' xi (the cross
  * coefficients divide by xi_a - xi_b). */
 int simox_set_ctip_xi(simox_ctx* ctx, int species, double xi);
+/* Warm start of simox_adjoint_eval's charge solve (no counterpart in the
+ * reference).  on = 1: the solve skips CTIP_SOLVER's nonlinear CG and refines
+ * the charges the context holds by the safeguarded Newton steps on their
+ * active set -- for a sequence of nearby parameter sets (finite differences,
+ * an optimiser's line search), which then all stay on the branch of the
+ * charge minimum the held charges lie on.  on = 0 (the default): CG first. */
+int simox_adjoint_warm_start(simox_ctx* ctx, int on);
 /* Charges q*, energy, forces (original order, [n][3], may be NULL) and the
  * gradients of E (grad_E) and of L = sum |F - T|^2 (grad_L; needs f_target
  * [n][3]) with respect to the parameters; either gradient may be NULL.  The

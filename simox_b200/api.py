@@ -96,6 +96,7 @@ def lib():
         "simox_adjoint_eval": [_vp, _dp, C.POINTER(AdjointReport), _dp, _dp, _dp],
         "simox_adjoint_eval_many": [C.POINTER(_vp), C.c_int, C.POINTER(_dp), C.POINTER(AdjointReport),
                                     C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp), C.c_int],
+        "simox_adjoint_warm_start": [_vp, C.c_int],
         "simox_remove_rigid_motion": [_vp],
         "simox_oxide_check": [_vp, C.c_int, C.c_double, _ip],
         "simox_new_o2": [_vp, C.c_int, C.c_double, C.c_double, C.c_ulonglong, C.c_ulonglong],
@@ -455,6 +456,10 @@ class Simox:
         t = _f64(f_target, (self.n, 3))
         _check(lib().simox_adjoint_eval(self._ctx, _d(t), C.byref(rep), _d(f), _d(gE), _d(gL)), "adjoint_eval")
         return rep.as_dict(), f, gE, gL
+
+    def adjoint_warm_start(self, on: bool = True):
+        """Refine the held charges by Newton steps (no CG first) in adjoint_eval."""
+        _check(lib().simox_adjoint_warm_start(self._ctx, 1 if on else 0), "adjoint_warm_start")
 
     def set_ctip_xi(self, species: int, xi: float):
         """Slater exponent xi of species 1..5 (recomputes the fafb coefficients)."""

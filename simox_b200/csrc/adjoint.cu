@@ -1009,9 +1009,10 @@ int adjoint_eval(simox_ctx* c, const double* f_target, simox_adjoint_report* rep
     // The entry charges (sorted order) are kept in u, free until the loss pass.
     if ((st = ensure_list(c))) return st;
     adj_load_q<<<nb, 256, 0, s>>>(n, c->xq_s, A->u);
-    simox_ctip_report cr;
-    if ((st = ctip_solve(c, 0, &cr))) return st;
+    simox_ctip_report cr{};
+    if (!c->adj_warm && (st = ctip_solve(c, 0, &cr))) return st;
     R.n_cg = cr.n_cg;
+    if (c->adj_warm) adj_load_q<<<nb, 256, 0, s>>>(n, c->xq_s, c->qs);   // the held charges, in pair order
     auto grad_u = [&](double* Uout) -> int {
         // c (chi + sum Z asym), sr = sym q, phi = c_pme phi(q); G and U
         ctip_pair(c, c->qs, A->sr, A->cc, S);
@@ -1237,6 +1238,13 @@ extern "C" int simox_set_ctip_xi(simox_ctx* c, int species, double xi) {
             if (i == species - 1 || j == species - 1)
                 sx::slater_fafb<double>(c->pot.param[i].xi, c->pot.param[j].xi, i == j, c->pot.param[i].fafb[j]);
     return sx::build_pair_tables(c);
+}
+
+// warm start of the adjoint's charge solve (see the header)
+extern "C" int simox_adjoint_warm_start(simox_ctx* c, int on) {
+    if (!c) return SIMOX_E_ARG;
+    c->adj_warm = on != 0;
+    return SIMOX_OK;
 }
 
 extern "C" int simox_adjoint_eval(simox_ctx* c, const double* f_target, simox_adjoint_report* rep, double* forces,

@@ -163,6 +163,7 @@ struct simox_ctx {
     int force_splits = 2;       // CTAs per skin cell of the mixed force pass (simox_set_tuning)
     unsigned long long md_step_no = 0;   // md_run's current step: the stochastic thermostat's draw counter
     sx::AdjointState* adj = nullptr;   // parameter-adjoint model (simox_set_eam_spline)
+    bool adj_warm = false;             // adjoint: refine the held charges by Newton, no CG first
     bool spline_on = false;
 
     // species present
