@@ -65,6 +65,8 @@ extern "C" {
                                        is not a checkpoint, or its box differs */
 #define SIMOX_E_RNG            -19  /* VV_NVT2_STOCH: a random-force draw rejected 100
                                        polar-method attempts (probability 3e-67) */
+#define SIMOX_E_SYNC           -20  /* a device-wide wait inside a kernel gave up after its
+                                       iteration limit (its CTAs did not all arrive) */
 
 /* ---- precision modes --------------------------------------------------- */
 #define SIMOX_FP64   0   /* every term in FP64 (the FP64 GPU oracle path) */

@@ -34,6 +34,7 @@ SIMOX_E_UNSUPPORTED = -16
 SIMOX_E_SCRATCH_LIMIT = -17
 SIMOX_E_IO = -18
 SIMOX_E_RNG = -19
+SIMOX_E_SYNC = -20
 
 SIMOX_FP64 = 0
 SIMOX_MIXED = 1
@@ -63,6 +64,7 @@ _STATUS = {
     SIMOX_E_SCRATCH_LIMIT: "size beyond the fixed scratch of simox_cell_sort_noalloc (65536 cells, stride 4096)",
     SIMOX_E_IO: "=== cannot open checkpoint, or not a checkpoint of this box ===",
     SIMOX_E_RNG: "random-force draw rejected 100 polar-method attempts",
+    SIMOX_E_SYNC: "a device-wide wait inside a kernel gave up (its CTAs did not all arrive)",
 }
 
 

@@ -34,6 +34,7 @@ int read_status(simox_ctx* c) {
     if (s & ST_UNSUPPORTED) return SIMOX_E_UNSUPPORTED;
     if (s & ST_LINE_NOBRACKET) return SIMOX_E_BRENT;
     if (s & ST_RNG) return SIMOX_E_RNG;
+    if (s & ST_SYNC) return SIMOX_E_SYNC;
     return SIMOX_OK;
 }
 
@@ -361,6 +362,7 @@ extern "C" const char* simox_status_string(int s) {
         case SIMOX_E_SCRATCH_LIMIT: return "size beyond the fixed scratch of simox_cell_sort_noalloc (65536 cells, stride 4096)";
         case SIMOX_E_IO: return "=== cannot open checkpoint, or not a checkpoint of this box ===";
         case SIMOX_E_RNG: return "random-force draw rejected 100 polar-method attempts";
+        case SIMOX_E_SYNC: return "a device-wide wait inside a kernel gave up (its CTAs did not all arrive)";
         default: return "unknown status";
     }
 }
@@ -376,7 +378,7 @@ static void free_ctx(simox_ctx* c) {
     adjoint_free(c);
     pme_free(c);
     void* bufs[] = {c->id, c->x, c->v, c->f, c->q, c->xm, c->cell_of, c->cell_xyz, c->cell_count, c->cell_start, c->cell_fill,
-                    c->sorted, c->pair13, c->entries, c->xq_s, c->t_s, c->rec_s, c->frec_s, c->nn, c->nbr, c->nn_max, c->nn_tot,
+                    c->sorted, c->pair13, c->entries, c->xq_s, c->t_s, c->rec_s, c->frec_s, c->xo_s, c->nn, c->nbr, c->nn_max, c->nn_tot,
                     c->cs_count, c->cs_start, c->cs_fill, c->cs_cell_of, c->cs_entries, c->perm, c->x0,
                     c->skin_flag, c->nn_s, c->nbr_s, c->rho_s, c->dF_s, c->dF_f, c->tab_d, c->tab_f, c->c_const, c->g, c->pv, c->Ap, c->qs, c->jp,
                     c->act, c->line, c->acc, c->status, c->rdf, c->f_rec, c->rho_fx, c->fx_acc};
@@ -475,7 +477,8 @@ extern "C" int simox_create(const simox_setup* s, const simox_potential* pot, si
               dalloc(&c->q, N) && dalloc(&c->cell_of, N) && dalloc(&c->cell_xyz, N) && dalloc(&c->cell_count, c->ncell) &&
               dalloc(&c->cell_start, c->ncell + 1) && dalloc(&c->cell_fill, c->ncell) && dalloc(&c->sorted, N) &&
               dalloc(&c->pair13, (size_t)c->ncell * 13) && dalloc(&c->entries, (size_t)c->ncell * kEntries) &&
-              dalloc(&c->xq_s, N) && dalloc(&c->t_s, N) && dalloc(&c->rec_s, N) && dalloc(&c->frec_s, N) && dalloc(&c->nn, 2 * N) &&
+              dalloc(&c->xq_s, N) && dalloc(&c->t_s, N) && dalloc(&c->rec_s, N) && dalloc(&c->frec_s, N) &&
+              dalloc(&c->xo_s, N) && dalloc(&c->nn, 2 * N) &&
               dalloc(&c->nbr, N * (size_t)c->nnb_cap) && dalloc(&c->nn_max, 1) && dalloc(&c->nn_tot, 1) &&
               dalloc(&c->rho_s, N) && dalloc(&c->dF_s, N) && dalloc(&c->dF_f, N) && dalloc(&c->rho_fx, N) &&
               dalloc(&c->fx_acc, 3 * N) && dalloc(&c->tab_d, kSpecies * kSpecies) &&

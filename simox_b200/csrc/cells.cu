@@ -211,7 +211,7 @@ __global__ void gather_sorted_kernel(int n, const int* __restrict__ sorted, cons
                                      const double* __restrict__ q, const int* __restrict__ id,
                                      double4* __restrict__ xq, int* __restrict__ ts, const int* __restrict__ cell_xyz,
                                      const int* __restrict__ cs_cell_of, RecParams R, float4* __restrict__ rec,
-                                     float4* __restrict__ frec) {
+                                     float4* __restrict__ frec, double4* __restrict__ xo) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     int o = sorted[k];
@@ -233,6 +233,7 @@ __global__ void gather_sorted_kernel(int n, const int* __restrict__ sorted, cons
         const unsigned w = (cx & 511u) | (((cx >> 10) & 511u) << 9) | (((cx >> 20) & 511u) << 18) | (sp << 27);
         rec[k] = make_float4((float)ox, (float)oy, (float)oz, __uint_as_float(w));
         frec[k] = make_float4((float)ox, (float)oy, (float)oz, (float)q[o]);
+        xo[k] = make_double4(ox, oy, oz, q[o]);
     }
 }
 
@@ -249,7 +250,7 @@ int gather_sorted(simox_ctx* c) {
         const bool skin = c->pair_order == c->perm && c->skin_mode;
         gather_sorted_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(
             c->n, c->pair_order, c->x, c->q, c->id, c->xq_s, c->t_s, c->cell_xyz, c->cs_cell_of, R,
-            skin ? c->rec_s : nullptr, c->frec_s);
+            skin ? c->rec_s : nullptr, c->frec_s, c->xo_s);
     }
     c->gathered = true;
     c->rho_ready = false;

@@ -296,6 +296,144 @@ __global__ void __launch_bounds__(1024)
     }
 }
 
+// The same Brent iteration with each h(b) spread over the whole GPU: every
+// CTA runs the identical control flow, sums its slice of the active set, and
+// a grid barrier exchanges the per-CTA partial sums, which every CTA then
+// adds in CTA order -- so all CTAs see the same h(b), take the same branches
+// and agree on the returned b.  Launched cooperatively, so all CTAs are
+// resident; each barrier wait still gives up after a bounded number of polls
+// (ST_SYNC), after which the kernel skips its remaining waits and ends.
+constexpr int BR_THREADS = 256;
+constexpr long long kBarrierPolls = 1LL << 22;
+
+// Grid barrier on (count, gen): returns false when the wait gave up.
+__device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned* gen, unsigned nb, int& ok_sh) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned g = atomicAdd(gen, 0u);
+        __threadfence();
+        if (atomicAdd(count, 1u) == nb - 1u) {
+            atomicExch(count, 0u);
+            __threadfence();
+            atomicAdd(gen, 1u);
+        } else {
+            long long it = 0;
+            while (atomicAdd(gen, 0u) == g) {
+                if (++it > kBarrierPolls) {
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        ok_sh = ok;
+    }
+    __syncthreads();
+    return ok_sh != 0;
+}
+
+__global__ void __launch_bounds__(BR_THREADS)
+    ctip_brent_grid_kernel(const int* __restrict__ ts, const double* __restrict__ q, const double* __restrict__ pv,
+                           const int* __restrict__ act, const int* __restrict__ nact, CtipSpecies S,
+                           double* __restrict__ line, double* __restrict__ acc, double ecrit, int* __restrict__ status,
+                           double* __restrict__ part, unsigned* __restrict__ bar) {
+    __shared__ double red[BR_THREADS / 32];
+    __shared__ double tot;
+    __shared__ int ok_sh;
+    const double gp = acc[A_GP], pap = acc[A_PAP];
+    const int na = *nact;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned nb = gridDim.x;
+    bool synced = true;
+    int ev = 0;
+    auto H = [&](double b) -> double {
+        double s = 0.0;
+        for (int k = blockIdx.x * BR_THREADS + threadIdx.x; k < na; k += nb * BR_THREADS) {
+            const int i = act[k];
+            const int sp = min(ts[i], 4);
+            const double qi = q[i], p = pv[i];
+            s += p * (pen_d(qi + b * p, S.qmin[sp], S.qmax[sp]) - pen_d(qi, S.qmin[sp], S.qmax[sp]));
+        }
+        s = warp_sum(s);
+        if (lane == 0) red[w] = s;
+        __syncthreads();
+        double* slot = part + (ev & 1) * nb;
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int j = 0; j < BR_THREADS / 32; j++) t += red[j];
+            slot[blockIdx.x] = t;
+        }
+        ev++;
+        if (synced) synced = grid_barrier(bar, bar + 1, nb, ok_sh);
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (unsigned j = 0; j < nb; j++) t += *(volatile double*)(slot + j);   // CTA order: same in every CTA
+            tot = t;
+        }
+        __syncthreads();
+        const double h = -gp + b * pap + tot;   // = -sum g(q + b p) p
+        __syncthreads();
+        return synced ? h : NAN;
+    };
+    const double E_crit = 1.0e-8, E_end = 1.0e-11;
+    double a = -1.0, b = 1.0, c, d = 0.0, e = 0.0, fa, fb, fc, xm, sv, x, y, z;
+    fa = H(a);
+    fb = H(b);
+    c = b;
+    fc = fb;
+    double alpha = b;
+    int n, ok = 0;
+    for (n = 1; n <= 100; n++) {
+        if ((fb > 0.0 && fc > 0.0) || (fb < 0.0 && fc < 0.0)) { c = a; fc = fa; d = b - a; e = d; }
+        if (fabs(fc) < fabs(fb)) { a = b; b = c; c = a; fa = fb; fb = fc; fc = fa; }
+        xm = 0.5 * (c - b);
+        if (fabs(xm) < E_crit || fabs(fb) < E_end) { alpha = b; ok = 1; break; }
+        if (fabs(e) >= E_crit && fabs(fa) > fabs(fb)) {
+            sv = fb / fa;
+            if (a == c) { x = 2.0 * xm * sv; y = 1.0 - sv; }
+            else {
+                y = fa / fc;
+                z = fb / fc;
+                x = sv * (2.0 * xm * y * (y - z) - (b - a) * (z - 1.0));
+                y = (y - 1.0) * (z - 1.0) * (sv - 1.0);
+            }
+            if (x > 0.0) y = -y;
+            x = fabs(x);
+            const double m1 = 3.0 * xm * y - fabs(E_crit * y), m2 = fabs(e * y);
+            if (2.0 * x < (m1 < m2 ? m1 : m2)) { e = d; d = x / y; }
+            else { d = xm; e = d; }
+        } else { d = xm; e = d; }
+        a = b;
+        fa = fb;
+        if (fabs(d) > E_crit) b = b + d;
+        else b = b + (xm >= 0.0 ? E_crit : -E_crit);
+        fb = H(b);
+        if (!synced) break;
+    }
+    if (!synced) {
+        if (threadIdx.x == 0) atomicOr(status, ST_SYNC);
+        return;
+    }
+    // every CTA has read gp, pap and the partials of its last evaluation
+    // before any CTA left the last barrier; CTA 0 writes the results
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (!ok) atomicOr(status, ST_LINE_NOBRACKET);
+        const double err = acc[A_PMAX] * fabs(alpha);          // ctip.f90:187
+        line[L_ALPHA] = alpha;
+        line[L_ERROR] = err;
+        line[L_DONE] = err > ecrit ? 0.0 : 1.0;
+        line[L_NEVAL] += (double)(2 + (ok ? n - 1 : 100));
+        line[L_GSUM_OLD] = acc[A_GSUM];
+        acc[A_GSUM] = 0.0;
+        acc[A_PSUM] = 0.0;
+        acc[A_PMAX] = 0.0;
+        acc[A_GP] = 0.0;
+        acc[A_PAP] = 0.0;
+    }
+}
+
 // q += alpha p; g -= alpha Ap + dpen; sum g   (ctip.f90:185 and the next dUdq)
 __global__ void __launch_bounds__(CT_THREADS)
     ctip_update_kernel(int n, const int* __restrict__ ts, double* __restrict__ q, double* __restrict__ g,
@@ -320,8 +458,8 @@ __global__ void __launch_bounds__(CT_THREADS)
 // write charges back (original order and the sorted copy); Eself pieces (ctip.f90:194-209)
 __global__ void __launch_bounds__(CT_THREADS)
     ctip_final_kernel(int n, const int* __restrict__ ts, const int* __restrict__ sorted, const double* __restrict__ qs,
-                      double* __restrict__ q, double4* __restrict__ xq, float4* __restrict__ frec, CtipSpecies S,
-                      double* __restrict__ acc) {
+                      double* __restrict__ q, double4* __restrict__ xq, float4* __restrict__ frec,
+                      double4* __restrict__ xo, CtipSpecies S, double* __restrict__ acc) {
     __shared__ double red[CT_THREADS / 32];
     double q2 = 0.0, es = 0.0, qsum = 0.0;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -330,7 +468,8 @@ __global__ void __launch_bounds__(CT_THREADS)
         const double qi = qs[i];
         q[sorted[i]] = qi;
         xq[i].w = qi;
-        frec[i].w = (float)qi;   // skin-mode force record (unused otherwise)
+        frec[i].w = (float)qi;   // skin-mode force records (unused otherwise)
+        xo[i].w = qi;
         q2 = -(qi * qi);
         qsum = qi;
         es = S.chi[s] * qi + 0.5 * S.Jp[s] * (qi * qi);
@@ -407,6 +546,36 @@ void ctip_pair(simox_ctx* c, const double* vin, double* out, double* cconst, con
     else launch_ctip_pair<double>(c, c->tab_d, vin, out, cconst, S);
 }
 
+// The line search on the whole GPU (cooperative launch, one CTA per SM); false
+// when that launch is not available here (the caller then runs the one-CTA
+// kernel).  Scratch: the per-CTA partial sums in the short-range work vector
+// (free during the line search) and the barrier words in the line slots.
+static bool brent_grid(simox_ctx* c, const CtipSpecies& S, double tol, int* nact) {
+    if (!c->coop_brent) return false;
+    const int nbk = num_sms(c);
+    if ((size_t)2 * nbk > (size_t)c->cap) return false;
+    unsigned* bar = reinterpret_cast<unsigned*>(c->line + 62);
+    cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), c->stream);
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(nbk);
+    cfg.blockDim = dim3(BR_THREADS);
+    cfg.stream = c->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, ctip_brent_grid_kernel, (const int*)c->t_s, (const double*)c->qs,
+                                             (const double*)c->pv, (const int*)c->act, (const int*)nact, S, c->line,
+                                             c->acc, tol, c->status, c->jp, bar);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        c->coop_brent = false;
+        return false;
+    }
+    return true;
+}
+
 // One nonlinear-CG iteration (ctip.f90:169-190): direction with the
 // reference's beta, mean projection, A p (PME potential + short-range pairs),
 // the Brent line search and the update.  Every launch goes to c->stream, so
@@ -423,16 +592,35 @@ static int ctip_iteration(simox_ctx* c, const CtipSpecies& S, double c_pme, doub
         Launch L(c, "ctip_project");
         ctip_proj_kernel<<<nb, CT_THREADS, 0, s>>>(n, c->pv, c->acc);
     }
-    if (int st = pme_potential(c, c->pv, c->Ap, c_pme)) return st;
-    ctip_pair(c, c->pv, c->jp, nullptr, S);
-    {
+    if (c->precision == SIMOX_MIXED && half_path(c)) {
+        // A p as one fused product: the half-list pair sums run on the side
+        // stream while the main stream spreads p and transforms the grid;
+        // one kernel then gathers the potential and adds the pair sums, J' p,
+        // the dots and the active set
+        cudaMemsetAsync(c->fx_acc, 0, sizeof(unsigned long long) * (size_t)n, s);
+        cudaStream_t ps = c->profiling ? s : c->side;   // profiled launches stay on one stream
+        if (ps != s) {
+            cudaEventRecord(c->ev_fork, s);
+            cudaStreamWaitEvent(ps, c->ev_fork, 0);
+        }
+        if (int st = ctip_half_launch(c, c->pv, ps)) return st;
+        if (ps != s) cudaEventRecord(c->ev_join, ps);
+        if (int st = pme_potential_grid(c, c->pv)) return st;
+        if (ps != s) cudaStreamWaitEvent(s, c->ev_join, 0);
+        CtipFinish F{c->t_s, c->qs, c->g, c->pv, c->fx_acc, ctip_half_unit(), c->Ap, c->act, nact, c->acc, S};
+        if (int st = pme_potential_finish(c, c_pme, F)) return st;
+    } else {
+        if (int st = pme_potential(c, c->pv, c->Ap, c_pme)) return st;
+        ctip_pair(c, c->pv, c->jp, nullptr, S);
         Launch L(c, "ctip_matvec_finish");
         ctip_matvec_finish_kernel<<<nb, CT_THREADS, 0, s>>>(n, c->t_s, c->qs, c->g, c->pv, c->jp, c->Ap, S, c->act,
                                                            nact, c->acc);
     }
     {
         Launch L(c, "ctip_brent");
-        ctip_brent_kernel<<<1, 1024, 0, s>>>(c->t_s, c->qs, c->pv, c->act, nact, S, c->line, c->acc, tol, c->status);
+        if (!brent_grid(c, S, tol, nact))
+            ctip_brent_kernel<<<1, 1024, 0, s>>>(c->t_s, c->qs, c->pv, c->act, nact, S, c->line, c->acc, tol,
+                                                 c->status);
     }
     {
         Launch L(c, "ctip_update");
@@ -582,7 +770,7 @@ int ctip_solve(simox_ctx* c, int max_cg, simox_ctip_report* rep, double tol) {
     cudaMemsetAsync(c->acc + A_QSUM, 0, sizeof(double), s);
     {
         Launch L(c, "ctip_final");
-        ctip_final_kernel<<<nb, CT_THREADS, 0, s>>>(n, c->t_s, c->pair_order, c->qs, c->q, c->xq_s, c->frec_s, S,
+        ctip_final_kernel<<<nb, CT_THREADS, 0, s>>>(n, c->t_s, c->pair_order, c->qs, c->q, c->xq_s, c->frec_s, c->xo_s, S,
                                                               c->acc);
     }
     cudaMemcpyAsync(c->h_acc, c->acc, sizeof(double) * A_COUNT, cudaMemcpyDeviceToHost, s);

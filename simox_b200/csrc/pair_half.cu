@@ -54,12 +54,38 @@ constexpr int kH1Threads = 256;
 constexpr int kH1Cap = 4096;
 // pass 2 and the charge solver: 512 threads, one CTA per SM, dynamic tiles
 constexpr int kH2Threads = 512;
-constexpr int kH2Cap = 4608;                              // 44 B per atom: 203 KB
-constexpr size_t kH2Smem = (size_t)kH2Cap * (sizeof(float4) + sizeof(float) + 3 * sizeof(u64));
+constexpr int kH2Cap = 3584;                              // 60 B per atom: 210 KB
+constexpr size_t kH2Smem = (size_t)kH2Cap * (sizeof(double4) + sizeof(float) + 6 * sizeof(unsigned));
 constexpr int kHCCap = 4608;                              // 40 B per atom: 184 KB
-constexpr size_t kHCSmem = (size_t)kHCCap * (sizeof(float4) + sizeof(double) + 2 * sizeof(u64));
+constexpr size_t kHCSmem = (size_t)kHCCap * (sizeof(float4) + sizeof(double) + 4 * sizeof(unsigned));
 
 __device__ __forceinline__ void add_fixed(u64* p, long long v) { atomicAdd(p, (u64)v); }
+
+// A 64-bit fixed-point sum in shared memory held as two 32-bit words: the
+// carry out of the low word goes into the high word, so the pair adds up
+// exactly (modulo 2^64) in any order.  Two 32-bit shared atomics run several
+// times faster than one 64-bit shared atomic on this GPU.
+__device__ __forceinline__ void add_split(unsigned* lo, unsigned* hi, int i, long long v) {
+    const unsigned vl = (unsigned)v, vh = (unsigned)((unsigned long long)v >> 32);
+    const unsigned old = atomicAdd(lo + i, vl);
+    atomicAdd(hi + i, vh + ((unsigned)(old + vl) < old ? 1u : 0u));
+}
+
+// Where a partner's share goes: the CTA's tile (split words, `stride`
+// entries per component) or, for a tile too large for shared memory, the
+// global 64-bit sums (`stride` entries per component).
+template <bool TILED> struct Sink;
+template <> struct Sink<true> {
+    unsigned* lo;
+    unsigned* hi;
+    int stride;
+    __device__ __forceinline__ void add(int c, int i, long long v) const { add_split(lo + c * stride, hi + c * stride, i, v); }
+};
+template <> struct Sink<false> {
+    u64* g;
+    int stride;
+    __device__ __forceinline__ void add(int c, int i, long long v) const { atomicAdd(g + (size_t)c * stride + i, (u64)v); }
+};
 
 // The 14 cells of a CTA's tile: first pair-order index of each and their
 // offsets in the tile (own cell first).
@@ -84,16 +110,17 @@ __device__ __forceinline__ void half_tile_setup(HalfTile& T, const int* __restri
     __syncthreads();
 }
 
-// Adds the tile's accumulators (nacc arrays of `stride` entries) into the
-// global ones (nacc arrays of `gstride`), skipping zeros.
-__device__ __forceinline__ void half_tile_flush(const HalfTile& T, int total, const u64* acc, int stride, int nacc,
-                                                u64* gacc, int gstride) {
+// Adds the tile's split sums (nacc components of `stride` entries) into the
+// global 64-bit sums (nacc components of `gstride`), skipping zeros.
+__device__ __forceinline__ void half_tile_flush_split(const HalfTile& T, int total, const unsigned* lo,
+                                                      const unsigned* hi, int stride, int nacc, u64* gacc,
+                                                      int gstride) {
     int t = 0;
     for (int i = threadIdx.x; i < total; i += blockDim.x) {
         while (T.off[t + 1] <= i) t++;
         const int gi = T.start[t] + (i - T.off[t]);
         for (int a = 0; a < nacc; a++) {
-            const u64 v = acc[a * stride + i];
+            const u64 v = ((u64)hi[a * stride + i] << 32) | lo[a * stride + i];
             if (v) atomicAdd(gacc + (size_t)a * gstride + gi, v);
         }
     }
@@ -118,7 +145,7 @@ __device__ __forceinline__ int filter_group_half(const Half1Params& H, const flo
                                                  const float4& ra, unsigned wa, int xm, int ym, int zm, int oX, int X,
                                                  const double4* __restrict__ xq, const float4* __restrict__ rec,
                                                  const int* __restrict__ order, const int* delta, int lim,
-                                                 u64* acc, double& rho) {
+                                                 const Sink<TILED>& acc, double& rho) {
     const FilterParams& F = H.F;
     const PairParams& P = F.pp;
     const int lane = threadIdx.x & 31;
@@ -169,7 +196,7 @@ __device__ __forceinline__ int filter_group_half(const Half1Params& H, const flo
             // stencil positions below 13 never occur in a half row: clamp into range anyway
             int slot = TILED ? (int)Y + delta[max(code - kHalfFirst, 0)] : (int)Y;
             slot = (unsigned)slot < (unsigned)lim ? slot : 0;
-            add_fixed(acc + slot, __float2ll_rn(vY * kRhoScale));
+            acc.add(0, slot, __float2ll_rn(vY * kRhoScale));
         }
     }
     return out;
@@ -181,7 +208,8 @@ __device__ __forceinline__ void filter_half_atoms(const Half1Params& H, const fl
                                                   const float4* __restrict__ rec, const int* __restrict__ order,
                                                   const int2* __restrict__ nn_s, const unsigned* __restrict__ nbr_s,
                                                   int2* __restrict__ nn, unsigned* __restrict__ nbr, const int* delta,
-                                                  int lim, u64* acc, int& lmax, unsigned long long& ltot, int& bad) {
+                                                  int lim, const Sink<TILED>& acc, int& lmax, unsigned long long& ltot,
+                                                  int& bad) {
     const FilterParams& F = H.F;
     const int lane = threadIdx.x & 31;
     const int g0 = H.g0;
@@ -224,9 +252,7 @@ __device__ __forceinline__ void filter_half_atoms(const Half1Params& H, const fl
             }
             lmax = max(lmax, tot);
             ltot += (unsigned long long)tot;
-            const long long w = __double2ll_rn(rho * kRhoScaleD);
-            if (TILED) add_fixed(acc + (X - a0), w);
-            else add_fixed(acc + X, w);
+            acc.add(0, TILED ? X - a0 : X, __double2ll_rn(rho * kRhoScaleD));
         }
     }
 }
@@ -238,7 +264,7 @@ __global__ void __launch_bounds__(kH1Threads)
                        const int2* __restrict__ nn_s, const unsigned* __restrict__ nbr_s, int2* __restrict__ nn,
                        unsigned* __restrict__ nbr, u64* __restrict__ rho_fx, int* __restrict__ status,
                        int* __restrict__ nn_max, unsigned long long* __restrict__ nn_tot) {
-    __shared__ u64 acc[kH1Cap];
+    __shared__ unsigned alo[kH1Cap], ahi[kH1Cap];
     __shared__ DensC<float> dsh[64];
     __shared__ int dflag[64];
     __shared__ float4 ssh[kEntries];
@@ -269,7 +295,10 @@ __global__ void __launch_bounds__(kH1Threads)
     const bool tiled = total <= kH1Cap;
     if (tid < kHalfCells) delta[tid] = T.off[tid] - T.start[tid];
     if (tiled)
-        for (int i = tid; i < total; i += blockDim.x) acc[i] = 0ull;
+        for (int i = tid; i < total; i += blockDim.x) {
+            alo[i] = 0u;
+            ahi[i] = 0u;
+        }
     __syncthreads();
     const int g0 = H.g0;
     const int a0 = T.start[0], na = T.off[1];
@@ -282,10 +311,10 @@ __global__ void __launch_bounds__(kH1Threads)
         bad = dflag[(g0 << 3) | g0] | dflag[(g0 << 3) | 3] | dflag[(3 << 3) | g0] | dflag[(3 << 3) | 3];
         if (tiled)
             filter_half_atoms<true>(H, ssh, dsh, b0, b1, a0, &next, xq, rec, order, nn_s, nbr_s, nn, nbr, delta,
-                                    total, acc, lmax, ltot, bad);
+                                    total, Sink<true>{alo, ahi, 0}, lmax, ltot, bad);
         else
             filter_half_atoms<false>(H, ssh, dsh, b0, b1, a0, &next, xq, rec, order, nn_s, nbr_s, nn, nbr, delta,
-                                     H.F.pp.n, rho_fx, lmax, ltot, bad);
+                                     H.F.pp.n, Sink<false>{rho_fx, 0}, lmax, ltot, bad);
     }
     if (bad) atomicOr(status, bad);
     if ((tid & 31) == 0) {
@@ -293,7 +322,7 @@ __global__ void __launch_bounds__(kH1Threads)
         if (ltot) atomicAdd(nn_tot, ltot);
     }
     __syncthreads();
-    if (tiled) half_tile_flush(T, total, acc, 0, 1, rho_fx, 0);
+    if (tiled) half_tile_flush_split(T, total, alo, ahi, 0, 1, rho_fx, 0);
 }
 
 // rho from the fixed-point sums, then F'(rho) (force.f90:256-351)
@@ -312,33 +341,60 @@ __global__ void embed_half_kernel(int n, const int* __restrict__ ts, const u64* 
 
 // ---------------------------------------------------------------------------
 // pass 2
+//
+// Separations are formed in FP64 and then rounded to FP32: each atom's record
+// holds its FP64 offset from the centre of the skin cell it was binned into;
+// the tile stores the partner cells' offsets already moved by their stencil
+// shift o * Lcs, so x_X - x_Y = off_X - tile_Y exactly up to FP64 rounding.
+// (Differences of FP32 offsets lose up to ~1e-6 A in the subtraction itself,
+// which the stiff near-neighbour forces turn into per-atom errors near the
+// 1e-5 bar.)
+
+struct Half2Params {
+    PackParams Q;
+    double3 lcs;               // skin-cell edges
+    int splits, g0, n, fstride;
+};
+
+// o_e * Lcs of stencil position e = (dk+1) 9 + (dj+1) 3 + (di+1)
+__device__ __forceinline__ double3 stencil_shift(int e, double3 lcs) {
+    return make_double3((e % 3 - 1) * lcs.x, ((e / 3) % 3 - 1) * lcs.y, (e / 9 - 1) * lcs.z);
+}
 
 // Two entries of X's half row as the halves of packed FP32 values: f/r of
 // each pair, X's share into the compensated FP32 sums, Y's share (the
-// opposite force) into Y's fixed-point accumulators.
-template <bool SAME, bool MHOMO, bool RDF, int TI>
-__device__ __forceinline__ void force_half_batch(const PackParams& Q, const float4* etab, const float4* __restrict__ rsrc,
-                                                 const float* __restrict__ dsrc, int lim, unsigned E1, unsigned E2,
-                                                 bool v1, bool v2ok, const float4& ra, float dFX, u64* ax, u64* ay,
-                                                 u64* az, v2 (&fh)[3], v2 (&fl)[3], int* hist, int& bad) {
+// opposite force) into Y's fixed-point sums.
+template <bool SAME, bool MHOMO, bool RDF, bool TILED, int TI>
+__device__ __forceinline__ void force_half_batch(const Half2Params& H, const int* edelta, const double3* esh,
+                                                 const double4* __restrict__ psrc, const float* __restrict__ dsrc,
+                                                 int lim, unsigned E1, unsigned E2, bool v1, bool v2ok,
+                                                 const double4& ra, float dFX, const Sink<TILED>& acc, v2 (&fh)[3],
+                                                 v2 (&fl)[3], int* hist, int& bad) {
     constexpr int NB = SIMOX_NRDF + 2;
+    const PackParams& Q = H.Q;
     const PackTab& T = Q.tab[TI];
-    const float kcqa = Q.kc * ra.w;
-    const float kcqaZY = T.kcZY * ra.w;
-    const float4 t1 = etab[(E1 >> kSkinCodeShift) & kCodeMask];
-    const float4 t2 = etab[(E2 >> kSkinCodeShift) & kCodeMask];
-    int i1 = (int)(E1 & kIdxMask) + __float_as_int(t1.w);
-    int i2 = (int)(E2 & kIdxMask) + __float_as_int(t2.w);
+    const float qa = (float)ra.w;
+    const float kcqa = Q.kc * qa;
+    const float kcqaZY = T.kcZY * qa;
+    const int c1 = min((int)((E1 >> kSkinCodeShift) & kCodeMask), kEntries - 1);
+    const int c2 = min((int)((E2 >> kSkinCodeShift) & kCodeMask), kEntries - 1);
+    int i1 = (int)(E1 & kIdxMask) + edelta[c1];
+    int i2 = (int)(E2 & kIdxMask) + edelta[c2];
     // keep every access inside the tile (or the atom range)
     i1 = (unsigned)i1 < (unsigned)lim ? i1 : 0;
     i2 = (unsigned)i2 < (unsigned)lim ? i2 : 0;
-    const float4 B1 = rsrc[i1], B2 = rsrc[i2];
+    double4 P1 = psrc[i1], P2 = psrc[i2];
+    if (!TILED) {   // global offsets: add the stencil shift here
+        const double3 s1 = esh[c1], s2 = esh[c2];
+        P1.x += s1.x; P1.y += s1.y; P1.z += s1.z;
+        P2.x += s2.x; P2.y += s2.y; P2.z += s2.z;
+    }
     const float D1 = dsrc[i1], D2 = dsrc[i2];
-    const v2 dx = mk2((ra.x - B1.x) - t1.x, (ra.x - B2.x) - t2.x);
-    const v2 dy = mk2((ra.y - B1.y) - t1.y, (ra.y - B2.y) - t2.y);
-    const v2 dz = mk2((ra.z - B1.z) - t1.z, (ra.z - B2.z) - t2.z);
+    const v2 dx = mk2((float)(ra.x - P1.x), (float)(ra.x - P2.x));
+    const v2 dy = mk2((float)(ra.y - P1.y), (float)(ra.y - P2.y));
+    const v2 dz = mk2((float)(ra.z - P1.z), (float)(ra.z - P2.z));
     const v2 r2 = fma2(dx, dx, fma2(dy, dy, dz * dz));
-    v2 fs = pair_fs_pk<SAME, MHOMO>(T, Q, r2, mk2(B1.w, B2.w), mk2(D1, D2), dFX, kcqa, kcqaZY);
+    v2 fs = pair_fs_pk<SAME, MHOMO>(T, Q, r2, mk2((float)P1.w, (float)P2.w), mk2(D1, D2), dFX, kcqa, kcqaZY);
     fs = mk2(v1 ? fs.v.x : 0.f, v2ok ? fs.v.y : 0.f);   // slots past the end of a group: placeholders
     const v2 px = fs * dx, py = fs * dy, pz = fs * dz;
     two_sum2(fh[0], fl[0], px);
@@ -346,15 +402,15 @@ __device__ __forceinline__ void force_half_batch(const PackParams& Q, const floa
     two_sum2(fh[2], fl[2], pz);
     if (v1) {
         if (!(fabsf(px.v.x) < kForceMax && fabsf(py.v.x) < kForceMax && fabsf(pz.v.x) < kForceMax)) bad |= ST_POSITION;
-        add_fixed(ax + i1, -__float2ll_rn(px.v.x * kForceScale));
-        add_fixed(ay + i1, -__float2ll_rn(py.v.x * kForceScale));
-        add_fixed(az + i1, -__float2ll_rn(pz.v.x * kForceScale));
+        acc.add(0, i1, -__float2ll_rn(px.v.x * kForceScale));
+        acc.add(1, i1, -__float2ll_rn(py.v.x * kForceScale));
+        acc.add(2, i1, -__float2ll_rn(pz.v.x * kForceScale));
     }
     if (v2ok) {
         if (!(fabsf(px.v.y) < kForceMax && fabsf(py.v.y) < kForceMax && fabsf(pz.v.y) < kForceMax)) bad |= ST_POSITION;
-        add_fixed(ax + i2, -__float2ll_rn(px.v.y * kForceScale));
-        add_fixed(ay + i2, -__float2ll_rn(py.v.y * kForceScale));
-        add_fixed(az + i2, -__float2ll_rn(pz.v.y * kForceScale));
+        acc.add(0, i2, -__float2ll_rn(px.v.y * kForceScale));
+        acc.add(1, i2, -__float2ll_rn(py.v.y * kForceScale));
+        acc.add(2, i2, -__float2ll_rn(pz.v.y * kForceScale));
     }
     if (RDF) {
         // INT(r/dr) of the pair's FP32 distance, once per pair, under the
@@ -372,20 +428,22 @@ __device__ __forceinline__ void force_half_batch(const PackParams& Q, const floa
 }
 
 template <bool TILED, bool RDF>
-__device__ __forceinline__ void force_half_atoms(const PackParams& Q, const float4* etab, const float4* __restrict__ rsrc,
-                                                 const float* __restrict__ dsrc, int lim, int b0, int b1, int a0,
-                                                 int* next, const float4* __restrict__ frec, const int* __restrict__ ts,
+__device__ __forceinline__ void force_half_atoms(const Half2Params& H, const int* edelta, const double3* esh,
+                                                 const double4* __restrict__ psrc, const float* __restrict__ dsrc,
+                                                 int lim, int b0, int b1, int a0, int* next,
+                                                 const double4* __restrict__ xo, const int* __restrict__ ts,
                                                  const int2* __restrict__ nn, const unsigned* __restrict__ nbr,
-                                                 const float* __restrict__ dF_f, int g0, u64* ax, u64* ay, u64* az,
-                                                 int* hist, int& bad) {
+                                                 const float* __restrict__ dF_f, const Sink<TILED>& acc, int* hist,
+                                                 int& bad) {
     const int lane = threadIdx.x & 31;
-    const int cap = Q.cap;
+    const int cap = H.Q.cap;
+    const int g0 = H.g0;
     for (;;) {
         int X = 0;
         if (lane == 0) X = atomicAdd(next, 1);
         X = __shfl_sync(0xffffffffu, X, 0) + b0;
         if (X >= b1) break;
-        const float4 ra = frec[X];
+        const double4 ra = xo[X];
         const int sX = ts[X];
         const float dFX = dF_f[X];
         const int2 m = nn[X];
@@ -417,11 +475,11 @@ __device__ __forceinline__ void force_half_atoms(const PackParams& Q, const floa
                 const int kb = (g1 ? j - nb0 : j) << 6, mg = g1 ? m.y : m.x;
                 const bool v1 = kb + lane < mg, v2ok = kb + 32 + lane < mg;
                 if (metal) {
-                    if (!g1) force_half_batch<true, true, RDF, 0>(Q, etab, rsrc, dsrc, lim, E1, E2, v1, v2ok, ra, dFX, ax, ay, az, fh, fl, hist, bad);
-                    else force_half_batch<false, false, RDF, 1>(Q, etab, rsrc, dsrc, lim, E1, E2, v1, v2ok, ra, dFX, ax, ay, az, fh, fl, hist, bad);
+                    if (!g1) force_half_batch<true, true, RDF, TILED, 0>(H, edelta, esh, psrc, dsrc, lim, E1, E2, v1, v2ok, ra, dFX, acc, fh, fl, hist, bad);
+                    else force_half_batch<false, false, RDF, TILED, 1>(H, edelta, esh, psrc, dsrc, lim, E1, E2, v1, v2ok, ra, dFX, acc, fh, fl, hist, bad);
                 } else {
-                    if (!g1) force_half_batch<false, false, RDF, 2>(Q, etab, rsrc, dsrc, lim, E1, E2, v1, v2ok, ra, dFX, ax, ay, az, fh, fl, hist, bad);
-                    else force_half_batch<true, false, RDF, 3>(Q, etab, rsrc, dsrc, lim, E1, E2, v1, v2ok, ra, dFX, ax, ay, az, fh, fl, hist, bad);
+                    if (!g1) force_half_batch<false, false, RDF, TILED, 2>(H, edelta, esh, psrc, dsrc, lim, E1, E2, v1, v2ok, ra, dFX, acc, fh, fl, hist, bad);
+                    else force_half_batch<true, false, RDF, TILED, 3>(H, edelta, esh, psrc, dsrc, lim, E1, E2, v1, v2ok, ra, dFX, acc, fh, fl, hist, bad);
                 }
             }
         }
@@ -432,31 +490,33 @@ __device__ __forceinline__ void force_half_atoms(const PackParams& Q, const floa
         fy = warp_sum(fy);
         fz = warp_sum(fz);
         if (lane == 0) {
-            add_fixed(ax + slotX, __double2ll_rn(fx * kForceScaleD));
-            add_fixed(ay + slotX, __double2ll_rn(fy * kForceScaleD));
-            add_fixed(az + slotX, __double2ll_rn(fz * kForceScaleD));
+            acc.add(0, slotX, __double2ll_rn(fx * kForceScaleD));
+            acc.add(1, slotX, __double2ll_rn(fy * kForceScaleD));
+            acc.add(2, slotX, __double2ll_rn(fz * kForceScaleD));
         }
     }
 }
 
 template <bool RDF>
 __global__ void __launch_bounds__(kH2Threads, 1)
-    force_half_kernel(const __grid_constant__ PackParams Q, int splits, const int* __restrict__ cs_start,
-                      const int* __restrict__ cs_entries, const float4* __restrict__ frec,
+    force_half_kernel(const __grid_constant__ Half2Params H, const int* __restrict__ cs_start,
+                      const int* __restrict__ cs_entries, const double4* __restrict__ xo,
                       const int* __restrict__ ts, const int2* __restrict__ nn, const unsigned* __restrict__ nbr,
-                      const float* __restrict__ dF_f, int g0, int n, u64* __restrict__ f_fx, int fstride,
-                      int* __restrict__ rdf, int* __restrict__ status) {
+                      const float* __restrict__ dF_f, u64* __restrict__ f_fx, int* __restrict__ rdf,
+                      int* __restrict__ status) {
     constexpr int NB = SIMOX_NRDF + 2;
     extern __shared__ __align__(16) unsigned char half_smem[];
-    float4* trec = reinterpret_cast<float4*>(half_smem);
-    u64* tacc = reinterpret_cast<u64*>(trec + kH2Cap);
-    float* tdf = reinterpret_cast<float*>(tacc + 3 * kH2Cap);
-    __shared__ float4 etab[kEntries];          // o_e * Lcs (x, y, z) and tile index delta (w)
+    double4* tpos = reinterpret_cast<double4*>(half_smem);                 // partner offsets + shift, charge
+    unsigned* tlo = reinterpret_cast<unsigned*>(tpos + kH2Cap);            // [3][cap] low words
+    unsigned* thi = tlo + 3 * kH2Cap;                                      // [3][cap] high words
+    float* tdf = reinterpret_cast<float*>(thi + 3 * kH2Cap);               // F'
+    __shared__ double3 esh[kEntries];          // o_e * Lcs
+    __shared__ int edelta[kEntries];           // tile index delta of each stencil position
     __shared__ HalfTile T;
     __shared__ int next;
     __shared__ int hist[RDF ? 4 * NB : 1];     // (metal, O) x (metal, O) kinds of the reference's (i, j)
     const int tid = threadIdx.x;
-    const int cell = blockIdx.x / splits, part = blockIdx.x - cell * splits;
+    const int cell = blockIdx.x / H.splits, part = blockIdx.x - cell * H.splits;
     if (tid == 0) next = 0;
     if (RDF)
         for (int k = tid; k < 4 * NB; k += kH2Threads) hist[k] = 0;
@@ -464,41 +524,47 @@ __global__ void __launch_bounds__(kH2Threads, 1)
     const int total = T.off[kHalfCells];
     const bool tiled = total <= kH2Cap;
     if (tid < kEntries) {
-        const float4 o = Q.sh[tid];
+        esh[tid] = stencil_shift(tid, H.lcs);
         // positions below 13 never occur in a half row: a delta that the
         // range clamp maps to slot 0
-        const int d = tid < kHalfFirst ? -(1 << 28) : (tiled ? T.off[tid - kHalfFirst] - T.start[tid - kHalfFirst] : 0);
-        etab[tid] = make_float4(o.x, o.y, o.z, __int_as_float(d));
+        edelta[tid] = tid < kHalfFirst ? -(1 << 28) : (tiled ? T.off[tid - kHalfFirst] - T.start[tid - kHalfFirst] : 0);
     }
+    __syncthreads();
     if (tiled) {
         int t = 0;
         for (int i = tid; i < total; i += kH2Threads) {
             while (T.off[t + 1] <= i) t++;
             const int src = T.start[t] + (i - T.off[t]);
-            cp_async16(&trec[i], frec + src);
-            cp_async4(&tdf[i], dF_f + src);
-            tacc[i] = 0ull;
-            tacc[kH2Cap + i] = 0ull;
-            tacc[2 * kH2Cap + i] = 0ull;
+            const double3 sh = esh[kHalfFirst + t];
+            double4 p = xo[src];
+            p.x += sh.x;
+            p.y += sh.y;
+            p.z += sh.z;
+            tpos[i] = p;
+            tdf[i] = dF_f[src];
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                tlo[c * kH2Cap + i] = 0u;
+                thi[c * kH2Cap + i] = 0u;
+            }
         }
-        cp_async_commit();
-        cp_async_wait<0>();
     }
     __syncthreads();
     const int a0 = T.start[0], na = T.off[1];
-    const int b0 = a0 + (int)((long long)na * part / splits);
-    const int b1 = a0 + (int)((long long)na * (part + 1) / splits);
+    const int b0 = a0 + (int)((long long)na * part / H.splits);
+    const int b1 = a0 + (int)((long long)na * (part + 1) / H.splits);
     int bad = 0;
     if (tiled)
-        force_half_atoms<true, RDF>(Q, etab, trec, tdf, total, b0, b1, a0, &next, frec, ts, nn, nbr, dF_f, g0, tacc,
-                                    tacc + kH2Cap, tacc + 2 * kH2Cap, hist, bad);
+        force_half_atoms<true, RDF>(H, edelta, esh, tpos, tdf, total, b0, b1, a0, &next, xo, ts, nn, nbr, dF_f,
+                                    Sink<true>{tlo, thi, kH2Cap}, hist, bad);
     else
-        force_half_atoms<false, RDF>(Q, etab, frec, dF_f, n, b0, b1, a0, &next, frec, ts, nn, nbr, dF_f, g0, f_fx,
-                                     f_fx + fstride, f_fx + 2 * fstride, hist, bad);
+        force_half_atoms<false, RDF>(H, edelta, esh, xo, dF_f, H.n, b0, b1, a0, &next, xo, ts, nn, nbr, dF_f,
+                                     Sink<false>{f_fx, H.fstride}, hist, bad);
     if (bad) atomicOr(status, bad);
     __syncthreads();
-    if (tiled) half_tile_flush(T, total, tacc, kH2Cap, 3, f_fx, fstride);
+    if (tiled) half_tile_flush_split(T, total, tlo, thi, kH2Cap, 3, f_fx, H.fstride);
     if (RDF) {
+        const int g0 = H.g0;
         for (int k = tid; k < 4 * NB; k += kH2Threads) {
             const int v = hist[k];
             if (v) {
@@ -564,15 +630,16 @@ __device__ __forceinline__ void ctip_pair_pk(const CtipHalfTab& T, const CtipHal
     ay_ = bc(C.kc) * (bc(-1.f) * eY * (ir + bc(T.xiy)) - fifj);
 }
 
-template <bool WITH_C, int TI>
+template <bool WITH_C, bool TILED, int TI>
 __device__ __forceinline__ void ctip_half_batch(const CtipHalfParams& C, const float4* etab,
                                                 const float4* __restrict__ rsrc, const double* __restrict__ vsrc,
                                                 int lim, unsigned E1, unsigned E2, bool v1, bool v2ok,
-                                                const float4& ra, double vX, u64* ao, u64* ac, double& sr, double& cz) {
+                                                const float4& ra, float vXf, const Sink<TILED>& acc, double& sr,
+                                                double& cz) {
     const CtipHalfTab& T = C.tab[TI];
     constexpr bool SAME = TI == 0 || TI == 3;
-    const float4 t1 = etab[(E1 >> kSkinCodeShift) & kCodeMask];
-    const float4 t2 = etab[(E2 >> kSkinCodeShift) & kCodeMask];
+    const float4 t1 = etab[min((int)((E1 >> kSkinCodeShift) & kCodeMask), kEntries - 1)];
+    const float4 t2 = etab[min((int)((E2 >> kSkinCodeShift) & kCodeMask), kEntries - 1)];
     int i1 = (int)(E1 & kIdxMask) + __float_as_int(t1.w);
     int i2 = (int)(E2 & kIdxMask) + __float_as_int(t2.w);
     i1 = (unsigned)i1 < (unsigned)lim ? i1 : 0;
@@ -584,20 +651,21 @@ __device__ __forceinline__ void ctip_half_batch(const CtipHalfParams& C, const f
     const v2 r2 = fma2(dx, dx, fma2(dy, dy, dz * dz));
     v2 sym, axy, ayx;
     ctip_pair_pk<SAME>(T, C, r2, sym, axy, ayx);
+    const v2 sv = sym * bc(vXf * kRhoScale);        // Y's share sym v_X, scaled
     if (v1) {
         sr = fma((double)sym.v.x, vsrc[i1], sr);
-        add_fixed(ao + i1, __double2ll_rn((double)sym.v.x * vX * kRhoScaleD));
+        acc.add(0, i1, __float2ll_rn(sv.v.x));
         if (WITH_C) {
             cz += (double)(T.ZY * axy.v.x);
-            add_fixed(ac + i1, __float2ll_rn(T.ZX * ayx.v.x * kRhoScale));
+            acc.add(1, i1, __float2ll_rn(T.ZX * ayx.v.x * kRhoScale));
         }
     }
     if (v2ok) {
         sr = fma((double)sym.v.y, vsrc[i2], sr);
-        add_fixed(ao + i2, __double2ll_rn((double)sym.v.y * vX * kRhoScaleD));
+        acc.add(0, i2, __float2ll_rn(sv.v.y));
         if (WITH_C) {
             cz += (double)(T.ZY * axy.v.y);
-            add_fixed(ac + i2, __float2ll_rn(T.ZX * ayx.v.y * kRhoScale));
+            acc.add(1, i2, __float2ll_rn(T.ZX * ayx.v.y * kRhoScale));
         }
     }
 }
@@ -608,7 +676,7 @@ __device__ __forceinline__ void ctip_half_atoms(const CtipHalfParams& C, const f
                                                 int lim, int b0, int b1, int a0, int* next,
                                                 const float4* __restrict__ frec, const int* __restrict__ ts,
                                                 const double* __restrict__ vin, const int2* __restrict__ nn,
-                                                const unsigned* __restrict__ nbr, u64* ao, u64* ac) {
+                                                const unsigned* __restrict__ nbr, const Sink<TILED>& acc) {
     const int lane = threadIdx.x & 31;
     const int cap = C.cap;
     for (;;) {
@@ -619,6 +687,7 @@ __device__ __forceinline__ void ctip_half_atoms(const CtipHalfParams& C, const f
         const float4 ra = frec[X];
         const int sX = ts[X];
         const double vX = vin[X];
+        const float vXf = (float)vX;
         const int2 m = nn[X];
         const unsigned* row = nbr + (size_t)X * cap;
         const bool metal = sX == C.g0;
@@ -627,27 +696,36 @@ __device__ __forceinline__ void ctip_half_atoms(const CtipHalfParams& C, const f
         if (metal || sX == 3) {
             const int nb0 = (m.x + 63) >> 6, nb = nb0 + ((m.y + 63) >> 6);
             const unsigned pad = ((unsigned)kSelf << kSkinCodeShift) | (unsigned)X;
-            for (int j = 0; j < nb; j++) {
+            // the next batch's entries are loaded before this batch's arithmetic
+            auto load = [&](int j, unsigned& a, unsigned& b) {
                 const bool g1 = j >= nb0;
                 const int kb = (g1 ? j - nb0 : j) << 6, mg = g1 ? m.y : m.x;
                 const unsigned* p = g1 ? row + (cap - 1 - kb - lane) : row + kb + lane;
+                a = kb + lane < mg ? p[0] : pad;
+                b = kb + 32 + lane < mg ? p[g1 ? -32 : 32] : pad;
+            };
+            unsigned na = pad, nbE = pad;
+            if (nb > 0) load(0, na, nbE);
+            for (int j = 0; j < nb; j++) {
+                const unsigned E1 = na, E2 = nbE;
+                if (j + 1 < nb) load(j + 1, na, nbE);
+                const bool g1 = j >= nb0;
+                const int kb = (g1 ? j - nb0 : j) << 6, mg = g1 ? m.y : m.x;
                 const bool v1 = kb + lane < mg, v2ok = kb + 32 + lane < mg;
-                const unsigned E1 = v1 ? p[0] : pad;
-                const unsigned E2 = v2ok ? p[g1 ? -32 : 32] : pad;
                 if (metal) {
-                    if (!g1) ctip_half_batch<WITH_C, 0>(C, etab, rsrc, vsrc, lim, E1, E2, v1, v2ok, ra, vX, ao, ac, sr, cz);
-                    else ctip_half_batch<WITH_C, 1>(C, etab, rsrc, vsrc, lim, E1, E2, v1, v2ok, ra, vX, ao, ac, sr, cz);
+                    if (!g1) ctip_half_batch<WITH_C, TILED, 0>(C, etab, rsrc, vsrc, lim, E1, E2, v1, v2ok, ra, vXf, acc, sr, cz);
+                    else ctip_half_batch<WITH_C, TILED, 1>(C, etab, rsrc, vsrc, lim, E1, E2, v1, v2ok, ra, vXf, acc, sr, cz);
                 } else {
-                    if (!g1) ctip_half_batch<WITH_C, 2>(C, etab, rsrc, vsrc, lim, E1, E2, v1, v2ok, ra, vX, ao, ac, sr, cz);
-                    else ctip_half_batch<WITH_C, 3>(C, etab, rsrc, vsrc, lim, E1, E2, v1, v2ok, ra, vX, ao, ac, sr, cz);
+                    if (!g1) ctip_half_batch<WITH_C, TILED, 2>(C, etab, rsrc, vsrc, lim, E1, E2, v1, v2ok, ra, vXf, acc, sr, cz);
+                    else ctip_half_batch<WITH_C, TILED, 3>(C, etab, rsrc, vsrc, lim, E1, E2, v1, v2ok, ra, vXf, acc, sr, cz);
                 }
             }
         }
         sr = warp_sum(sr);
         if (WITH_C) cz = warp_sum(cz);
         if (lane == 0) {
-            add_fixed(ao + slotX, __double2ll_rn(sr * kRhoScaleD));
-            if (WITH_C) add_fixed(ac + slotX, __double2ll_rn(cz * kRhoScaleD));
+            acc.add(0, slotX, __double2ll_rn(sr * kRhoScaleD));
+            if (WITH_C) acc.add(1, slotX, __double2ll_rn(cz * kRhoScaleD));
         }
     }
 }
@@ -661,7 +739,8 @@ __global__ void __launch_bounds__(kH2Threads, 1)
     extern __shared__ __align__(16) unsigned char ctip_smem[];
     float4* trec = reinterpret_cast<float4*>(ctip_smem);
     double* tv = reinterpret_cast<double*>(trec + kHCCap);
-    u64* tacc = reinterpret_cast<u64*>(tv + kHCCap);
+    unsigned* tlo = reinterpret_cast<unsigned*>(tv + kHCCap);   // [2][cap]
+    unsigned* thi = tlo + 2 * kHCCap;                             // [2][cap]
     __shared__ float4 etab[kEntries];
     __shared__ HalfTile T;
     __shared__ int next;
@@ -683,8 +762,12 @@ __global__ void __launch_bounds__(kH2Threads, 1)
             const int src = T.start[t] + (i - T.off[t]);
             cp_async16(&trec[i], frec + src);
             tv[i] = vin[src];
-            tacc[i] = 0ull;
-            if (WITH_C) tacc[kHCCap + i] = 0ull;
+            tlo[i] = 0u;
+            thi[i] = 0u;
+            if (WITH_C) {
+                tlo[kHCCap + i] = 0u;
+                thi[kHCCap + i] = 0u;
+            }
         }
         cp_async_commit();
         cp_async_wait<0>();
@@ -694,13 +777,13 @@ __global__ void __launch_bounds__(kH2Threads, 1)
     const int b0 = a0 + (int)((long long)na * part / C.splits);
     const int b1 = a0 + (int)((long long)na * (part + 1) / C.splits);
     if (tiled)
-        ctip_half_atoms<WITH_C, true>(C, etab, trec, tv, total, b0, b1, a0, &next, frec, ts, vin, nn, nbr, tacc,
-                                      tacc + kHCCap);
+        ctip_half_atoms<WITH_C, true>(C, etab, trec, tv, total, b0, b1, a0, &next, frec, ts, vin, nn, nbr,
+                                      Sink<true>{tlo, thi, kHCCap});
     else
-        ctip_half_atoms<WITH_C, false>(C, etab, frec, vin, C.n, b0, b1, a0, &next, frec, ts, vin, nn, nbr, gacc,
-                                       gacc + gstride);
+        ctip_half_atoms<WITH_C, false>(C, etab, frec, vin, C.n, b0, b1, a0, &next, frec, ts, vin, nn, nbr,
+                                       Sink<false>{gacc, gstride});
     __syncthreads();
-    if (tiled) half_tile_flush(T, total, tacc, kHCCap, WITH_C ? 2 : 1, gacc, gstride);
+    if (tiled) half_tile_flush_split(T, total, tlo, thi, kHCCap, WITH_C ? 2 : 1, gacc, gstride);
 }
 
 // out = fixed-point sums; cconst = chi + the fixed-point asym sums
@@ -830,8 +913,9 @@ int filter_density_half(simox_ctx* c) {
 int force_half(simox_ctx* c, bool rdf) {
     if (int st = half_prepare(c->device)) return st;
     PairParams P = pair_params(c);
-    PackParams Q;
-    std::memset(&Q, 0, sizeof(Q));
+    Half2Params H;
+    std::memset(&H, 0, sizeof(H));
+    PackParams& Q = H.Q;
     Q.pa = (float)(kErfcP * P.a);
     Q.na2l = (float)(-P.a * P.a * 1.4426950408889634);
     Q.tas = (float)(2.0 * P.a / SX_SQRTPI);
@@ -844,24 +928,28 @@ int force_half(simox_ctx* c, bool rdf) {
     Q.tab[1] = pack_tab(c->pot, g0, 3);
     Q.tab[2] = pack_tab(c->pot, 3, g0);
     Q.tab[3] = pack_tab(c->pot, 3, 3);
-    const int splits = std::max(1, std::min(16, c->force_splits));
-    const int fstride = c->cap;
-    cudaMemsetAsync(c->fx_acc, 0, sizeof(u64) * 3 * (size_t)fstride, c->stream);
+    H.lcs = make_double3(c->lcs[0], c->lcs[1], c->lcs[2]);
+    H.splits = std::max(1, std::min(16, c->force_splits));
+    H.g0 = g0;
+    H.n = c->n;
+    H.fstride = c->cap;
+    cudaMemsetAsync(c->fx_acc, 0, sizeof(u64) * 3 * (size_t)H.fstride, c->stream);
     {
         Launch L(c, "pair_force");
+        const int g = c->ncell_s * H.splits;
         if (rdf)
-            force_half_kernel<true><<<c->ncell_s * splits, kH2Threads, kH2Smem, c->stream>>>(
-                Q, splits, c->cs_start, c->cs_entries, c->frec_s, c->t_s, reinterpret_cast<const int2*>(c->nn),
-                c->nbr, c->dF_f, g0, c->n, c->fx_acc, fstride, c->rdf, c->status);
+            force_half_kernel<true><<<g, kH2Threads, kH2Smem, c->stream>>>(
+                H, c->cs_start, c->cs_entries, c->xo_s, c->t_s, reinterpret_cast<const int2*>(c->nn), c->nbr,
+                c->dF_f, c->fx_acc, c->rdf, c->status);
         else
-            force_half_kernel<false><<<c->ncell_s * splits, kH2Threads, kH2Smem, c->stream>>>(
-                Q, splits, c->cs_start, c->cs_entries, c->frec_s, c->t_s, reinterpret_cast<const int2*>(c->nn),
-                c->nbr, c->dF_f, g0, c->n, c->fx_acc, fstride, c->rdf, c->status);
+            force_half_kernel<false><<<g, kH2Threads, kH2Smem, c->stream>>>(
+                H, c->cs_start, c->cs_entries, c->xo_s, c->t_s, reinterpret_cast<const int2*>(c->nn), c->nbr,
+                c->dF_f, c->fx_acc, c->rdf, c->status);
     }
     {
         Launch L(c, "pair_force_finalize");
-        force_half_finalize_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->n, c->fx_acc, fstride, c->pair_order,
-                                                                               c->f);
+        force_half_finalize_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->n, c->fx_acc, H.fstride,
+                                                                               c->pair_order, c->f);
     }
     return check_launch(c);
 }
@@ -904,8 +992,7 @@ static CtipHalfTab ctip_half_tab(const simox_potential& P, int X, int Y) {
     return t;
 }
 
-int ctip_pair_half(simox_ctx* c, const double* vin, double* out, double* cconst, const CtipSpecies& S) {
-    if (int st = half_prepare(c->device)) return st;
+static CtipHalfParams ctip_half_params(const simox_ctx* c) {
     CtipHalfParams C;
     std::memset(&C, 0, sizeof(C));
     C.pa = (float)(kErfcP * c->a);
@@ -921,6 +1008,24 @@ int ctip_pair_half(simox_ctx* c, const double* vin, double* out, double* cconst,
     C.tab[1] = ctip_half_tab(c->pot, g0, 3);
     C.tab[2] = ctip_half_tab(c->pot, 3, g0);
     C.tab[3] = ctip_half_tab(c->pot, 3, 3);
+    return C;
+}
+
+double ctip_half_unit() { return kRhoUnit; }
+
+int ctip_half_launch(simox_ctx* c, const double* vin, cudaStream_t s) {
+    if (int st = half_prepare(c->device)) return st;
+    const CtipHalfParams C = ctip_half_params(c);
+    Launch L(c, "ctip_matvec_pairs");
+    ctip_half_kernel<false><<<c->ncell_s * C.splits, kH2Threads, kHCSmem, s>>>(
+        C, c->cs_start, c->cs_entries, c->frec_s, c->t_s, reinterpret_cast<const int2*>(c->nn), c->nbr, vin,
+        c->fx_acc, c->cap);
+    return check_launch(c);
+}
+
+int ctip_pair_half(simox_ctx* c, const double* vin, double* out, double* cconst, const CtipSpecies& S) {
+    if (int st = half_prepare(c->device)) return st;
+    const CtipHalfParams C = ctip_half_params(c);
     const int gstride = c->cap;
     cudaMemsetAsync(c->fx_acc, 0, sizeof(u64) * (cconst ? 2 : 1) * (size_t)gstride, c->stream);
     const int g = c->ncell_s * C.splits;

@@ -363,6 +363,59 @@ __global__ void __launch_bounds__(128)
     phi[k] = scale * sum;
 }
 
+// The potential gather of PHI_MESH (ctip.f90:381-393) fused with the end of
+// the charge solver's matrix-vector product: Ap = scale phi(p) + J' p + sr,
+// the dots g.p and p.Ap and the atoms whose charge can cross a bound for a
+// step in [-1, 1] (the Brent line search's active set).
+template <typename R, int P>
+__global__ void __launch_bounds__(128)
+    gather_pot_ctip_kernel(PmeParams S, const double4* __restrict__ xq, const R* __restrict__ grid, double scale,
+                           CtipFinish F) {
+    __shared__ double red[128 / 32];
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    double gp = 0.0, pap = 0.0;
+    if (k < S.n) {
+        const double4 a = xq[k];
+        double wx[P], wy[P], wz[P], d[P];
+        const double ux = (double)S.K.x * (a.x + S.box.x * 0.5) / S.box.x;
+        const double uy = (double)S.K.y * (a.y + S.box.y * 0.5) / S.box.y;
+        const double uz = (double)S.K.z * (a.z + S.box.z * 0.5) / S.box.z;
+        bspline_w<P>(ux, wx, d);
+        bspline_w<P>(uy, wy, d);
+        bspline_w<P>(uz, wz, d);
+        const int bx = __double2int_rz(ux) - P / 2 + 1;
+        const int by = __double2int_rz(uy) - P / 2 + 1;
+        const int bz = __double2int_rz(uz) - P / 2 + 1;
+        int ix[P];
+#pragma unroll
+        for (int s = 0; s < P; s++) ix[s] = wrapi(bx + s, S.K.x);
+        double sum = 0.0;
+#pragma unroll
+        for (int c = 0; c < P; c++) {
+            const size_t gz = (size_t)wrapi(bz + c, S.K.z) * S.K.y;
+#pragma unroll
+            for (int b = 0; b < P; b++) {
+                const size_t gyz = (gz + wrapi(by + b, S.K.y)) * S.K.x;
+                R tw = 0;
+#pragma unroll
+                for (int aa = 0; aa < P; aa++) tw += (R)wx[aa] * grid[gyz + ix[aa]];
+                sum += (double)tw * wy[b] * wz[c];
+            }
+        }
+        const int sp = min(F.ts[k], 4);
+        const double p = F.pv[k];
+        const double sr = (double)(long long)F.sr_fx[k] * F.sr_unit;
+        const double ap = scale * sum + F.S.Jp[sp] * p + sr;
+        F.Ap[k] = ap;
+        gp = F.g[k] * p;
+        pap = p * ap;
+        const double qi = F.q[k], ab = fabs(p);
+        if (qi - ab < F.S.qmin[sp] || qi + ab > F.S.qmax[sp]) F.act[atomicAdd(F.nact, 1)] = k;
+    }
+    block_add<128>(gp, F.acc, A_GP, red);
+    block_add<128>(pap, F.acc, A_PAP, red);
+}
+
 // psi(m) = exp(-pi^2 m2/a^2)/m2, m = 0 -> 0   (force.f90:500-514)
 __global__ void psi_kernel(int3 K, double3 box, double a2, double* __restrict__ psi) {
     const size_t N = (size_t)K.x * K.y * K.z;
@@ -824,6 +877,46 @@ int pme_potential(simox_ctx* c, const double* qalt, double* phi, double scale) {
         default: return SIMOX_E_ARG;
     }
     if (st) return st;
+    return check_launch(c);
+}
+
+template <typename R, int P>
+static int pme_grid_t(simox_ctx* c, PmeRes& Rs, const double* qalt) {
+    PmeParams S = pme_params(c);
+    run_spread<R, P>(c, Rs, S, qalt);
+    return run_convolution(c, Rs, false);
+}
+
+int pme_potential_grid(simox_ctx* c, const double* qalt) {
+    if (!c->psi_valid) return SIMOX_E_STATE;
+    if (c->n == 0) return SIMOX_OK;
+    PmeRes& Rs = c->pme[1].ready ? c->pme[1] : c->pme[0];
+    int st;
+    switch (c->order) {
+        case 4: st = Rs.dbl ? pme_grid_t<double, 4>(c, Rs, qalt) : pme_grid_t<float, 4>(c, Rs, qalt); break;
+        case 6: st = Rs.dbl ? pme_grid_t<double, 6>(c, Rs, qalt) : pme_grid_t<float, 6>(c, Rs, qalt); break;
+        case 8: st = Rs.dbl ? pme_grid_t<double, 8>(c, Rs, qalt) : pme_grid_t<float, 8>(c, Rs, qalt); break;
+        default: return SIMOX_E_ARG;
+    }
+    return st ? st : check_launch(c);
+}
+
+template <typename R, int P>
+static void finish_t(simox_ctx* c, PmeRes& Rs, double scale, const CtipFinish& F) {
+    PmeParams S = pme_params(c);
+    gather_pot_ctip_kernel<R, P><<<(S.n + 127) / 128, 128, 0, c->stream>>>(S, c->xq_s, (const R*)Rs.grid, scale, F);
+}
+
+int pme_potential_finish(simox_ctx* c, double scale, const CtipFinish& F) {
+    if (c->n == 0) return SIMOX_OK;
+    PmeRes& Rs = c->pme[1].ready ? c->pme[1] : c->pme[0];
+    Launch L(c, "ctip_matvec_finish");
+    switch (c->order) {
+        case 4: Rs.dbl ? finish_t<double, 4>(c, Rs, scale, F) : finish_t<float, 4>(c, Rs, scale, F); break;
+        case 6: Rs.dbl ? finish_t<double, 6>(c, Rs, scale, F) : finish_t<float, 6>(c, Rs, scale, F); break;
+        case 8: Rs.dbl ? finish_t<double, 8>(c, Rs, scale, F) : finish_t<float, 8>(c, Rs, scale, F); break;
+        default: return SIMOX_E_ARG;
+    }
     return check_launch(c);
 }
 

@@ -35,7 +35,8 @@ constexpr unsigned kCodeMask = 31u;
 enum : int {
     ST_CELL_OVERFLOW = 1, ST_NBR_OVERFLOW = 2, ST_UNKNOWN_PAIR = 4, ST_UNKNOWN_ELEMENT = 8,
     ST_POSITION = 16, ST_UNSUPPORTED = 32, ST_LINE_NOBRACKET = 64,  // Brent: 100 steps without convergence
-    ST_RNG = 128                                                     // thermostat: 100 rejected draws
+    ST_RNG = 128,                                                    // thermostat: 100 rejected draws
+    ST_SYNC = 256                                                    // a grid-wide wait gave up
 };
 
 // Slots of the FP64 accumulator array (energies and reductions).
@@ -164,6 +165,7 @@ struct simox_ctx {
     unsigned long long md_step_no = 0;   // md_run's current step: the stochastic thermostat's draw counter
     sx::AdjointState* adj = nullptr;   // parameter-adjoint model (simox_set_eam_spline)
     bool adj_warm = false;             // adjoint: refine the held charges by Newton, no CG first
+    bool coop_brent = true;            // the charge solver's line search as one cooperative grid
     bool spline_on = false;
 
     // species present
@@ -217,6 +219,8 @@ struct simox_ctx {
     int* t_s = nullptr;         // species 0..4
     float4* rec_s = nullptr;    // skin filter record in pair order: skin-cell offset, (cell, species)
     float4* frec_s = nullptr;   // skin force record in pair order: skin-cell offset, charge
+    double4* xo_s = nullptr;    // the same offset in FP64 (x, y, z) and the charge (w): the
+                                // half-list force pass forms separations from it in FP64
     int g0_species = -1;        // the one non-oxygen species present, or -1
     bool rho_ready = false;     // rho/F' of the filter pass are current (context precision)
 
@@ -351,9 +355,31 @@ struct CtipSpecies {
 
 int ctip_solve(simox_ctx* c, int max_cg, simox_ctip_report* rep, double tol = 1.0e-3);
 CtipSpecies ctip_species(const simox_ctx* c);
+// The end of one charge-solver matrix-vector product, fused into the PME
+// potential gather: Ap = scale phi(p) + J' p + sr (sr from fixed-point sums
+// of the half-list pair kernel), the dots g.p and p.Ap, the active set.
+struct CtipFinish {
+    const int* ts;
+    const double* q;
+    const double* g;
+    const double* pv;
+    const unsigned long long* sr_fx;   // sum_Y sym_XY p_Y, fixed point
+    double sr_unit;                    // its scale
+    double* Ap;
+    int* act;
+    int* nact;
+    double* acc;
+    CtipSpecies S;
+};
+// spread + convolution of qalt (no gather), then the fused gather + finish
+int pme_potential_grid(simox_ctx* c, const double* qalt);
+int pme_potential_finish(simox_ctx* c, double scale, const CtipFinish& F);
 // out = sum_Y sym_XY vin_Y (sorted order); cconst (may be null) = chi + sum_Y Z_Y asym_XY
 void ctip_pair(simox_ctx* c, const double* vin, double* out, double* cconst, const CtipSpecies& S);
 int ctip_pair_half(simox_ctx* c, const double* vin, double* out, double* cconst, const CtipSpecies& S);
+// the half-list pair kernel alone (sums into c->fx_acc, which the caller zeroes) on stream s
+int ctip_half_launch(simox_ctx* c, const double* vin, cudaStream_t s);
+double ctip_half_unit();
 int ctip_alloc(simox_ctx* c);
 // integrate.cu
 int vv1(simox_ctx* c, double dt, bool reflect);

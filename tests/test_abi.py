@@ -27,7 +27,7 @@ def test_library_exports_every_symbol(simox_lib):
 
 
 def test_status_strings_match(simox_lib):
-    for code in range(0, -20, -1):
+    for code in range(0, -21, -1):
         assert simox_lib.simox_status_string(code).decode() == _abi.status_text(code)
 
 
