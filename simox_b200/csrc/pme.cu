@@ -241,6 +241,108 @@ __global__ void __launch_bounds__(SP_THREADS)
     }
 }
 
+// Owner spread (skin-cell pair order).  Skin cell (ci, cj, ck) of an
+// ncs-grid owns the grid points g with ceil(ci K / ncs) <= g < ceil((ci+1) K
+// / ncs) on each axis, so every point has exactly one owner.  Its CTA takes
+// the atoms of the 27 cells around it, places each in its own frame (the
+// atom's wrap relative to its listed cell plus the stencil cell's periodic
+// shift, whole multiples of K), and adds q W of the stencil points it owns
+// into 64-bit fixed-point sums (2^50 units) in shared memory, held as
+// carry-linked 32-bit word pairs; the sums are exact, so the grid does not
+// depend on the order of the adds.  The owned points are then stored once:
+// no clearing of the grid and no global atomics.  The weights are those of
+// the reference formula on the atom's own coordinate, so each atom's
+// contribution equals the other spreads' term for term.
+constexpr int SO_THREADS = 256;
+constexpr double kSpreadScale = 1125899906842624.0;        // 2^50
+constexpr double kSpreadUnit = 1.0 / 1125899906842624.0;
+
+struct SpreadOwner {
+    int3 ncs;
+    double3 lcs;               // skin-cell edges
+};
+
+template <typename R, int P>
+__global__ void __launch_bounds__(SO_THREADS)
+    spread_owner_kernel(PmeParams S, SpreadOwner O, const int* __restrict__ cs_start,
+                        const int* __restrict__ cs_entries, const double4* __restrict__ xq,
+                        const double4* __restrict__ xo, const double* __restrict__ qalt, R* __restrict__ grid,
+                        int round_weights) {
+    extern __shared__ unsigned sow[];   // [npts] low words, [npts] high words
+    const int cell = blockIdx.x;
+    const int ci = cell % O.ncs.x, cj = (cell / O.ncs.x) % O.ncs.y, ck = cell / (O.ncs.x * O.ncs.y);
+    const int x0 = (ci * S.K.x + O.ncs.x - 1) / O.ncs.x, x1 = ((ci + 1) * S.K.x + O.ncs.x - 1) / O.ncs.x;
+    const int y0 = (cj * S.K.y + O.ncs.y - 1) / O.ncs.y, y1 = ((cj + 1) * S.K.y + O.ncs.y - 1) / O.ncs.y;
+    const int z0 = (ck * S.K.z + O.ncs.z - 1) / O.ncs.z, z1 = ((ck + 1) * S.K.z + O.ncs.z - 1) / O.ncs.z;
+    const int ex = x1 - x0, ey = y1 - y0, ez = z1 - z0, np = ex * ey * ez;
+    unsigned* lo = sow;
+    unsigned* hi = sow + np;
+    for (int i = threadIdx.x; i < 2 * np; i += SO_THREADS) sow[i] = 0u;
+    __syncthreads();
+    for (int e = 0; e < 27; e++) {
+        const int nc = cs_entries[cell * 27 + e];
+        const int di = e % 3 - 1, dj = (e / 3) % 3 - 1, dk = e / 9 - 1;
+        // the stencil cell's periodic shift in grid units
+        const int sx = ci + di < 0 ? -S.K.x : (ci + di >= O.ncs.x ? S.K.x : 0);
+        const int sy = cj + dj < 0 ? -S.K.y : (cj + dj >= O.ncs.y ? S.K.y : 0);
+        const int sz = ck + dk < 0 ? -S.K.z : (ck + dk >= O.ncs.z ? S.K.z : 0);
+        const int ni = nc % O.ncs.x, nj = (nc / O.ncs.x) % O.ncs.y, nk = nc / (O.ncs.x * O.ncs.y);
+        const double cx = -0.5 * S.box.x + (ni + 0.5) * O.lcs.x;
+        const double cy = -0.5 * S.box.y + (nj + 0.5) * O.lcs.y;
+        const double cz = -0.5 * S.box.z + (nk + 0.5) * O.lcs.z;
+        const int k1 = cs_start[nc + 1];
+        for (int k = cs_start[nc] + threadIdx.x; k < k1; k += SO_THREADS) {
+            const double4 a = xq[k];
+            const double q = qalt ? qalt[k] : a.w;
+            if (q == 0.0) continue;
+            const double4 o = xo[k];
+            // the atom's wrap relative to its listed cell (VV_NVE1 wraps positions, the cell lists stay)
+            const int mx = (int)rint((cx + o.x - a.x) / S.box.x) * S.K.x + sx;
+            const int my = (int)rint((cy + o.y - a.y) / S.box.y) * S.K.y + sy;
+            const int mz = (int)rint((cz + o.z - a.z) / S.box.z) * S.K.z + sz;
+            const double ux = (double)S.K.x * (a.x + S.box.x * 0.5) / S.box.x;
+            const double uy = (double)S.K.y * (a.y + S.box.y * 0.5) / S.box.y;
+            const double uz = (double)S.K.z * (a.z + S.box.z * 0.5) / S.box.z;
+            const int bx = __double2int_rz(ux) - P / 2 + 1 + mx - x0;
+            const int by = __double2int_rz(uy) - P / 2 + 1 + my - y0;
+            const int bz = __double2int_rz(uz) - P / 2 + 1 + mz - z0;
+            if (bx >= ex || bx + P <= 0 || by >= ey || by + P <= 0 || bz >= ez || bz + P <= 0) continue;
+            double wx[P], wy[P], wz[P], d[P];
+            bspline_w<P>(ux, wx, d);
+            bspline_w<P>(uy, wy, d);
+            bspline_w<P>(uz, wz, d);
+#pragma unroll
+            for (int c = 0; c < P; c++) {
+                const int gz = bz + c;
+                if (gz < 0 || gz >= ez) continue;
+#pragma unroll
+                for (int b = 0; b < P; b++) {
+                    const int gy = by + b;
+                    if (gy < 0 || gy >= ey) continue;
+                    const int row = (gz * ey + gy) * ex;
+#pragma unroll
+                    for (int aa = 0; aa < P; aa++) {
+                        const int gx = bx + aa;
+                        if (gx < 0 || gx >= ex) continue;
+                        double w = wx[aa] * wy[b] * wz[c];
+                        if (round_weights) w = (double)(float)w;   // CMPLX() default kind, force.f90:406
+                        const long long v = __double2ll_rn(q * w * kSpreadScale);
+                        const unsigned vl = (unsigned)v, vh = (unsigned)((unsigned long long)v >> 32);
+                        const unsigned old = atomicAdd(lo + row + gx, vl);
+                        atomicAdd(hi + row + gx, vh + ((unsigned)(old + vl) < old ? 1u : 0u));
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < np; i += SO_THREADS) {
+        const int gx = i % ex, gy = (i / ex) % ey, gz = i / (ex * ey);
+        const long long v = (long long)(((unsigned long long)hi[i] << 32) | lo[i]);
+        grid[((size_t)(z0 + gz) * S.K.y + (y0 + gy)) * S.K.x + (x0 + gx)] = (R)((double)v * kSpreadUnit);
+    }
+}
+
 // half-spectrum multiply by G/N and energy sum_k G |Q^|^2 (Hermitian weights)
 template <typename R>
 __global__ void __launch_bounds__(256)
@@ -591,8 +693,46 @@ static bool spread_tile_ready(int device) {
     return done[device].load();
 }
 
+// owner-spread shared memory (two 32-bit words per owned point) of this
+// context's skin grid, or 0 when the owner spread does not apply: the pair
+// order must be the skin order, and a stencil (p/2 points on either side of
+// an atom, which may sit up to skin/2 outside its cell) must not reach past
+// the neighbouring cells
+static size_t owner_smem(const simox_ctx* c) {
+    if (!(c->using_skin && c->pair_order == c->perm)) return 0;
+    size_t np = 1;
+    for (int d = 0; d < 3; d++) {
+        const int per = c->fft[d] / c->ncs[d];                    // fewest points a cell owns
+        const double skin_pts = 0.5 * c->skin * c->fft[d] / c->box[d];
+        if (c->order / 2 + 2 + skin_pts > per) return 0;
+        np *= (size_t)((c->fft[d] + c->ncs[d] - 1) / c->ncs[d]);   // most points a cell owns
+    }
+    const size_t b = 2 * sizeof(unsigned) * np;
+    return b <= (size_t)200 * 1024 ? b : 0;
+}
+
+template <typename R, int P>
+static bool owner_ready(int device) {
+    static std::atomic<bool> done[64] = {};   // contexts may run on several host threads
+    if (device < 0 || device >= 64) return false;
+    if (!done[device].load())
+        done[device] = cudaFuncSetAttribute(spread_owner_kernel<R, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            200 * 1024) == cudaSuccess;
+    return done[device].load();
+}
+
 template <typename R, int P>
 static void run_spread(simox_ctx* c, PmeRes& Rs, const PmeParams& S, const double* qalt) {
+    const size_t osm = c->n > 0 ? owner_smem(c) : 0;
+    if (osm && owner_ready<R, P>(c->device)) {
+        Launch L(c, "pme_spread");
+        SpreadOwner O;
+        O.ncs = make_int3(c->ncs[0], c->ncs[1], c->ncs[2]);
+        O.lcs = make_double3(c->lcs[0], c->lcs[1], c->lcs[2]);
+        spread_owner_kernel<R, P><<<c->ncell_s, SO_THREADS, osm, c->stream>>>(
+            S, O, c->cs_start, c->cs_entries, c->xq_s, c->xo_s, qalt, (R*)Rs.grid, Rs.dbl ? 1 : 0);
+        return;
+    }
     cudaMemsetAsync(Rs.grid, 0, c->ngrid * sizeof(R), c->stream);
     Launch L(c, "pme_spread");
     // FP32 grids: one CTA per cell of the atom order (skin cells or reference cells)
