@@ -262,79 +262,145 @@ struct SpreadOwner {
     double3 lcs;               // skin-cell edges
 };
 
+// Per atom (pair order): the first stencil point INT(u) - p/2 + 1 on each
+// axis in the frame of the skin cell the atom is listed in (its wrap relative
+// to that cell added in whole K), w = 0 for an uncharged atom (nothing to
+// spread).  One pass, so the owners' scans of their 27 neighbour cells
+// compare integers only.
+template <int P>
+__global__ void spread_base_kernel(PmeParams S, SpreadOwner O, int n, const int* __restrict__ cs_cell_of,
+                                   const int* __restrict__ order, const double4* __restrict__ xq,
+                                   const double4* __restrict__ xo, const double* __restrict__ qalt,
+                                   int4* __restrict__ base) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const double4 a = xq[k];
+    const double q = qalt ? qalt[k] : a.w;
+    const double4 o = xo[k];
+    const int nc = cs_cell_of[order[k]];
+    const int ni = nc % O.ncs.x, nj = (nc / O.ncs.x) % O.ncs.y, nk = nc / (O.ncs.x * O.ncs.y);
+    // the atom's wrap relative to its listed cell (VV_NVE1 wraps positions, the cell lists stay)
+    const int mx = (int)rint((-0.5 * S.box.x + (ni + 0.5) * O.lcs.x + o.x - a.x) / S.box.x);
+    const int my = (int)rint((-0.5 * S.box.y + (nj + 0.5) * O.lcs.y + o.y - a.y) / S.box.y);
+    const int mz = (int)rint((-0.5 * S.box.z + (nk + 0.5) * O.lcs.z + o.z - a.z) / S.box.z);
+    const double ux = (double)S.K.x * (a.x + S.box.x * 0.5) / S.box.x;
+    const double uy = (double)S.K.y * (a.y + S.box.y * 0.5) / S.box.y;
+    const double uz = (double)S.K.z * (a.z + S.box.z * 0.5) / S.box.z;
+    base[k] = make_int4(__double2int_rz(ux) - P / 2 + 1 + mx * S.K.x, __double2int_rz(uy) - P / 2 + 1 + my * S.K.y,
+                        __double2int_rz(uz) - P / 2 + 1 + mz * S.K.z, q != 0.0 ? 1 : 0);
+}
+
+// Owner spread, per CTA: (1) scan the 27 neighbour cells' precomputed
+// stencil bases and append each charged atom whose stencil reaches an owned
+// point to a shared list (atom, base relative to the owned block); (2) every
+// thread takes listed atoms, evaluates their weights and adds the owned
+// points of the stencil.  Listing first keeps all lanes on atoms that
+// contribute: scanning the neighbour cells directly leaves most lanes of a
+// warp idle through the whole stencil loop (an atom of an edge or corner
+// cell reaches the block with a few percent probability).  The list is
+// processed and emptied whenever the next chunk of a cell could overflow it.
+constexpr int SO_LIST = 1024;
+
+__device__ __forceinline__ int so_pack(int bx, int by, int bz) {
+    return (bx + 512) | ((by + 512) << 10) | ((bz + 512) << 20);
+}
+
 template <typename R, int P>
-__global__ void __launch_bounds__(SO_THREADS)
+__device__ __forceinline__ void so_spread_list(const PmeParams& S, const int2* __restrict__ list, int count,
+                                               const double4* __restrict__ xq, const double* __restrict__ qalt,
+                                               unsigned* lo, unsigned* hi, int ex, int ey, int ez,
+                                               int round_weights) {
+    for (int i = threadIdx.x; i < count; i += SO_THREADS) {
+        const int2 L = list[i];
+        const int k = L.x;
+        const int bx = (L.y & 1023) - 512, by = ((L.y >> 10) & 1023) - 512, bz = ((L.y >> 20) & 1023) - 512;
+        const double4 a = xq[k];
+        const double q = qalt ? qalt[k] : a.w;
+        const double ux = (double)S.K.x * (a.x + S.box.x * 0.5) / S.box.x;
+        const double uy = (double)S.K.y * (a.y + S.box.y * 0.5) / S.box.y;
+        const double uz = (double)S.K.z * (a.z + S.box.z * 0.5) / S.box.z;
+        double wx[P], wy[P], wz[P], d[P];
+        bspline_w<P>(ux, wx, d);
+        bspline_w<P>(uy, wy, d);
+        bspline_w<P>(uz, wz, d);
+        unsigned mx = 0, my = 0, mz = 0;   // stencil points inside the owned block, per axis
+#pragma unroll
+        for (int s = 0; s < P; s++) {
+            mx |= (unsigned)(bx + s >= 0 && bx + s < ex) << s;
+            my |= (unsigned)(by + s >= 0 && by + s < ey) << s;
+            mz |= (unsigned)(bz + s >= 0 && bz + s < ez) << s;
+        }
+#pragma unroll
+        for (int c = 0; c < P; c++) {
+            if (!((mz >> c) & 1u)) continue;
+#pragma unroll
+            for (int b = 0; b < P; b++) {
+                if (!((my >> b) & 1u)) continue;
+                const int row = ((bz + c) * ey + (by + b)) * ex + bx;
+#pragma unroll
+                for (int aa = 0; aa < P; aa++) {
+                    if (!((mx >> aa) & 1u)) continue;
+                    double w = wx[aa] * wy[b] * wz[c];
+                    if (round_weights) w = (double)(float)w;   // CMPLX() default kind, force.f90:406
+                    const long long v = __double2ll_rn(q * w * kSpreadScale);
+                    const unsigned vl = (unsigned)v, vh = (unsigned)((unsigned long long)v >> 32);
+                    const unsigned old = atomicAdd(lo + row + aa, vl);
+                    atomicAdd(hi + row + aa, vh + ((unsigned)(old + vl) < old ? 1u : 0u));
+                }
+            }
+        }
+    }
+}
+
+template <typename R, int P>
+__global__ void __launch_bounds__(SO_THREADS, 3)
     spread_owner_kernel(PmeParams S, SpreadOwner O, const int* __restrict__ cs_start,
                         const int* __restrict__ cs_entries, const double4* __restrict__ xq,
-                        const double4* __restrict__ xo, const double* __restrict__ qalt, R* __restrict__ grid,
+                        const int4* __restrict__ sbase, const double* __restrict__ qalt, R* __restrict__ grid,
                         int round_weights) {
-    extern __shared__ unsigned sow[];   // [npts] low words, [npts] high words
+    extern __shared__ unsigned sow[];   // [npad] low words, [npad] high words, [SO_LIST] list entries
+    __shared__ int count;
     const int cell = blockIdx.x;
     const int ci = cell % O.ncs.x, cj = (cell / O.ncs.x) % O.ncs.y, ck = cell / (O.ncs.x * O.ncs.y);
     const int x0 = (ci * S.K.x + O.ncs.x - 1) / O.ncs.x, x1 = ((ci + 1) * S.K.x + O.ncs.x - 1) / O.ncs.x;
     const int y0 = (cj * S.K.y + O.ncs.y - 1) / O.ncs.y, y1 = ((cj + 1) * S.K.y + O.ncs.y - 1) / O.ncs.y;
     const int z0 = (ck * S.K.z + O.ncs.z - 1) / O.ncs.z, z1 = ((ck + 1) * S.K.z + O.ncs.z - 1) / O.ncs.z;
     const int ex = x1 - x0, ey = y1 - y0, ez = z1 - z0, np = ex * ey * ez;
+    const int npad = (np + 1) & ~1;
     unsigned* lo = sow;
-    unsigned* hi = sow + np;
-    for (int i = threadIdx.x; i < 2 * np; i += SO_THREADS) sow[i] = 0u;
+    unsigned* hi = sow + npad;
+    int2* list = reinterpret_cast<int2*>(sow + 2 * npad);
+    for (int i = threadIdx.x; i < 2 * npad; i += SO_THREADS) sow[i] = 0u;
+    if (threadIdx.x == 0) count = 0;
     __syncthreads();
     for (int e = 0; e < 27; e++) {
         const int nc = cs_entries[cell * 27 + e];
         const int di = e % 3 - 1, dj = (e / 3) % 3 - 1, dk = e / 9 - 1;
         // the stencil cell's periodic shift in grid units
-        const int sx = ci + di < 0 ? -S.K.x : (ci + di >= O.ncs.x ? S.K.x : 0);
-        const int sy = cj + dj < 0 ? -S.K.y : (cj + dj >= O.ncs.y ? S.K.y : 0);
-        const int sz = ck + dk < 0 ? -S.K.z : (ck + dk >= O.ncs.z ? S.K.z : 0);
-        const int ni = nc % O.ncs.x, nj = (nc / O.ncs.x) % O.ncs.y, nk = nc / (O.ncs.x * O.ncs.y);
-        const double cx = -0.5 * S.box.x + (ni + 0.5) * O.lcs.x;
-        const double cy = -0.5 * S.box.y + (nj + 0.5) * O.lcs.y;
-        const double cz = -0.5 * S.box.z + (nk + 0.5) * O.lcs.z;
+        const int sx = (ci + di < 0 ? -S.K.x : (ci + di >= O.ncs.x ? S.K.x : 0)) - x0;
+        const int sy = (cj + dj < 0 ? -S.K.y : (cj + dj >= O.ncs.y ? S.K.y : 0)) - y0;
+        const int sz = (ck + dk < 0 ? -S.K.z : (ck + dk >= O.ncs.z ? S.K.z : 0)) - z0;
         const int k1 = cs_start[nc + 1];
-        for (int k = cs_start[nc] + threadIdx.x; k < k1; k += SO_THREADS) {
-            const double4 a = xq[k];
-            const double q = qalt ? qalt[k] : a.w;
-            if (q == 0.0) continue;
-            const double4 o = xo[k];
-            // the atom's wrap relative to its listed cell (VV_NVE1 wraps positions, the cell lists stay)
-            const int mx = (int)rint((cx + o.x - a.x) / S.box.x) * S.K.x + sx;
-            const int my = (int)rint((cy + o.y - a.y) / S.box.y) * S.K.y + sy;
-            const int mz = (int)rint((cz + o.z - a.z) / S.box.z) * S.K.z + sz;
-            const double ux = (double)S.K.x * (a.x + S.box.x * 0.5) / S.box.x;
-            const double uy = (double)S.K.y * (a.y + S.box.y * 0.5) / S.box.y;
-            const double uz = (double)S.K.z * (a.z + S.box.z * 0.5) / S.box.z;
-            const int bx = __double2int_rz(ux) - P / 2 + 1 + mx - x0;
-            const int by = __double2int_rz(uy) - P / 2 + 1 + my - y0;
-            const int bz = __double2int_rz(uz) - P / 2 + 1 + mz - z0;
-            if (bx >= ex || bx + P <= 0 || by >= ey || by + P <= 0 || bz >= ez || bz + P <= 0) continue;
-            double wx[P], wy[P], wz[P], d[P];
-            bspline_w<P>(ux, wx, d);
-            bspline_w<P>(uy, wy, d);
-            bspline_w<P>(uz, wz, d);
-#pragma unroll
-            for (int c = 0; c < P; c++) {
-                const int gz = bz + c;
-                if (gz < 0 || gz >= ez) continue;
-#pragma unroll
-                for (int b = 0; b < P; b++) {
-                    const int gy = by + b;
-                    if (gy < 0 || gy >= ey) continue;
-                    const int row = (gz * ey + gy) * ex;
-#pragma unroll
-                    for (int aa = 0; aa < P; aa++) {
-                        const int gx = bx + aa;
-                        if (gx < 0 || gx >= ex) continue;
-                        double w = wx[aa] * wy[b] * wz[c];
-                        if (round_weights) w = (double)(float)w;   // CMPLX() default kind, force.f90:406
-                        const long long v = __double2ll_rn(q * w * kSpreadScale);
-                        const unsigned vl = (unsigned)v, vh = (unsigned)((unsigned long long)v >> 32);
-                        const unsigned old = atomicAdd(lo + row + gx, vl);
-                        atomicAdd(hi + row + gx, vh + ((unsigned)(old + vl) < old ? 1u : 0u));
-                    }
-                }
+        for (int kb = cs_start[nc]; kb < k1; kb += SO_LIST) {
+            const int kc = min(k1, kb + SO_LIST);
+            const int cnt = count;   // the previous appends ended at the last barrier
+            __syncthreads();         // every thread has read count before anyone appends again
+            if (cnt + (kc - kb) > SO_LIST) {
+                so_spread_list<R, P>(S, list, cnt, xq, qalt, lo, hi, ex, ey, ez, round_weights);
+                __syncthreads();
+                if (threadIdx.x == 0) count = 0;
+                __syncthreads();
             }
+            for (int k = kb + threadIdx.x; k < kc; k += SO_THREADS) {
+                const int4 B = sbase[k];
+                const int bx = B.x + sx, by = B.y + sy, bz = B.z + sz;
+                if (!B.w || bx >= ex || bx + P <= 0 || by >= ey || by + P <= 0 || bz >= ez || bz + P <= 0) continue;
+                list[atomicAdd(&count, 1)] = make_int2(k, so_pack(bx, by, bz));
+            }
+            __syncthreads();
         }
     }
+    so_spread_list<R, P>(S, list, count, xq, qalt, lo, hi, ex, ey, ez, round_weights);
     __syncthreads();
     for (int i = threadIdx.x; i < np; i += SO_THREADS) {
         const int gx = i % ex, gy = (i / ex) % ey, gz = i / (ex * ey);
@@ -706,8 +772,9 @@ static size_t owner_smem(const simox_ctx* c) {
         const double skin_pts = 0.5 * c->skin * c->fft[d] / c->box[d];
         if (c->order / 2 + 2 + skin_pts > per) return 0;
         np *= (size_t)((c->fft[d] + c->ncs[d] - 1) / c->ncs[d]);   // most points a cell owns
+        if (per > 400) return 0;                                   // relative bases are packed in 10 bits
     }
-    const size_t b = 2 * sizeof(unsigned) * np;
+    const size_t b = 2 * sizeof(unsigned) * ((np + 1) & ~(size_t)1) + SO_LIST * sizeof(int2);
     return b <= (size_t)200 * 1024 ? b : 0;
 }
 
@@ -729,8 +796,10 @@ static void run_spread(simox_ctx* c, PmeRes& Rs, const PmeParams& S, const doubl
         SpreadOwner O;
         O.ncs = make_int3(c->ncs[0], c->ncs[1], c->ncs[2]);
         O.lcs = make_double3(c->lcs[0], c->lcs[1], c->lcs[2]);
+        spread_base_kernel<P><<<(c->n + 255) / 256, 256, 0, c->stream>>>(S, O, c->n, c->cs_cell_of, c->pair_order, c->xq_s,
+                                                                        c->xo_s, qalt, c->sbase);
         spread_owner_kernel<R, P><<<c->ncell_s, SO_THREADS, osm, c->stream>>>(
-            S, O, c->cs_start, c->cs_entries, c->xq_s, c->xo_s, qalt, (R*)Rs.grid, Rs.dbl ? 1 : 0);
+            S, O, c->cs_start, c->cs_entries, c->xq_s, c->sbase, qalt, (R*)Rs.grid, Rs.dbl ? 1 : 0);
         return;
     }
     cudaMemsetAsync(Rs.grid, 0, c->ngrid * sizeof(R), c->stream);
