@@ -61,37 +61,71 @@ constexpr size_t kHCSmem = (size_t)kHCCap * (sizeof(float4) + sizeof(double) + 4
 
 __device__ __forceinline__ void add_fixed(u64* p, long long v) { atomicAdd(p, (u64)v); }
 
-// A 64-bit fixed-point sum in shared memory held as two 32-bit words: the
-// carry out of the low word goes into the high word, so the pair adds up
-// exactly (modulo 2^64) in any order.  Two 32-bit shared atomics run several
-// times faster than one 64-bit shared atomic on this GPU.
-__device__ __forceinline__ void add_split(unsigned* lo, unsigned* hi, int i, long long v) {
-    const unsigned vl = (unsigned)v, vh = (unsigned)((unsigned long long)v >> 32);
-    const unsigned old = atomicAdd(lo + i, vl);
-    atomicAdd(hi + i, vh + ((unsigned)(old + vl) < old ? 1u : 0u));
-}
-
-// Where a partner's share goes: the CTA's tile (split words, `stride`
-// entries per component) or, for a tile too large for shared memory, the
-// global 64-bit sums (`stride` entries per component).
-template <bool TILED> struct Sink;
-template <> struct Sink<true> {
-    unsigned* lo;
-    unsigned* hi;
-    int stride;
-    __device__ __forceinline__ void add(int c, int i, long long v) const { add_split(lo + c * stride, hi + c * stride, i, v); }
-};
-template <> struct Sink<false> {
-    u64* g;
-    int stride;
-    __device__ __forceinline__ void add(int c, int i, long long v) const { atomicAdd(g + (size_t)c * stride + i, (u64)v); }
-};
-
 // The 14 cells of a CTA's tile: first pair-order index of each and their
 // offsets in the tile (own cell first).
 struct HalfTile {
     int start[kHalfCells];
     int off[kHalfCells + 1];
+};
+
+// pair-order index of tile slot i
+__device__ __forceinline__ int tile_src(const HalfTile& T, int i) {
+    int t = 0;
+    while (t < kHalfCells - 1 && T.off[t + 1] <= i) t++;
+    return T.start[t] + (i - T.off[t]);
+}
+
+// Partner shares in a CTA's tile.  A share v (64-bit fixed point) is split
+// as v = h 2^23 + l with l = v mod 2^23 and h = v >> 23 (arithmetic), and the
+// l words and h words of a slot are summed independently by fire-and-forget
+// shared adds (no returned value to wait for, no carry between the words).
+// A slot takes at most kSlotAdds = 512 shares -- one from each X of the
+// CTA's range, which the kernels check before choosing the tile -- so the l
+// sums stay below 2^32 and, for |v| < 2^45, the h sums within int32: the two
+// words give the exact 64-bit sum whatever the order of the adds.  A share
+// of 2^45 or more goes to the global 64-bit sum directly.
+constexpr int kSlotBits = 23;
+constexpr int kSlotAdds = 1 << (32 - kSlotBits);
+constexpr long long kSlotLim = 1LL << 45;
+
+__device__ __forceinline__ void red_shared_u32(unsigned* p, unsigned v) {
+    asm volatile("red.shared.add.u32 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(p)), "r"(v) : "memory");
+}
+
+// the exact sum of a slot's shares from its two words
+__device__ __forceinline__ long long slot_value(unsigned lo, unsigned hi) {
+    return (long long)(int)hi * (1LL << kSlotBits) + (long long)lo;
+}
+
+// Where a partner's share goes: the CTA's tile (two words per slot, `stride`
+// slots per component) or, for a tile too large for shared memory or a CTA
+// range above kSlotAdds atoms, the global 64-bit sums (`gstride` entries per
+// component, pair order).  X's own row sum always goes to the global sum.
+template <bool TILED> struct Sink;
+template <> struct Sink<true> {
+    unsigned* lo;
+    unsigned* hi;
+    int stride;
+    u64* g;
+    int gstride;
+    const HalfTile* T;
+    __device__ __forceinline__ void add(int c, int i, long long v) const {
+        if ((unsigned long long)(v + kSlotLim) < (unsigned long long)(2 * kSlotLim)) {
+            red_shared_u32(lo + c * stride + i, (unsigned)v & ((1u << kSlotBits) - 1u));
+            red_shared_u32(hi + c * stride + i, (unsigned)(v >> kSlotBits));
+        } else {
+            atomicAdd(g + (size_t)c * gstride + tile_src(*T, i), (u64)v);
+        }
+    }
+    __device__ __forceinline__ void own(int c, int X, long long v) const {
+        atomicAdd(g + (size_t)c * gstride + X, (u64)v);
+    }
+};
+template <> struct Sink<false> {
+    u64* g;
+    int stride;
+    __device__ __forceinline__ void add(int c, int i, long long v) const { atomicAdd(g + (size_t)c * stride + i, (u64)v); }
+    __device__ __forceinline__ void own(int c, int X, long long v) const { add(c, X, v); }
 };
 
 __device__ __forceinline__ void half_tile_setup(HalfTile& T, const int* __restrict__ cs_start,
@@ -110,18 +144,23 @@ __device__ __forceinline__ void half_tile_setup(HalfTile& T, const int* __restri
     __syncthreads();
 }
 
-// Adds the tile's split sums (nacc components of `stride` entries) into the
-// global 64-bit sums (nacc components of `gstride`), skipping zeros.
-__device__ __forceinline__ void half_tile_flush_split(const HalfTile& T, int total, const unsigned* lo,
-                                                      const unsigned* hi, int stride, int nacc, u64* gacc,
-                                                      int gstride) {
+// X range [b0, b1) of CTA part `part` of `splits` over the own cell
+__device__ __forceinline__ int2 half_range(const HalfTile& T, int part, int splits) {
+    const int a0 = T.start[0], na = T.off[1];
+    return make_int2(a0 + (int)((long long)na * part / splits), a0 + (int)((long long)na * (part + 1) / splits));
+}
+
+// Adds the tile's sums (nacc components of `stride` slots) into the global
+// 64-bit sums (nacc components of `gstride`), skipping zeros.
+__device__ __forceinline__ void half_tile_flush(const HalfTile& T, int total, const unsigned* lo,
+                                                const unsigned* hi, int stride, int nacc, u64* gacc, int gstride) {
     int t = 0;
     for (int i = threadIdx.x; i < total; i += blockDim.x) {
         while (T.off[t + 1] <= i) t++;
         const int gi = T.start[t] + (i - T.off[t]);
         for (int a = 0; a < nacc; a++) {
-            const u64 v = ((u64)hi[a * stride + i] << 32) | lo[a * stride + i];
-            if (v) atomicAdd(gacc + (size_t)a * gstride + gi, v);
+            const long long v = slot_value(lo[a * stride + i], hi[a * stride + i]);
+            if (v) atomicAdd(gacc + (size_t)a * gstride + gi, (u64)v);
         }
     }
 }
@@ -252,7 +291,7 @@ __device__ __forceinline__ void filter_half_atoms(const Half1Params& H, const fl
             }
             lmax = max(lmax, tot);
             ltot += (unsigned long long)tot;
-            acc.add(0, TILED ? X - a0 : X, __double2ll_rn(rho * kRhoScaleD));
+            acc.own(0, X, __double2ll_rn(rho * kRhoScaleD));
         }
     }
 }
@@ -292,7 +331,9 @@ __global__ void __launch_bounds__(kH1Threads)
     const int cell = blockIdx.x / H.splits, part = blockIdx.x - cell * H.splits;
     half_tile_setup(T, cs_start, cs_entries, cell);
     const int total = T.off[kHalfCells];
-    const bool tiled = total <= kH1Cap;
+    const int2 br = half_range(T, part, H.splits);
+    const int b0 = br.x, b1 = br.y;
+    const bool tiled = total <= kH1Cap && b1 - b0 <= kSlotAdds;
     if (tid < kHalfCells) delta[tid] = T.off[tid] - T.start[tid];
     if (tiled)
         for (int i = tid; i < total; i += blockDim.x) {
@@ -301,9 +342,7 @@ __global__ void __launch_bounds__(kH1Threads)
         }
     __syncthreads();
     const int g0 = H.g0;
-    const int a0 = T.start[0], na = T.off[1];
-    const int b0 = a0 + (int)((long long)na * part / H.splits);
-    const int b1 = a0 + (int)((long long)na * (part + 1) / H.splits);
+    const int a0 = T.start[0];
     int lmax = 0, bad = 0;
     unsigned long long ltot = 0;
     if (b1 > b0) {
@@ -311,7 +350,7 @@ __global__ void __launch_bounds__(kH1Threads)
         bad = dflag[(g0 << 3) | g0] | dflag[(g0 << 3) | 3] | dflag[(3 << 3) | g0] | dflag[(3 << 3) | 3];
         if (tiled)
             filter_half_atoms<true>(H, ssh, dsh, b0, b1, a0, &next, xq, rec, order, nn_s, nbr_s, nn, nbr, delta,
-                                    total, Sink<true>{alo, ahi, 0}, lmax, ltot, bad);
+                                    total, Sink<true>{alo, ahi, 0, rho_fx, 0, &T}, lmax, ltot, bad);
         else
             filter_half_atoms<false>(H, ssh, dsh, b0, b1, a0, &next, xq, rec, order, nn_s, nbr_s, nn, nbr, delta,
                                      H.F.pp.n, Sink<false>{rho_fx, 0}, lmax, ltot, bad);
@@ -322,7 +361,7 @@ __global__ void __launch_bounds__(kH1Threads)
         if (ltot) atomicAdd(nn_tot, ltot);
     }
     __syncthreads();
-    if (tiled) half_tile_flush_split(T, total, alo, ahi, 0, 1, rho_fx, 0);
+    if (tiled) half_tile_flush(T, total, alo, ahi, 0, 1, rho_fx, 0);
 }
 
 // rho from the fixed-point sums, then F'(rho) (force.f90:256-351)
@@ -450,7 +489,6 @@ __device__ __forceinline__ void force_half_atoms(const Half2Params& H, const int
         const unsigned* row = nbr + (size_t)X * cap;
         v2 fh[3] = {bc(0.f), bc(0.f), bc(0.f)}, fl[3] = {bc(0.f), bc(0.f), bc(0.f)};
         const bool metal = sX == g0;
-        const int slotX = TILED ? X - a0 : X;
         if (!metal && sX != 3) {
             if (m.x + m.y > 0) bad |= ST_UNKNOWN_PAIR;
         } else {
@@ -490,9 +528,9 @@ __device__ __forceinline__ void force_half_atoms(const Half2Params& H, const int
         fy = warp_sum(fy);
         fz = warp_sum(fz);
         if (lane == 0) {
-            acc.add(0, slotX, __double2ll_rn(fx * kForceScaleD));
-            acc.add(1, slotX, __double2ll_rn(fy * kForceScaleD));
-            acc.add(2, slotX, __double2ll_rn(fz * kForceScaleD));
+            acc.own(0, X, __double2ll_rn(fx * kForceScaleD));
+            acc.own(1, X, __double2ll_rn(fy * kForceScaleD));
+            acc.own(2, X, __double2ll_rn(fz * kForceScaleD));
         }
     }
 }
@@ -522,7 +560,9 @@ __global__ void __launch_bounds__(kH2Threads, 1)
         for (int k = tid; k < 4 * NB; k += kH2Threads) hist[k] = 0;
     half_tile_setup(T, cs_start, cs_entries, cell);
     const int total = T.off[kHalfCells];
-    const bool tiled = total <= kH2Cap;
+    const int2 br = half_range(T, part, H.splits);
+    const int b0 = br.x, b1 = br.y;
+    const bool tiled = total <= kH2Cap && b1 - b0 <= kSlotAdds;
     if (tid < kEntries) {
         esh[tid] = stencil_shift(tid, H.lcs);
         // positions below 13 never occur in a half row: a delta that the
@@ -550,19 +590,17 @@ __global__ void __launch_bounds__(kH2Threads, 1)
         }
     }
     __syncthreads();
-    const int a0 = T.start[0], na = T.off[1];
-    const int b0 = a0 + (int)((long long)na * part / H.splits);
-    const int b1 = a0 + (int)((long long)na * (part + 1) / H.splits);
+    const int a0 = T.start[0];
     int bad = 0;
     if (tiled)
         force_half_atoms<true, RDF>(H, edelta, esh, tpos, tdf, total, b0, b1, a0, &next, xo, ts, nn, nbr, dF_f,
-                                    Sink<true>{tlo, thi, kH2Cap}, hist, bad);
+                                    Sink<true>{tlo, thi, kH2Cap, f_fx, H.fstride, &T}, hist, bad);
     else
         force_half_atoms<false, RDF>(H, edelta, esh, xo, dF_f, H.n, b0, b1, a0, &next, xo, ts, nn, nbr, dF_f,
                                      Sink<false>{f_fx, H.fstride}, hist, bad);
     if (bad) atomicOr(status, bad);
     __syncthreads();
-    if (tiled) half_tile_flush_split(T, total, tlo, thi, kH2Cap, 3, f_fx, H.fstride);
+    if (tiled) half_tile_flush(T, total, tlo, thi, kH2Cap, 3, f_fx, H.fstride);
     if (RDF) {
         const int g0 = H.g0;
         for (int k = tid; k < 4 * NB; k += kH2Threads) {
@@ -691,7 +729,6 @@ __device__ __forceinline__ void ctip_half_atoms(const CtipHalfParams& C, const f
         const int2 m = nn[X];
         const unsigned* row = nbr + (size_t)X * cap;
         const bool metal = sX == C.g0;
-        const int slotX = TILED ? X - a0 : X;
         double sr = 0.0, cz = 0.0;
         if (metal || sX == 3) {
             const int nb0 = (m.x + 63) >> 6, nb = nb0 + ((m.y + 63) >> 6);
@@ -724,8 +761,8 @@ __device__ __forceinline__ void ctip_half_atoms(const CtipHalfParams& C, const f
         sr = warp_sum(sr);
         if (WITH_C) cz = warp_sum(cz);
         if (lane == 0) {
-            acc.add(0, slotX, __double2ll_rn(sr * kRhoScaleD));
-            if (WITH_C) acc.add(1, slotX, __double2ll_rn(cz * kRhoScaleD));
+            acc.own(0, X, __double2ll_rn(sr * kRhoScaleD));
+            if (WITH_C) acc.own(1, X, __double2ll_rn(cz * kRhoScaleD));
         }
     }
 }
@@ -749,7 +786,9 @@ __global__ void __launch_bounds__(kH2Threads, 1)
     if (tid == 0) next = 0;
     half_tile_setup(T, cs_start, cs_entries, cell);
     const int total = T.off[kHalfCells];
-    const bool tiled = total <= kHCCap;
+    const int2 br = half_range(T, part, C.splits);
+    const int b0 = br.x, b1 = br.y;
+    const bool tiled = total <= kHCCap && b1 - b0 <= kSlotAdds;
     if (tid < kEntries) {
         const float4 o = C.sh[tid];
         const int d = tid < kHalfFirst ? -(1 << 28) : (tiled ? T.off[tid - kHalfFirst] - T.start[tid - kHalfFirst] : 0);
@@ -773,17 +812,15 @@ __global__ void __launch_bounds__(kH2Threads, 1)
         cp_async_wait<0>();
     }
     __syncthreads();
-    const int a0 = T.start[0], na = T.off[1];
-    const int b0 = a0 + (int)((long long)na * part / C.splits);
-    const int b1 = a0 + (int)((long long)na * (part + 1) / C.splits);
+    const int a0 = T.start[0];
     if (tiled)
         ctip_half_atoms<WITH_C, true>(C, etab, trec, tv, total, b0, b1, a0, &next, frec, ts, vin, nn, nbr,
-                                      Sink<true>{tlo, thi, kHCCap});
+                                      Sink<true>{tlo, thi, kHCCap, gacc, gstride, &T});
     else
         ctip_half_atoms<WITH_C, false>(C, etab, frec, vin, C.n, b0, b1, a0, &next, frec, ts, vin, nn, nbr,
                                        Sink<false>{gacc, gstride});
     __syncthreads();
-    if (tiled) half_tile_flush_split(T, total, tlo, thi, kHCCap, WITH_C ? 2 : 1, gacc, gstride);
+    if (tiled) half_tile_flush(T, total, tlo, thi, kHCCap, WITH_C ? 2 : 1, gacc, gstride);
 }
 
 // out = fixed-point sums; cconst = chi + the fixed-point asym sums
