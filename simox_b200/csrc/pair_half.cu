@@ -88,9 +88,7 @@ constexpr int kSlotBits = 23;
 constexpr int kSlotAdds = 1 << (32 - kSlotBits);
 constexpr long long kSlotLim = 1LL << 45;
 
-__device__ __forceinline__ void red_shared_u32(unsigned* p, unsigned v) {
-    asm volatile("red.shared.add.u32 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(p)), "r"(v) : "memory");
-}
+__device__ __forceinline__ void red_shared_u32(unsigned* p, unsigned v) { atomicAdd(p, v); }   // result unused
 
 // the exact sum of a slot's shares from its two words
 __device__ __forceinline__ long long slot_value(unsigned lo, unsigned hi) {

@@ -20,12 +20,13 @@
   where a charge crosses a bound: a difference whose interval [theta - h,
   theta + h] holds such a crossing is off by O(h) (J of O at h = 1e-4 moved
   its energy difference by 2e-3 relative).  Every component is differenced
-  at h = 1e-4, 1e-5 and 1e-6.  The energy, stationary in q, is checked at
-  h = 1e-6; the loss, which the charge solve's last digits reach through the
-  forces, at the largest step whose two solves keep the set of charges
-  outside their bounds that theta itself has.  Energy components within
-  1e-4, loss components within 1e-3 of their own size (plus 1e-6 of the
-  largest).
+  at h = 1e-4, 1e-5 and 1e-6 and checked at the largest of them whose two
+  solves keep the set of charges outside their bounds that theta itself
+  has.  The h = 1e-6 differences are printed beside them: there the FP64
+  evaluation's own noise (~1e-7 eV in E, from the order of its atomic sums;
+  xi of O read 26.896 against 26.951 at the wider steps and the adjoint)
+  reaches the difference.  Energy components within 1e-4, loss components
+  within 1e-3 of their own size (plus 1e-6 of the largest).
 """
 import numpy as np
 import pytest
@@ -147,15 +148,15 @@ def test_energy_and_loss_gradients_match_finite_differences():
                     fd[h] = ((vals[0][0] - vals[1][0]) / (2 * h), (vals[0][1] - vals[1][1]) / (2 * h))
                 hl = next((h for h in (1e-4, 1e-5, 1e-6) if same[h]), None)
                 assert hl is not None, f"component {k}: a charge crosses a bound within 1e-6 of theta"
-                report.append((k, gE[j], fd[1e-4][0], fd[1e-6][0], gL[j], hl, fd[hl][1]))
-                assert same[1e-6] and abs(fd[1e-6][0] - gE[j]) <= tolE, (k, fd, gE[j])
+                report.append((k, hl, gE[j], fd[hl][0], fd[1e-6][0], gL[j], fd[hl][1], fd[1e-6][1]))
+                assert abs(fd[hl][0] - gE[j]) <= tolE, (k, hl, fd, gE[j])
                 assert abs(fd[hl][1] - gL[j]) <= tolL, (k, hl, fd, gL[j])
         finally:
             g.adjoint_warm_start(False)
             _params(g, P, spl, th0)
-        print("\ncomponent  dE/dth: adjoint  FD(1e-4)  FD(1e-6)   dL/dth: adjoint  step  FD")
+        print("\ncomponent step  dE/dth: adjoint  FD  FD(1e-6)   dL/dth: adjoint  FD  FD(1e-6)")
         for row in report:
-            print("%4d  % .8e % .8e % .8e   % .8e %.0e % .8e" % row)
+            print("%4d %.0e  % .8e % .8e % .8e   % .8e % .8e % .8e" % row)
 
 
 def test_gradients_match_cpu_reference_at_2000_atoms():
