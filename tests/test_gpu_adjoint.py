@@ -19,10 +19,14 @@
   piecewise quadratic (zero inside [qmin, qmax]), so q*(theta) has a kink
   where a charge crosses a bound: a difference whose interval [theta - h,
   theta + h] holds such a crossing is off by O(h) (J of O at h = 1e-4 moved
-  its energy difference by 2e-3 relative).  Every component is differenced
-  at h = 1e-4, 1e-5 and 1e-6 and checked at the largest of them whose two
-  solves keep the set of charges outside their bounds that theta itself
-  has.  The h = 1e-6 differences are printed beside them: there the FP64
+  its energy difference by 2e-3 relative).  The functional is not convex
+  either, so a refinement can also settle on another stationary point with
+  the same bounded set (chi of O once read -89.651 against -89.609 at every
+  other step and in the adjoint).  Every component is differenced at
+  h = 1e-4, 1e-5 and 1e-6 and checked at the largest of them whose two
+  solves stay on theta's branch: the same set of charges outside their
+  bounds, and the mean of the two solutions within 10 h of theta's charges
+  (a smooth branch differs from them by O(h^2)).  The h = 1e-6 differences are printed beside them: there the FP64
   evaluation's own noise (~1e-7 eV in E, from the order of its atomic sums;
   xi of O read 26.896 against 26.951 at the wider steps and the adjoint)
   reaches the difference.  Energy components within 1e-4, loss components
@@ -134,7 +138,7 @@ def test_energy_and_loss_gradients_match_finite_differences():
                 tolL = 1e-3 * abs(gL[j]) + 1e-6 * np.abs(gL).max()
                 fd, same = {}, {}
                 for h in (1e-4, 1e-5, 1e-6):
-                    vals, same[h] = [], True
+                    vals, same[h], qs = [], True, []
                     for sgn in (1.0, -1.0):
                         th = th0.copy()
                         th[k] += sgn * h
@@ -144,10 +148,12 @@ def test_energy_and_loss_gradients_match_finite_differences():
                         assert r["residual"] <= 1e-8 * np.sqrt(s.n), r
                         assert r["n_cg"] == 0
                         vals.append((r["E"], r["loss"]))
-                        same[h] &= bool(np.array_equal(bounded(g.get_state()["q"]), set0))
+                        qs.append(g.get_state()["q"])
+                        same[h] &= bool(np.array_equal(bounded(qs[-1]), set0))
+                    same[h] &= bool(np.abs(0.5 * (qs[0] + qs[1]) - q0).max() <= 10.0 * h)
                     fd[h] = ((vals[0][0] - vals[1][0]) / (2 * h), (vals[0][1] - vals[1][1]) / (2 * h))
                 hl = next((h for h in (1e-4, 1e-5, 1e-6) if same[h]), None)
-                assert hl is not None, f"component {k}: a charge crosses a bound within 1e-6 of theta"
+                assert hl is not None, f"component {k}: no step of 1e-4..1e-6 keeps both solves on theta's branch"
                 report.append((k, hl, gE[j], fd[hl][0], fd[1e-6][0], gL[j], fd[hl][1], fd[1e-6][1]))
                 assert abs(fd[hl][0] - gE[j]) <= tolE, (k, hl, fd, gE[j])
                 assert abs(fd[hl][1] - gL[j]) <= tolL, (k, hl, fd, gL[j])
