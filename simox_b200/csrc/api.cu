@@ -378,7 +378,7 @@ static void free_ctx(simox_ctx* c) {
     adjoint_free(c);
     pme_free(c);
     void* bufs[] = {c->id, c->x, c->v, c->f, c->q, c->xm, c->cell_of, c->cell_xyz, c->cell_count, c->cell_start, c->cell_fill,
-                    c->sorted, c->pair13, c->entries, c->xq_s, c->t_s, c->rec_s, c->frec_s, c->xo_s, c->sbase, c->nn, c->nbr, c->nn_max, c->nn_tot,
+                    c->sorted, c->pair13, c->entries, c->xq_s, c->t_s, c->rec_s, c->frec_s, c->xo_s, c->nn, c->nbr, c->nn_max, c->nn_tot,
                     c->cs_count, c->cs_start, c->cs_fill, c->cs_cell_of, c->cs_entries, c->perm, c->x0,
                     c->skin_flag, c->nn_s, c->nbr_s, c->rho_s, c->dF_s, c->dF_f, c->tab_d, c->tab_f, c->c_const, c->g, c->pv, c->Ap, c->qs, c->jp,
                     c->act, c->line, c->acc, c->status, c->rdf, c->f_rec, c->rho_fx, c->fx_acc};
@@ -478,7 +478,7 @@ extern "C" int simox_create(const simox_setup* s, const simox_potential* pot, si
               dalloc(&c->cell_start, c->ncell + 1) && dalloc(&c->cell_fill, c->ncell) && dalloc(&c->sorted, N) &&
               dalloc(&c->pair13, (size_t)c->ncell * 13) && dalloc(&c->entries, (size_t)c->ncell * kEntries) &&
               dalloc(&c->xq_s, N) && dalloc(&c->t_s, N) && dalloc(&c->rec_s, N) && dalloc(&c->frec_s, N) &&
-              dalloc(&c->xo_s, N) && dalloc(&c->sbase, N) && dalloc(&c->nn, 2 * N) &&
+              dalloc(&c->xo_s, N) && dalloc(&c->nn, 2 * N) &&
               dalloc(&c->nbr, N * (size_t)c->nnb_cap) && dalloc(&c->nn_max, 1) && dalloc(&c->nn_tot, 1) &&
               dalloc(&c->rho_s, N) && dalloc(&c->dF_s, N) && dalloc(&c->dF_f, N) && dalloc(&c->rho_fx, N) &&
               dalloc(&c->fx_acc, 3 * N) && dalloc(&c->tab_d, kSpecies * kSpecies) &&

@@ -18,14 +18,15 @@
 //   pass 1 (filter_half_kernel): the skin filter (the reference's FP64
 //          r2 < Rcut2 test near the cutoff, force.f90:51-54) and both
 //          densities of each kept pair (force.f90:84-85); kept entries are
-//          compacted into the exact half row with bit 31 = "X is the
-//          reference's i".  embed_half_kernel then forms F'(rho)
-//          (force.f90:256-351).
+//          compacted into the exact half row.  embed_half_kernel then forms
+//          F'(rho) (force.f90:256-351).
 //   pass 2 (force_half_kernel): the pair force of force.f90:81-98 and
 //          101-140 with the density back-pass of force.f90:353-358 folded in,
 //          once per pair, on packed FP32 (two entries per lane), and the RDF
 //          (force.f90:76,180), each pair counted once under the reference's
-//          (i, j) species order.
+//          (i, j) species order; on RDF steps the pass finds which atom of a
+//          pair is the reference's i from the reference cells
+//          (cellsort.f90:18-30), so ordinary steps skip that work.
 //   charge solver (ctip_half_kernel): sum_Y sym_XY v_Y and chi + sum_Y
 //          Z_Y asym_XY of ctip.f90:85-110 and dUdq (ctip.f90:307-333).
 //   energies (energy_half_kernel): the FP64 pair energies once per pair and
@@ -156,21 +157,19 @@ struct Half1Params {
 
 // One group of X's half skin row (G = 0: metal partners of species g0 at the
 // row front; G = 1: oxygen at the back).  Kept entries are compacted into X's
-// exact half row with bit 31 = "X is the reference's i"; their density at X
+// exact half row; their density at X
 // is summed in rho and their density at Y is added to Y's accumulator.
 template <int G, bool TILED>
 __device__ __forceinline__ int filter_group_half(const Half1Params& H, const float4* ssh, const DensC<float>& du,
                                                  const DensC<float>& dv, int sX, int sY,
                                                  const unsigned* __restrict__ sp, int mg, unsigned* __restrict__ dp,
-                                                 const float4& ra, unsigned wa, int xm, int ym, int zm, int oX, int X,
-                                                 const double4* __restrict__ xq, const float4* __restrict__ rec,
-                                                 const int* __restrict__ order, const int* delta, int lim,
+                                                 const float4& ra, int X, const double4* __restrict__ xq,
+                                                 const float4* __restrict__ rec, const int* delta, int lim,
                                                  const Sink<TILED>& acc, double& rho) {
     const FilterParams& F = H.F;
     const PairParams& P = F.pp;
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
-    const int ay = (wa >> 9) & 511, az = (wa >> 18) & 511;
     auto ent = [&](int k) { return k < mg ? sp[G == 0 ? k : -k] : 0u; };
     unsigned E1 = ent(lane), E2 = ent(lane + 32);
     float4 rb1 = rec[E1 & kSkinIdxMask];
@@ -197,17 +196,9 @@ __device__ __forceinline__ int filter_group_half(const Half1Params& H, const flo
                 keep = __dadd_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)), __dmul_rn(ddz, ddz)) < F.rcut2;
             }
         }
-        // X is the reference's i: Y's reference cell is one of the 13 forward
-        // cells of X's (cellsort.f90:18-30), or the same cell and X comes first
-        const unsigned wb = __float_as_uint(rb.w);
-        const int bx = wb & 511, by = (wb >> 9) & 511, bz = (wb >> 18) & 511;
-        const bool same = ((wb ^ wa) & 0x07ffffffu) == 0u;
-        int oY = 0x7fffffff;
-        if (keep & same) oY = order[Y];
-        const bool isa = (bz == zm) | ((bz == az) & ((by == ym) | ((by == ay) & ((bx == xm) | (same & (oX < oY))))));
         const unsigned mask = __ballot_sync(0xffffffffu, keep);
         const int pos = out + __popc(mask & lt);
-        if (keep & (pos < P.cap)) dp[G == 0 ? pos : -pos] = e | ((unsigned)isa << 31);
+        if (keep & (pos < P.cap)) dp[G == 0 ? pos : -pos] = e;
         out += __popc(mask);
         const float r = r2 * rsqrt_approx(r2);
         const float vX = dens_term<float>(du, r), vY = dens_term<float>(dv, r);
@@ -246,21 +237,15 @@ __device__ __forceinline__ void filter_half_atoms(const Half1Params& H, const fl
             if (lane == 0) nn[X] = make_int2(0, 0);
             continue;
         }
-        const int ax = wa & 511, ay = (wa >> 9) & 511, az = (wa >> 18) & 511;
-        const int xm = ax == 0 ? F.nc.x - 1 : ax - 1;
-        const int ym = ay == 0 ? F.nc.y - 1 : ay - 1;
-        const int zm = az == 0 ? F.nc.z - 1 : az - 1;
-        const int oX = order[X];
         const int2 ms = nn_s[X];
         const unsigned* srow = nbr_s + (size_t)X * F.cap_s;
         unsigned* row = nbr + (size_t)X * F.pp.cap;
         double rho = 0.0;
         const int out0 = filter_group_half<0, TILED>(H, ssh, dsh[(sX << 3) | g0], dsh[(g0 << 3) | sX], sX, g0,
-                                                     srow, ms.x, row, ra, wa, xm, ym, zm, oX, X, xq, rec, order,
-                                                     delta, lim, acc, rho);
+                                                     srow, ms.x, row, ra, X, xq, rec, delta, lim, acc, rho);
         const int out1 = filter_group_half<1, TILED>(H, ssh, dsh[(sX << 3) | 3], dsh[(3 << 3) | sX], sX, 3,
-                                                     srow + (F.cap_s - 1), ms.y, row + (F.pp.cap - 1), ra, wa,
-                                                     xm, ym, zm, oX, X, xq, rec, order, delta, lim, acc, rho);
+                                                     srow + (F.cap_s - 1), ms.y, row + (F.pp.cap - 1), ra, X, xq,
+                                                     rec, delta, lim, acc, rho);
         rho = warp_sum(rho);
         if (lane == 0) {
             const int tot = out0 + out1;
@@ -373,8 +358,41 @@ __global__ void embed_half_kernel(int n, const int* __restrict__ ts, const u64* 
 struct Half2Params {
     PackParams Q;
     double3 lcs;               // skin-cell edges
+    int3 nc;                   // reference cell grid (RDF: the reference's i)
     int splits, g0, n, fstride;
 };
+
+// X's reference cell for the reference's-i test of the RDF: wa = X's record
+// word (reference cell 9 bits per axis), the cells below X's on each axis
+// (periodic) and X's reference order
+struct RefX {
+    unsigned wa;
+    int xm, ym, zm, oX;
+};
+
+__device__ __forceinline__ RefX ref_x(const Half2Params& H, const float4* __restrict__ rec,
+                                      const int* __restrict__ order, int X) {
+    RefX R;
+    R.wa = __float_as_uint(rec[X].w);
+    const int ax = R.wa & 511, ay = (R.wa >> 9) & 511, az = (R.wa >> 18) & 511;
+    R.xm = ax == 0 ? H.nc.x - 1 : ax - 1;
+    R.ym = ay == 0 ? H.nc.y - 1 : ay - 1;
+    R.zm = az == 0 ? H.nc.z - 1 : az - 1;
+    R.oX = order[X];
+    return R;
+}
+
+// X is the reference's i of the listed pair (X, Y): Y's reference cell is one
+// of the 13 forward cells of X's (cellsort.f90:18-30), or the same cell and X
+// comes first in the reference's order
+__device__ __forceinline__ bool ref_isa(const RefX& R, const float4* __restrict__ rec,
+                                        const int* __restrict__ order, int Y) {
+    const unsigned wb = __float_as_uint(rec[Y].w);
+    const int bx = wb & 511, by = (wb >> 9) & 511, bz = (wb >> 18) & 511;
+    const int ay = (R.wa >> 9) & 511, az = (R.wa >> 18) & 511;
+    const bool same = ((wb ^ R.wa) & 0x07ffffffu) == 0u;
+    return (bz == R.zm) | ((bz == az) & ((by == R.ym) | ((by == ay) & ((bx == R.xm) | (same && R.oX < order[Y])))));
+}
 
 // o_e * Lcs of stencil position e = (dk+1) 9 + (dj+1) 3 + (di+1)
 __device__ __forceinline__ double3 stencil_shift(int e, double3 lcs) {
@@ -389,7 +407,8 @@ __device__ __forceinline__ void force_half_batch(const Half2Params& H, const int
                                                  const double4* __restrict__ psrc, const float* __restrict__ dsrc,
                                                  int lim, unsigned E1, unsigned E2, bool v1, bool v2ok,
                                                  const double4& ra, float dFX, const Sink<TILED>& acc, v2 (&fh)[3],
-                                                 v2 (&fl)[3], int* hist, int& bad) {
+                                                 v2 (&fl)[3], int* hist, const RefX& RX, const float4* __restrict__ rec,
+                                                 const int* __restrict__ order, int& bad) {
     constexpr int NB = SIMOX_NRDF + 2;
     const PackParams& Q = H.Q;
     const PackTab& T = Q.tab[TI];
@@ -438,11 +457,13 @@ __device__ __forceinline__ void force_half_batch(const Half2Params& H, const int
         constexpr int kxy = TI, kyx = ((TI & 1) << 1) | (TI >> 1);
         if (v1) {
             const float r = r2.v.x * rsqrt_approx(r2.v.x);
-            atomicAdd(&hist[((E1 & kIsA) ? kxy : kyx) * NB + min(max((int)(r * Q.inv_dr), 0), NB - 1)], 2);
+            const bool isa = ref_isa(RX, rec, order, (int)(E1 & kIdxMask));
+            atomicAdd(&hist[(isa ? kxy : kyx) * NB + min(max((int)(r * Q.inv_dr), 0), NB - 1)], 2);
         }
         if (v2ok) {
             const float r = r2.v.y * rsqrt_approx(r2.v.y);
-            atomicAdd(&hist[((E2 & kIsA) ? kxy : kyx) * NB + min(max((int)(r * Q.inv_dr), 0), NB - 1)], 2);
+            const bool isa = ref_isa(RX, rec, order, (int)(E2 & kIdxMask));
+            atomicAdd(&hist[(isa ? kxy : kyx) * NB + min(max((int)(r * Q.inv_dr), 0), NB - 1)], 2);
         }
     }
 }
@@ -454,6 +475,7 @@ __device__ __forceinline__ void force_half_atoms(const Half2Params& H, const int
                                                  const double4* __restrict__ xo, const int* __restrict__ ts,
                                                  const int2* __restrict__ nn, const unsigned* __restrict__ nbr,
                                                  const float* __restrict__ dF_f, const Sink<TILED>& acc, int* hist,
+                                                 const float4* __restrict__ rec, const int* __restrict__ order,
                                                  int& bad) {
     const int lane = threadIdx.x & 31;
     const int cap = H.Q.cap;
@@ -466,6 +488,7 @@ __device__ __forceinline__ void force_half_atoms(const Half2Params& H, const int
         const double4 ra = xo[X];
         const int sX = ts[X];
         const float dFX = dF_f[X];
+        const RefX RX = RDF ? ref_x(H, rec, order, X) : RefX{};
         const int2 m = nn[X];
         const unsigned* row = nbr + (size_t)X * cap;
         v2 fh[3] = {bc(0.f), bc(0.f), bc(0.f)}, fl[3] = {bc(0.f), bc(0.f), bc(0.f)};
@@ -494,11 +517,11 @@ __device__ __forceinline__ void force_half_atoms(const Half2Params& H, const int
                 const int kb = (g1 ? j - nb0 : j) << 6, mg = g1 ? m.y : m.x;
                 const bool v1 = kb + lane < mg, v2ok = kb + 32 + lane < mg;
                 if (metal) {
-                    if (!g1) force_half_batch<true, true, RDF, TILED, 0>(H, edelta, esh, psrc, dsrc, lim, E1, E2, v1, v2ok, ra, dFX, acc, fh, fl, hist, bad);
-                    else force_half_batch<false, false, RDF, TILED, 1>(H, edelta, esh, psrc, dsrc, lim, E1, E2, v1, v2ok, ra, dFX, acc, fh, fl, hist, bad);
+                    if (!g1) force_half_batch<true, true, RDF, TILED, 0>(H, edelta, esh, psrc, dsrc, lim, E1, E2, v1, v2ok, ra, dFX, acc, fh, fl, hist, RX, rec, order, bad);
+                    else force_half_batch<false, false, RDF, TILED, 1>(H, edelta, esh, psrc, dsrc, lim, E1, E2, v1, v2ok, ra, dFX, acc, fh, fl, hist, RX, rec, order, bad);
                 } else {
-                    if (!g1) force_half_batch<false, false, RDF, TILED, 2>(H, edelta, esh, psrc, dsrc, lim, E1, E2, v1, v2ok, ra, dFX, acc, fh, fl, hist, bad);
-                    else force_half_batch<true, false, RDF, TILED, 3>(H, edelta, esh, psrc, dsrc, lim, E1, E2, v1, v2ok, ra, dFX, acc, fh, fl, hist, bad);
+                    if (!g1) force_half_batch<false, false, RDF, TILED, 2>(H, edelta, esh, psrc, dsrc, lim, E1, E2, v1, v2ok, ra, dFX, acc, fh, fl, hist, RX, rec, order, bad);
+                    else force_half_batch<true, false, RDF, TILED, 3>(H, edelta, esh, psrc, dsrc, lim, E1, E2, v1, v2ok, ra, dFX, acc, fh, fl, hist, RX, rec, order, bad);
                 }
             }
         }
@@ -522,7 +545,7 @@ __global__ void __launch_bounds__(kH2Threads, 1)
                       const int* __restrict__ cs_entries, const double4* __restrict__ xo,
                       const int* __restrict__ ts, const int2* __restrict__ nn, const unsigned* __restrict__ nbr,
                       const float* __restrict__ dF_f, u64* __restrict__ f_fx, int* __restrict__ rdf,
-                      int* __restrict__ status) {
+                      const float4* __restrict__ rec, const int* __restrict__ order, int* __restrict__ status) {
     constexpr int NB = SIMOX_NRDF + 2;
     extern __shared__ __align__(16) unsigned char half_smem[];
     double4* tpos = reinterpret_cast<double4*>(half_smem);                 // partner offsets + shift, charge
@@ -575,10 +598,10 @@ __global__ void __launch_bounds__(kH2Threads, 1)
     int bad = 0;
     if (tiled)
         force_half_atoms<true, RDF>(H, edelta, esh, tpos, tdf, total, b0, b1, a0, &next, xo, ts, nn, nbr, dF_f,
-                                    Sink<true>{tlo, thi, kH2Cap, f_fx, H.fstride}, hist, bad);
+                                    Sink<true>{tlo, thi, kH2Cap, f_fx, H.fstride}, hist, rec, order, bad);
     else
         force_half_atoms<false, RDF>(H, edelta, esh, xo, dF_f, H.n, b0, b1, a0, &next, xo, ts, nn, nbr, dF_f,
-                                     Sink<false>{f_fx, H.fstride}, hist, bad);
+                                     Sink<false>{f_fx, H.fstride}, hist, rec, order, bad);
     if (bad) atomicOr(status, bad);
     __syncthreads();
     if (tiled) half_tile_flush(T, total, tlo, thi, kH2Cap, 3, f_fx, H.fstride);
@@ -947,6 +970,7 @@ int force_half(simox_ctx* c, bool rdf) {
     Q.tab[2] = pack_tab(c->pot, 3, g0);
     Q.tab[3] = pack_tab(c->pot, 3, 3);
     H.lcs = make_double3(c->lcs[0], c->lcs[1], c->lcs[2]);
+    H.nc = make_int3(c->nc[0], c->nc[1], c->nc[2]);
     H.splits = std::max(1, std::min(16, c->force_splits));
     H.g0 = g0;
     H.n = c->n;
@@ -958,11 +982,11 @@ int force_half(simox_ctx* c, bool rdf) {
         if (rdf)
             force_half_kernel<true><<<g, kH2Threads, kH2Smem, c->stream>>>(
                 H, c->cs_start, c->cs_entries, c->xo_s, c->t_s, reinterpret_cast<const int2*>(c->nn), c->nbr,
-                c->dF_f, c->fx_acc, c->rdf, c->status);
+                c->dF_f, c->fx_acc, c->rdf, c->rec_s, c->pair_order, c->status);
         else
             force_half_kernel<false><<<g, kH2Threads, kH2Smem, c->stream>>>(
                 H, c->cs_start, c->cs_entries, c->xo_s, c->t_s, reinterpret_cast<const int2*>(c->nn), c->nbr,
-                c->dF_f, c->fx_acc, c->rdf, c->status);
+                c->dF_f, c->fx_acc, c->rdf, c->rec_s, c->pair_order, c->status);
     }
     {
         Launch L(c, "pair_force_finalize");

@@ -84,67 +84,81 @@ __device__ __forceinline__ int wrapi(int v, int K) {
     return v < 0 ? v + K : v;
 }
 
-// spread: grid[x + K1(y + K2 z)] += q * W (cell-sorted atoms)
+// Spread: grid[x + K1(y + K2 z)] = sum q W, summed exactly in 64-bit fixed
+// point (2^48 units), so the grid does not depend on the order of the adds.
+// Atoms are stored cell by cell (skin cells or reference cells), and one CTA
+// takes one cell: it finds the box of grid points its atoms' stencils cover
+// (unwrapped indices), adds q W there in shared memory -- each 64-bit sum
+// held as two 32-bit words with the carry of the low word added into the high
+// one -- and then adds the box to the global 64-bit grid `acc` (wrapped), one
+// global atomic per touched point instead of one per atom and stencil point.
+// A cell whose box exceeds the patch adds straight into `acc`.  A second
+// kernel converts `acc` to the grid's type and clears it for the next spread.
+// Measured at 128k corundum (PME 128^3, order 6): 38 us for the shared adds,
+// about 50 us with the global merge and the conversion.
+//
+// Per point the work is one FP64 multiply (q scale wx) * (wy wz) and one FP64
+// add: RN(x) as an integer is read from the bits of x + 1.5 2^52, the
+// magic-number rounding, exact for |x| < 2^51 (|q W| < 8); larger values take
+// the conversion instruction.  The FP64 grid keeps the reference's product
+// order (wx wy) wz, rounded to FP32 as force.f90:406 does, times q.
+constexpr int SP_THREADS = 256;
+constexpr int SP_CAP = 9216;                              // patch points: 72 KB, three CTAs per SM
+constexpr double kSpreadScale = 281474976710656.0;        // 2^48
+constexpr double kSpreadUnit = 1.0 / 281474976710656.0;
+constexpr double kMagic = 6755399441055744.0;             // 1.5 2^52
+
+__device__ __forceinline__ long long spread_fixed(double x) {
+    return fabs(x) < 2251799813685248.0 ? __double_as_longlong(x + kMagic) - __double_as_longlong(kMagic)
+                                        : __double2ll_rn(x);
+}
+
+__device__ __forceinline__ void patch_add(unsigned* lo, unsigned* hi, int i, long long v) {
+    const unsigned vl = (unsigned)v, vh = (unsigned)((unsigned long long)v >> 32);
+    const unsigned old = atomicAdd(lo + i, vl);
+    atomicAdd(hi + i, vh + ((unsigned)(old + vl) < old ? 1u : 0u));
+}
+
+// x = q W scaled, W = wx wy wz: the reference's FP32-rounded product order on
+// the FP64 grid, (q scale wx) (wy wz) otherwise
+template <bool ROUND>
+__device__ __forceinline__ double spread_term(double q, double qwx, double wx, double wy, double wz, double wyz) {
+    if constexpr (ROUND) return q * (double)(float)(wx * wy * wz) * kSpreadScale;
+    else return qwx * wyz;
+}
+
+// an atom of a cell whose box exceeds the patch: straight into the global sums
 template <typename R, int P>
-__global__ void __launch_bounds__(128)
-    spread_kernel(PmeParams S, const double4* __restrict__ xq, const double* __restrict__ qalt,
-                  R* __restrict__ grid, int round_weights) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= S.n) return;
-    const double4 a = xq[k];
-    const double q = qalt ? qalt[k] : a.w;
-    if (q == 0.0) return;
-    double wx[P], wy[P], wz[P], d[P];
-    const double ux = (double)S.K.x * (a.x + S.box.x * 0.5) / S.box.x;
-    const double uy = (double)S.K.y * (a.y + S.box.y * 0.5) / S.box.y;
-    const double uz = (double)S.K.z * (a.z + S.box.z * 0.5) / S.box.z;
-    bspline_w<P>(ux, wx, d);
-    bspline_w<P>(uy, wy, d);
-    bspline_w<P>(uz, wz, d);
-    const int bx = __double2int_rz(ux) - P / 2 + 1;
-    const int by = __double2int_rz(uy) - P / 2 + 1;
-    const int bz = __double2int_rz(uz) - P / 2 + 1;
-    int ix[P];
-#pragma unroll
-    for (int s = 0; s < P; s++) ix[s] = wrapi(bx + s, S.K.x);
-#pragma unroll
+__device__ __noinline__ void spread_atom_global(const PmeParams& S, double q, const double* wx, const double* wy,
+                                                const double* wz, int bx, int by, int bz,
+                                                unsigned long long* __restrict__ acc) {
+    constexpr bool ROUND = sizeof(R) == 8;
+    const double qs = q * kSpreadScale;
     for (int c = 0; c < P; c++) {
         const size_t gz = (size_t)wrapi(bz + c, S.K.z) * S.K.y;
-#pragma unroll
         for (int b = 0; b < P; b++) {
             const size_t gyz = (gz + wrapi(by + b, S.K.y)) * S.K.x;
-#pragma unroll
-            for (int aa = 0; aa < P; aa++) {
-                double w = wx[aa] * wy[b] * wz[c];
-                if (round_weights) w = (double)(float)w;   // CMPLX() default kind, force.f90:406
-                atomicAdd(grid + gyz + ix[aa], (R)(q * w));
-            }
+            const double wyz = wy[b] * wz[c];
+            for (int aa = 0; aa < P; aa++)
+                atomicAdd(acc + gyz + wrapi(bx + aa, S.K.x),
+                          (unsigned long long)spread_fixed(spread_term<ROUND>(q, wx[aa] * qs, wx[aa], wy[b], wz[c], wyz)));
         }
     }
 }
 
-// FP32 spread through a shared-memory grid patch.  Atoms are stored cell
-// by cell, so one CTA takes one cell: it finds the box of grid points its
-// atoms' stencils cover (unwrapped indices), accumulates q*W there with
-// shared-memory atomics, then adds the patch to the global grid (wrapped)
-// with one global atomic per touched point instead of one per atom and
-// stencil point.  A cell whose box exceeds the patch spreads directly into
-// the global grid.
-constexpr int SP_THREADS = 256;
-constexpr int SP_PATCH = 16384;   // grid points (64 KB of FP32)
-
-template <int P>
-__global__ void __launch_bounds__(SP_THREADS)
-    spread_tile_kernel(PmeParams S, const double4* __restrict__ xq, const double* __restrict__ qalt,
-                       const int* __restrict__ ranges, float* __restrict__ grid) {
-    extern __shared__ float patch[];
-    __shared__ int lo[3], hi[3];
+template <typename R, int P>
+__global__ void __launch_bounds__(SP_THREADS, sizeof(R) == 8 ? 2 : 3)
+    spread_patch_kernel(PmeParams S, const double4* __restrict__ xq, const double* __restrict__ qalt,
+                        const int* __restrict__ ranges, unsigned long long* __restrict__ acc) {
+    constexpr bool ROUND = sizeof(R) == 8;   // FP64 grid: the reference's FP32 weight products
+    extern __shared__ unsigned sp_words[];  // [SP_CAP] low words, [SP_CAP] high words
+    __shared__ int lo3[3], hi3[3];
     const int a0 = ranges[blockIdx.x], a1 = ranges[blockIdx.x + 1];
     if (a1 <= a0) return;
     const int tid = threadIdx.x;
     if (tid < 3) {
-        lo[tid] = 0x7fffffff;
-        hi[tid] = -0x7fffffff;
+        lo3[tid] = 0x7fffffff;
+        hi3[tid] = -0x7fffffff;
     }
     __syncthreads();
     int mn[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, mx[3] = {-0x7fffffff, -0x7fffffff, -0x7fffffff};
@@ -169,16 +183,21 @@ __global__ void __launch_bounds__(SP_THREADS)
             mx[d] = max(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
         }
         if ((tid & 31) == 0) {
-            atomicMin(&lo[d], mn[d]);
-            atomicMax(&hi[d], mx[d]);
+            atomicMin(&lo3[d], mn[d]);
+            atomicMax(&hi3[d], mx[d]);
         }
     }
     __syncthreads();
-    if (hi[0] < lo[0]) return;   // no charged atom
-    const int ex = hi[0] - lo[0] + P, ey = hi[1] - lo[1] + P, ez = hi[2] - lo[2] + P;
-    const bool tiled = (long long)ex * ey * ez <= SP_PATCH;
+    if (hi3[0] < lo3[0]) return;   // no charged atom
+    const int ex = hi3[0] - lo3[0] + P, ey = hi3[1] - lo3[1] + P, ez = hi3[2] - lo3[2] + P;
+    const bool tiled = (long long)ex * ey * ez <= SP_CAP;
+    unsigned* plo = sp_words;
+    unsigned* phi = sp_words + SP_CAP;
     if (tiled) {
-        for (int i = tid; i < ex * ey * ez; i += SP_THREADS) patch[i] = 0.f;
+        for (int i = tid; i < ex * ey * ez; i += SP_THREADS) {
+            plo[i] = 0u;
+            phi[i] = 0u;
+        }
         __syncthreads();
     }
     for (int k = a0 + tid; k < a1; k += SP_THREADS) {
@@ -195,35 +214,24 @@ __global__ void __launch_bounds__(SP_THREADS)
         const int bx = __double2int_rz(ux) - P / 2 + 1;
         const int by = __double2int_rz(uy) - P / 2 + 1;
         const int bz = __double2int_rz(uz) - P / 2 + 1;
-        float qx[P];
+        if (!tiled) {
+            spread_atom_global<R, P>(S, q, wx, wy, wz, bx, by, bz, acc);
+            continue;
+        }
+        const double qs = q * kSpreadScale;
+        double qwx[P];
 #pragma unroll
-        for (int aa = 0; aa < P; aa++) qx[aa] = (float)(q * wx[aa]);
-        if (tiled) {
-            float* pz = patch + ((bz - lo[2]) * ey + (by - lo[1])) * ex + (bx - lo[0]);
+        for (int aa = 0; aa < P; aa++) qwx[aa] = ROUND ? 0.0 : wx[aa] * qs;
+        const int rx = bx - lo3[0], ry = by - lo3[1], rz = bz - lo3[2];
 #pragma unroll
-            for (int cc = 0; cc < P; cc++) {
+        for (int c = 0; c < P; c++) {
 #pragma unroll
-                for (int b = 0; b < P; b++) {
-                    const float wyz = (float)(wy[b] * wz[cc]);
-                    float* pr = pz + (cc * ey + b) * ex;
+            for (int b = 0; b < P; b++) {
+                const int row = ((rz + c) * ey + (ry + b)) * ex + rx;
+                const double wyz = ROUND ? 0.0 : wy[b] * wz[c];
 #pragma unroll
-                    for (int aa = 0; aa < P; aa++) atomicAdd(pr + aa, qx[aa] * wyz);
-                }
-            }
-        } else {
-            int ix[P];
-#pragma unroll
-            for (int s2 = 0; s2 < P; s2++) ix[s2] = wrapi(bx + s2, S.K.x);
-#pragma unroll
-            for (int cc = 0; cc < P; cc++) {
-                const size_t gz = (size_t)wrapi(bz + cc, S.K.z) * S.K.y;
-#pragma unroll
-                for (int b = 0; b < P; b++) {
-                    const float wyz = (float)(wy[b] * wz[cc]);
-                    const size_t gyz = (gz + wrapi(by + b, S.K.y)) * S.K.x;
-#pragma unroll
-                    for (int aa = 0; aa < P; aa++) atomicAdd(grid + gyz + ix[aa], qx[aa] * wyz);
-                }
+                for (int aa = 0; aa < P; aa++)
+                    patch_add(plo, phi, row + aa, spread_fixed(spread_term<ROUND>(q, qwx[aa], wx[aa], wy[b], wz[c], wyz)));
             }
         }
     }
@@ -232,181 +240,22 @@ __global__ void __launch_bounds__(SP_THREADS)
     const int warp = tid >> 5, lane = tid & 31;
     for (int rowi = warp; rowi < ey * ez; rowi += SP_THREADS / 32) {
         const int iy = rowi % ey, iz = rowi / ey;
-        const size_t gyz = ((size_t)wrapi(lo[2] + iz, S.K.z) * S.K.y + wrapi(lo[1] + iy, S.K.y)) * S.K.x;
-        const float* pr = patch + (size_t)rowi * ex;
+        const size_t gyz = ((size_t)wrapi(lo3[2] + iz, S.K.z) * S.K.y + wrapi(lo3[1] + iy, S.K.y)) * S.K.x;
         for (int ix = lane; ix < ex; ix += 32) {
-            const float v = pr[ix];
-            if (v != 0.f) atomicAdd(grid + gyz + wrapi(lo[0] + ix, S.K.x), v);
+            const int i = rowi * ex + ix;
+            const unsigned long long v = ((unsigned long long)phi[i] << 32) | plo[i];
+            if (v) atomicAdd(acc + gyz + wrapi(lo3[0] + ix, S.K.x), v);
         }
     }
 }
 
-// Owner spread (skin-cell pair order).  Skin cell (ci, cj, ck) of an
-// ncs-grid owns the grid points g with ceil(ci K / ncs) <= g < ceil((ci+1) K
-// / ncs) on each axis, so every point has exactly one owner.  Its CTA takes
-// the atoms of the 27 cells around it, places each in its own frame (the
-// atom's wrap relative to its listed cell plus the stencil cell's periodic
-// shift, whole multiples of K), and adds q W of the stencil points it owns
-// into 64-bit fixed-point sums (2^50 units) in shared memory, held as
-// carry-linked 32-bit word pairs; the sums are exact, so the grid does not
-// depend on the order of the adds.  The owned points are then stored once:
-// no clearing of the grid and no global atomics.  The weights are those of
-// the reference formula on the atom's own coordinate, so each atom's
-// contribution equals the other spreads' term for term.
-constexpr int SO_THREADS = 256;
-constexpr double kSpreadScale = 1125899906842624.0;        // 2^50
-constexpr double kSpreadUnit = 1.0 / 1125899906842624.0;
-
-struct SpreadOwner {
-    int3 ncs;
-    double3 lcs;               // skin-cell edges
-};
-
-// Per atom (pair order): the first stencil point INT(u) - p/2 + 1 on each
-// axis in the frame of the skin cell the atom is listed in (its wrap relative
-// to that cell added in whole K), w = 0 for an uncharged atom (nothing to
-// spread).  One pass, so the owners' scans of their 27 neighbour cells
-// compare integers only.
-template <int P>
-__global__ void spread_base_kernel(PmeParams S, SpreadOwner O, int n, const int* __restrict__ cs_cell_of,
-                                   const int* __restrict__ order, const double4* __restrict__ xq,
-                                   const double4* __restrict__ xo, const double* __restrict__ qalt,
-                                   int4* __restrict__ base) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    const double4 a = xq[k];
-    const double q = qalt ? qalt[k] : a.w;
-    const double4 o = xo[k];
-    const int nc = cs_cell_of[order[k]];
-    const int ni = nc % O.ncs.x, nj = (nc / O.ncs.x) % O.ncs.y, nk = nc / (O.ncs.x * O.ncs.y);
-    // the atom's wrap relative to its listed cell (VV_NVE1 wraps positions, the cell lists stay)
-    const int mx = (int)rint((-0.5 * S.box.x + (ni + 0.5) * O.lcs.x + o.x - a.x) / S.box.x);
-    const int my = (int)rint((-0.5 * S.box.y + (nj + 0.5) * O.lcs.y + o.y - a.y) / S.box.y);
-    const int mz = (int)rint((-0.5 * S.box.z + (nk + 0.5) * O.lcs.z + o.z - a.z) / S.box.z);
-    const double ux = (double)S.K.x * (a.x + S.box.x * 0.5) / S.box.x;
-    const double uy = (double)S.K.y * (a.y + S.box.y * 0.5) / S.box.y;
-    const double uz = (double)S.K.z * (a.z + S.box.z * 0.5) / S.box.z;
-    base[k] = make_int4(__double2int_rz(ux) - P / 2 + 1 + mx * S.K.x, __double2int_rz(uy) - P / 2 + 1 + my * S.K.y,
-                        __double2int_rz(uz) - P / 2 + 1 + mz * S.K.z, q != 0.0 ? 1 : 0);
-}
-
-// Owner spread, per CTA: (1) scan the 27 neighbour cells' precomputed
-// stencil bases and append each charged atom whose stencil reaches an owned
-// point to a shared list (atom, base relative to the owned block); (2) every
-// thread takes listed atoms, evaluates their weights and adds the owned
-// points of the stencil.  Listing first keeps all lanes on atoms that
-// contribute: scanning the neighbour cells directly leaves most lanes of a
-// warp idle through the whole stencil loop (an atom of an edge or corner
-// cell reaches the block with a few percent probability).  The list is
-// processed and emptied whenever the next chunk of a cell could overflow it.
-constexpr int SO_LIST = 1024;
-
-__device__ __forceinline__ int so_pack(int bx, int by, int bz) {
-    return (bx + 512) | ((by + 512) << 10) | ((bz + 512) << 20);
-}
-
-template <typename R, int P>
-__device__ __forceinline__ void so_spread_list(const PmeParams& S, const int2* __restrict__ list, int count,
-                                               const double4* __restrict__ xq, const double* __restrict__ qalt,
-                                               unsigned* lo, unsigned* hi, int ex, int ey, int ez,
-                                               int round_weights) {
-    for (int i = threadIdx.x; i < count; i += SO_THREADS) {
-        const int2 L = list[i];
-        const int k = L.x;
-        const int bx = (L.y & 1023) - 512, by = ((L.y >> 10) & 1023) - 512, bz = ((L.y >> 20) & 1023) - 512;
-        const double4 a = xq[k];
-        const double q = qalt ? qalt[k] : a.w;
-        const double ux = (double)S.K.x * (a.x + S.box.x * 0.5) / S.box.x;
-        const double uy = (double)S.K.y * (a.y + S.box.y * 0.5) / S.box.y;
-        const double uz = (double)S.K.z * (a.z + S.box.z * 0.5) / S.box.z;
-        double wx[P], wy[P], wz[P], d[P];
-        bspline_w<P>(ux, wx, d);
-        bspline_w<P>(uy, wy, d);
-        bspline_w<P>(uz, wz, d);
-        unsigned mx = 0, my = 0, mz = 0;   // stencil points inside the owned block, per axis
-#pragma unroll
-        for (int s = 0; s < P; s++) {
-            mx |= (unsigned)(bx + s >= 0 && bx + s < ex) << s;
-            my |= (unsigned)(by + s >= 0 && by + s < ey) << s;
-            mz |= (unsigned)(bz + s >= 0 && bz + s < ez) << s;
-        }
-#pragma unroll
-        for (int c = 0; c < P; c++) {
-            if (!((mz >> c) & 1u)) continue;
-#pragma unroll
-            for (int b = 0; b < P; b++) {
-                if (!((my >> b) & 1u)) continue;
-                const int row = ((bz + c) * ey + (by + b)) * ex + bx;
-#pragma unroll
-                for (int aa = 0; aa < P; aa++) {
-                    if (!((mx >> aa) & 1u)) continue;
-                    double w = wx[aa] * wy[b] * wz[c];
-                    if (round_weights) w = (double)(float)w;   // CMPLX() default kind, force.f90:406
-                    const long long v = __double2ll_rn(q * w * kSpreadScale);
-                    const unsigned vl = (unsigned)v, vh = (unsigned)((unsigned long long)v >> 32);
-                    const unsigned old = atomicAdd(lo + row + aa, vl);
-                    atomicAdd(hi + row + aa, vh + ((unsigned)(old + vl) < old ? 1u : 0u));
-                }
-            }
-        }
-    }
-}
-
-template <typename R, int P>
-__global__ void __launch_bounds__(SO_THREADS, 3)
-    spread_owner_kernel(PmeParams S, SpreadOwner O, const int* __restrict__ cs_start,
-                        const int* __restrict__ cs_entries, const double4* __restrict__ xq,
-                        const int4* __restrict__ sbase, const double* __restrict__ qalt, R* __restrict__ grid,
-                        int round_weights) {
-    extern __shared__ unsigned sow[];   // [npad] low words, [npad] high words, [SO_LIST] list entries
-    __shared__ int count;
-    const int cell = blockIdx.x;
-    const int ci = cell % O.ncs.x, cj = (cell / O.ncs.x) % O.ncs.y, ck = cell / (O.ncs.x * O.ncs.y);
-    const int x0 = (ci * S.K.x + O.ncs.x - 1) / O.ncs.x, x1 = ((ci + 1) * S.K.x + O.ncs.x - 1) / O.ncs.x;
-    const int y0 = (cj * S.K.y + O.ncs.y - 1) / O.ncs.y, y1 = ((cj + 1) * S.K.y + O.ncs.y - 1) / O.ncs.y;
-    const int z0 = (ck * S.K.z + O.ncs.z - 1) / O.ncs.z, z1 = ((ck + 1) * S.K.z + O.ncs.z - 1) / O.ncs.z;
-    const int ex = x1 - x0, ey = y1 - y0, ez = z1 - z0, np = ex * ey * ez;
-    const int npad = (np + 1) & ~1;
-    unsigned* lo = sow;
-    unsigned* hi = sow + npad;
-    int2* list = reinterpret_cast<int2*>(sow + 2 * npad);
-    for (int i = threadIdx.x; i < 2 * npad; i += SO_THREADS) sow[i] = 0u;
-    if (threadIdx.x == 0) count = 0;
-    __syncthreads();
-    for (int e = 0; e < 27; e++) {
-        const int nc = cs_entries[cell * 27 + e];
-        const int di = e % 3 - 1, dj = (e / 3) % 3 - 1, dk = e / 9 - 1;
-        // the stencil cell's periodic shift in grid units
-        const int sx = (ci + di < 0 ? -S.K.x : (ci + di >= O.ncs.x ? S.K.x : 0)) - x0;
-        const int sy = (cj + dj < 0 ? -S.K.y : (cj + dj >= O.ncs.y ? S.K.y : 0)) - y0;
-        const int sz = (ck + dk < 0 ? -S.K.z : (ck + dk >= O.ncs.z ? S.K.z : 0)) - z0;
-        const int k1 = cs_start[nc + 1];
-        for (int kb = cs_start[nc]; kb < k1; kb += SO_LIST) {
-            const int kc = min(k1, kb + SO_LIST);
-            const int cnt = count;   // the previous appends ended at the last barrier
-            __syncthreads();         // every thread has read count before anyone appends again
-            if (cnt + (kc - kb) > SO_LIST) {
-                so_spread_list<R, P>(S, list, cnt, xq, qalt, lo, hi, ex, ey, ez, round_weights);
-                __syncthreads();
-                if (threadIdx.x == 0) count = 0;
-                __syncthreads();
-            }
-            for (int k = kb + threadIdx.x; k < kc; k += SO_THREADS) {
-                const int4 B = sbase[k];
-                const int bx = B.x + sx, by = B.y + sy, bz = B.z + sz;
-                if (!B.w || bx >= ex || bx + P <= 0 || by >= ey || by + P <= 0 || bz >= ez || bz + P <= 0) continue;
-                list[atomicAdd(&count, 1)] = make_int2(k, so_pack(bx, by, bz));
-            }
-            __syncthreads();
-        }
-    }
-    so_spread_list<R, P>(S, list, count, xq, qalt, lo, hi, ex, ey, ez, round_weights);
-    __syncthreads();
-    for (int i = threadIdx.x; i < np; i += SO_THREADS) {
-        const int gx = i % ex, gy = (i / ex) % ey, gz = i / (ex * ey);
-        const long long v = (long long)(((unsigned long long)hi[i] << 32) | lo[i]);
-        grid[((size_t)(z0 + gz) * S.K.y + (y0 + gy)) * S.K.x + (x0 + gx)] = (R)((double)v * kSpreadUnit);
-    }
+// grid = acc in the grid's type; acc cleared for the next spread
+template <typename R>
+__global__ void spread_convert_kernel(size_t n, unsigned long long* __restrict__ acc, R* __restrict__ grid) {
+    const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    grid[i] = (R)((double)(long long)acc[i] * kSpreadUnit);
+    acc[i] = 0ull;
 }
 
 // half-spectrum multiply by G/N and energy sum_k G |Q^|^2 (Hermitian weights)
@@ -663,7 +512,7 @@ static void pme_res_free(PmeRes& R) {
         cufftDestroy(R.r2c);
         cufftDestroy(R.c2r);
     }
-    cudaFree(R.grid); cudaFree(R.cgrid); cudaFree(R.infl);
+    cudaFree(R.grid); cudaFree(R.cgrid); cudaFree(R.infl); cudaFree(R.acc);
     R = PmeRes();
 }
 
@@ -682,6 +531,8 @@ static int pme_res_init(simox_ctx* c, PmeRes& R, bool dbl) {
     if (cudaMalloc(&R.grid, c->ngrid * rs) != cudaSuccess) return SIMOX_E_NOMEM;
     if (cudaMalloc(&R.cgrid, c->nhalf * 2 * rs) != cudaSuccess) return SIMOX_E_NOMEM;
     if (cudaMalloc(&R.infl, c->nhalf * rs) != cudaSuccess) return SIMOX_E_NOMEM;
+    if (cudaMalloc(&R.acc, c->ngrid * sizeof(unsigned long long)) != cudaSuccess) return SIMOX_E_NOMEM;
+    if (cudaMemset(R.acc, 0, c->ngrid * sizeof(unsigned long long)) != cudaSuccess) return SIMOX_E_NOMEM;
     // cuFFT plans: dims slowest-first (K3, K2, K1); K1 is the contiguous x axis
     if (cufftPlan3d(&R.r2c, K[2], K[1], K[0], dbl ? CUFFT_D2Z : CUFFT_R2C) != CUFFT_SUCCESS) return SIMOX_E_FFT_SIZE;
     if (cufftPlan3d(&R.c2r, K[2], K[1], K[0], dbl ? CUFFT_Z2D : CUFFT_C2R) != CUFFT_SUCCESS) {
@@ -749,71 +600,30 @@ int pme_self(simox_ctx* c) {
     return check_launch(c);
 }
 
-template <int P>
-static bool spread_tile_ready(int device) {
+template <typename R, int P>
+static bool spread_ready(int device) {
     static std::atomic<bool> done[64] = {};   // contexts may run on several host threads
     if (device < 0 || device >= 64) return false;
     if (!done[device].load())
-        done[device] = cudaFuncSetAttribute(spread_tile_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)(SP_PATCH * sizeof(float))) == cudaSuccess;
+        done[device] = cudaFuncSetAttribute(spread_patch_kernel<R, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)(2 * SP_CAP * sizeof(unsigned))) == cudaSuccess;
     return done[device].load();
 }
 
-// owner-spread shared memory (two 32-bit words per owned point) of this
-// context's skin grid, or 0 when the owner spread does not apply: the pair
-// order must be the skin order, and a stencil (p/2 points on either side of
-// an atom, which may sit up to skin/2 outside its cell) must not reach past
-// the neighbouring cells
-static size_t owner_smem(const simox_ctx* c) {
-    if (!(c->using_skin && c->pair_order == c->perm)) return 0;
-    size_t np = 1;
-    for (int d = 0; d < 3; d++) {
-        const int per = c->fft[d] / c->ncs[d];                    // fewest points a cell owns
-        const double skin_pts = 0.5 * c->skin * c->fft[d] / c->box[d];
-        if (c->order / 2 + 2 + skin_pts > per) return 0;
-        np *= (size_t)((c->fft[d] + c->ncs[d] - 1) / c->ncs[d]);   // most points a cell owns
-        if (per > 400) return 0;                                   // relative bases are packed in 10 bits
-    }
-    const size_t b = 2 * sizeof(unsigned) * ((np + 1) & ~(size_t)1) + SO_LIST * sizeof(int2);
-    return b <= (size_t)200 * 1024 ? b : 0;
-}
-
+// one CTA per cell of the atom order (skin cells or reference cells)
 template <typename R, int P>
-static bool owner_ready(int device) {
-    static std::atomic<bool> done[64] = {};   // contexts may run on several host threads
-    if (device < 0 || device >= 64) return false;
-    if (!done[device].load())
-        done[device] = cudaFuncSetAttribute(spread_owner_kernel<R, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            200 * 1024) == cudaSuccess;
-    return done[device].load();
-}
-
-template <typename R, int P>
-static void run_spread(simox_ctx* c, PmeRes& Rs, const PmeParams& S, const double* qalt) {
-    const size_t osm = c->n > 0 ? owner_smem(c) : 0;
-    if (osm && owner_ready<R, P>(c->device)) {
-        Launch L(c, "pme_spread");
-        SpreadOwner O;
-        O.ncs = make_int3(c->ncs[0], c->ncs[1], c->ncs[2]);
-        O.lcs = make_double3(c->lcs[0], c->lcs[1], c->lcs[2]);
-        spread_base_kernel<P><<<(c->n + 255) / 256, 256, 0, c->stream>>>(S, O, c->n, c->cs_cell_of, c->pair_order, c->xq_s,
-                                                                        c->xo_s, qalt, c->sbase);
-        spread_owner_kernel<R, P><<<c->ncell_s, SO_THREADS, osm, c->stream>>>(
-            S, O, c->cs_start, c->cs_entries, c->xq_s, c->sbase, qalt, (R*)Rs.grid, Rs.dbl ? 1 : 0);
-        return;
-    }
-    cudaMemsetAsync(Rs.grid, 0, c->ngrid * sizeof(R), c->stream);
+static int run_spread(simox_ctx* c, PmeRes& Rs, const PmeParams& S, const double* qalt) {
+    if (!spread_ready<R, P>(c->device)) return SIMOX_E_CUDA;
     Launch L(c, "pme_spread");
-    // FP32 grids: one CTA per cell of the atom order (skin cells or reference cells)
-    if (!Rs.dbl && c->n > 0 && spread_tile_ready<P>(c->device)) {
+    if (c->n > 0) {
         const bool skin = c->using_skin && c->pair_order == c->perm;
         const int* ranges = skin ? c->cs_start : c->cell_start;
         const int nr = skin ? c->ncell_s : c->ncell;
-        spread_tile_kernel<P><<<nr, SP_THREADS, SP_PATCH * sizeof(float), c->stream>>>(S, c->xq_s, qalt, ranges,
-                                                                                       (float*)Rs.grid);
-        return;
+        spread_patch_kernel<R, P><<<nr, SP_THREADS, 2 * SP_CAP * sizeof(unsigned), c->stream>>>(S, c->xq_s, qalt,
+                                                                                               ranges, Rs.acc);
     }
-    spread_kernel<R, P><<<(S.n + 127) / 128, 128, 0, c->stream>>>(S, c->xq_s, qalt, (R*)Rs.grid, Rs.dbl ? 1 : 0);
+    spread_convert_kernel<R><<<(unsigned)((c->ngrid + 255) / 256), 256, 0, c->stream>>>(c->ngrid, Rs.acc, (R*)Rs.grid);
+    return check_launch(c);
 }
 
 static int run_convolution(simox_ctx* c, PmeRes& Rs, bool eflag) {
@@ -860,8 +670,8 @@ static PmeParams pme_params(const simox_ctx* c) {
 template <typename R, int P>
 static int pme_forces_t(simox_ctx* c, PmeRes& Rs, bool eflag, double* f_store) {
     PmeParams S = pme_params(c);
-    run_spread<R, P>(c, Rs, S, nullptr);
-    int st = run_convolution(c, Rs, eflag);
+    int st = run_spread<R, P>(c, Rs, S, nullptr);
+    if (!st) st = run_convolution(c, Rs, eflag);
     if (st) return st;
     Launch L(c, "pme_gather_force");
     gather_force_kernel<R, P><<<(S.n + 127) / 128, 128, 0, c->stream>>>(
@@ -872,8 +682,8 @@ static int pme_forces_t(simox_ctx* c, PmeRes& Rs, bool eflag, double* f_store) {
 template <typename R, int P>
 static int pme_pot_t(simox_ctx* c, PmeRes& Rs, const double* qalt, double* phi, double scale) {
     PmeParams S = pme_params(c);
-    run_spread<R, P>(c, Rs, S, qalt);
-    int st = run_convolution(c, Rs, false);
+    int st = run_spread<R, P>(c, Rs, S, qalt);
+    if (!st) st = run_convolution(c, Rs, false);
     if (st) return st;
     Launch L(c, "pme_gather_pot");
     gather_pot_kernel<R, P><<<(S.n + 127) / 128, 128, 0, c->stream>>>(S, c->xq_s, (const R*)Rs.grid, phi, scale);
@@ -1037,8 +847,8 @@ template <int P>
 static int force_charge_adjoint_t(simox_ctx* c, PmeRes& Rs, const double* wt, double* out) {
     PmeParams S = pme_params(c);
     const int nb = (S.n + 127) / 128;
-    run_spread<double, P>(c, Rs, S, nullptr);
-    int st = run_convolution(c, Rs, false);
+    int st = run_spread<double, P>(c, Rs, S, nullptr);
+    if (!st) st = run_convolution(c, Rs, false);
     if (st) return st;
     {
         Launch L(c, "adjoint_pme_field");
@@ -1092,7 +902,7 @@ int pme_potential(simox_ctx* c, const double* qalt, double* phi, double scale) {
 template <typename R, int P>
 static int pme_grid_t(simox_ctx* c, PmeRes& Rs, const double* qalt) {
     PmeParams S = pme_params(c);
-    run_spread<R, P>(c, Rs, S, qalt);
+    if (int st = run_spread<R, P>(c, Rs, S, qalt)) return st;
     return run_convolution(c, Rs, false);
 }
 

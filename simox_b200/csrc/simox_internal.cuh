@@ -127,6 +127,7 @@ struct PmeRes {
     void* grid = nullptr;       // real grid K1*K2*K3 (x fastest)
     void* cgrid = nullptr;      // half-spectrum complex grid
     void* infl = nullptr;       // G/N on the half spectrum
+    unsigned long long* acc = nullptr;   // spread sums, 64-bit fixed point (zero between spreads)
     cufftHandle r2c = 0, c2r = 0;
 };
 
@@ -219,7 +220,6 @@ struct simox_ctx {
     int* t_s = nullptr;         // species 0..4
     float4* rec_s = nullptr;    // skin filter record in pair order: skin-cell offset, (cell, species)
     float4* frec_s = nullptr;   // skin force record in pair order: skin-cell offset, charge
-    int4* sbase = nullptr;      // PME owner spread: each atom's first stencil point (pair order)
     double4* xo_s = nullptr;    // the same offset in FP64 (x, y, z) and the charge (w): the
                                 // half-list force pass forms separations from it in FP64
     int g0_species = -1;        // the one non-oxygen species present, or -1
