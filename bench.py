@@ -609,6 +609,8 @@ def main():
                     help="profiling run: set-up, then --steps MD steps of the workload (charges as "
                          "generated, no CTIP, no comparison runs); prints nothing else")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="precision of --ncu")
+    ap.add_argument("--ncu-ctip", type=int, default=0,
+                    help="--ncu: after the set-up run this many CTIP_SOLVER CG iterations instead of MD steps")
     ap.add_argument("--freq-stat", type=int, default=FREQ_STAT,
                     help="--ncu: energies on steps with MOD(step, freq_stat) == 0 (1: every step)")
     ap.add_argument("--batch", type=int, default=0,
@@ -633,8 +635,11 @@ def main():
         s = build_system()
         g = equilibrated_context(s, args.precision)
         from simox_b200 import systems as S
-        g.md_run(args.steps, 1.0 / S.TFM, first_step=2, thermostat=True, T_given=600.0 * S.KB, freq_new=FREQ_NEW,
-                 freq_sort=1, freq_stat=args.freq_stat)
+        if args.ncu_ctip:
+            g.ctip_solver(max_cg=args.ncu_ctip)
+        else:
+            g.md_run(args.steps, 1.0 / S.TFM, first_step=2, thermostat=True, T_given=600.0 * S.KB,
+                     freq_new=FREQ_NEW, freq_sort=1, freq_stat=args.freq_stat)
         g.sync()
         g.close()
         return 0
