@@ -610,7 +610,8 @@ def main():
                          "generated, no CTIP, no comparison runs); prints nothing else")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="precision of --ncu")
     ap.add_argument("--ncu-ctip", type=int, default=0,
-                    help="--ncu: after the set-up run this many CTIP_SOLVER CG iterations instead of MD steps")
+                    help="--ncu: after the set-up run this many CTIP_SOLVER CG iterations (host-driven loop) "
+                         "instead of MD steps")
     ap.add_argument("--freq-stat", type=int, default=FREQ_STAT,
                     help="--ncu: energies on steps with MOD(step, freq_stat) == 0 (1: every step)")
     ap.add_argument("--batch", type=int, default=0,
@@ -636,7 +637,9 @@ def main():
         g = equilibrated_context(s, args.precision)
         from simox_b200 import systems as S
         if args.ncu_ctip:
+            g.profile(True)   # host-driven CG loop: every iteration's kernels are plain launches
             g.ctip_solver(max_cg=args.ncu_ctip)
+            g.profile(False)
         else:
             g.md_run(args.steps, 1.0 / S.TFM, first_step=2, thermostat=True, T_given=600.0 * S.KB,
                      freq_new=FREQ_NEW, freq_sort=1, freq_stat=args.freq_stat)

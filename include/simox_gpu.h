@@ -372,7 +372,7 @@ int simox_adjoint_eval_many(simox_ctx* const* ctxs, int m, const double* const* 
  * depend on it: every atom's force is summed by one warp in the same order
  * whatever the CTA split. */
 typedef struct {
-    int force_splits;    /* CTAs per skin cell in the mixed pair passes, 1..16 (default 2) */
+    int force_splits;    /* CTAs per skin cell in the mixed pair passes, 1..16 (default 1) */
     int half_list;       /* get only: 1 when the current pair order keeps each pair once (mixed
                             precision, skin list, one metal species plus oxygen); the neighbour
                             statistics then count pairs, not list entries of both atoms      */
