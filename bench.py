@@ -234,11 +234,13 @@ def time_device(g, s, steps, warmup, dist, device):
     barrier(dist, device)
     g.sync()
     l0 = g.launch_count()
+    r0 = g.skin_rebuilds()
     g.timer_begin()
     e = run_md(g, s, warmup + 1, steps, rdf)
     ms = g.timer_end()
     g.sync()
     launches = g.launch_count() - l0
+    time_device.rebuilds = g.skin_rebuilds() - r0
     barrier(dist, device)
     return ms, e, launches, warm_s
 
@@ -275,9 +277,12 @@ def time_e2e(g, s, steps, first):
 
 
 def profile_steps(g, s, steps, first):
+    """Per-kernel event spans of `steps` eager steps run like the timed ones
+    (RDF accumulated every step, energies on the status steps)."""
+    from simox_b200 import _abi
     g.profile(True)
     g.profile_reset()
-    run_md(g, s, first, steps, None)
+    run_md(g, s, first, steps, np.zeros(_abi.RDF_LEN, np.int32))
     prof = g.profile_read()
     g.profile(False)
     return prof
@@ -662,6 +667,7 @@ def main():
     g = equilibrated_context(s, "mixed", device=local)
     clocks = ClockSampler(local)
     ms, e, launches, warm_s = time_device(g, s, args.steps, args.warmup, dist, device)
+    rebuilds = time_device.rebuilds
     clk = clocks.stop()
     ms_max = reduce_max(dist, ms, device)
     value = world * s.n * args.steps / (ms_max / 1e3)
@@ -730,7 +736,8 @@ def main():
             ctip_fp64 = ctip_object(g64, "fp64")
         g64.close()
         ms64 = reduce_max(dist, ms64, device)
-        fp64 = {"value": world * s.n * args.steps / (ms64 / 1e3), "unit": UNIT, "ms_per_step": ms64 / args.steps}
+        fp64 = {"value": world * s.n * args.steps / (ms64 / 1e3), "unit": UNIT, "ms_per_step": ms64 / args.steps,
+                "skin_rebuilds_in_timed_steps": time_device.rebuilds}
 
     ferr = force_error(s, device=local)
 
@@ -768,6 +775,7 @@ def main():
             "force_err_vs_fp64": ferr,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
             "gpu_launches": launches,
+            "skin_rebuilds_in_timed_steps": rebuilds,
             "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                          "traffic_over_algorithmic": (traffic / dom_bytes) if traffic else None,

@@ -303,6 +303,9 @@ int simox_launch_count(simox_ctx* ctx, long long* n);
 int simox_sync(simox_ctx* ctx);
 /* Neighbour statistics of the last list build: max and total list length. */
 int simox_neighbor_stats(simox_ctx* ctx, int* max_nnb, long long* total_nnb);
+/* Skin-list rebuilds (the device decides when an atom moved more than
+ * skin/2) since the skin grid was set up. */
+int simox_skin_rebuilds(simox_ctx* ctx, long long* n);
 
 /* ---- parameter adjoint ---------------------------------------------------
  * No counterpart in the reference (which has fixed parameters and no

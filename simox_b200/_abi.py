@@ -141,7 +141,7 @@ EXPORTED = [
     "simox_checkpoint_write", "simox_checkpoint_read", "simox_format_status",
     "simox_md_run", "simox_timer_begin", "simox_timer_end", "simox_profile_enable",
     "simox_profile_read", "simox_profile_reset", "simox_launch_count", "simox_sync",
-    "simox_neighbor_stats", "simox_cell_sort_noalloc",
+    "simox_neighbor_stats", "simox_skin_rebuilds", "simox_cell_sort_noalloc",
     "simox_set_tuning", "simox_get_tuning",
     "simox_batch_create", "simox_batch_destroy", "simox_batch_md_run", "simox_batch_autotune",
     "simox_batch_launch_count",

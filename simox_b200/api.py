@@ -82,6 +82,7 @@ def lib():
         "simox_launch_count": [_vp, C.POINTER(C.c_longlong)],
         "simox_sync": [_vp],
         "simox_neighbor_stats": [_vp, _ip, C.POINTER(C.c_longlong)],
+        "simox_skin_rebuilds": [_vp, C.POINTER(C.c_longlong)],
         "simox_cell_sort_noalloc": [_vp, C.c_int, _dp, C.c_double, _vp, _vp, C.c_int, _vp],
         "simox_set_tuning": [_vp, C.POINTER(Tuning)],
         "simox_get_tuning": [_vp, C.POINTER(Tuning)],
@@ -474,6 +475,12 @@ class Simox:
         t = Tuning()
         _check(lib().simox_get_tuning(self._ctx, C.byref(t)), "get_tuning")
         return {"force_splits": t.force_splits, "half_list": t.half_list}
+
+    def skin_rebuilds(self) -> int:
+        """Skin-list rebuilds so far (decided on the device)."""
+        n = C.c_longlong(0)
+        _check(lib().simox_skin_rebuilds(self._ctx, C.byref(n)), "skin_rebuilds")
+        return n.value
 
     def neighbor_stats(self):
         """(longest exact-list row, total exact-list entries).  With the half

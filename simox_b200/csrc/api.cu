@@ -978,6 +978,15 @@ extern "C" int simox_sync(simox_ctx* c) {
     return cuda_status(cudaStreamSynchronize(c->stream));
 }
 
+extern "C" int simox_skin_rebuilds(simox_ctx* c, long long* n) {
+    if (!c || !n) return SIMOX_E_ARG;
+    int v[2] = {0, 0};
+    if (c->skin_flag) cudaMemcpyAsync(v, c->skin_flag, sizeof(v), cudaMemcpyDeviceToHost, c->stream);
+    int st = cuda_status(cudaStreamSynchronize(c->stream));
+    *n = v[1];
+    return st;
+}
+
 extern "C" int simox_neighbor_stats(simox_ctx* c, int* max_nnb, long long* total_nnb) {
     if (!c) return SIMOX_E_ARG;
     int mx = 0;

@@ -497,12 +497,14 @@ __global__ void skin_check_kernel(int n, const double* __restrict__ x, const dou
     if (__any_sync(0xffffffffu, need) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
 }
 
-// bin on the skin grid and remember the positions of this rebuild
+// bin on the skin grid and remember the positions of this rebuild;
+// cond[0] = rebuild flag, cond[1] counts the rebuilds
 __global__ void skin_bin_kernel(int n, const double* __restrict__ x, double3 hbox, double3 ilc, int3 nc,
                                 int* __restrict__ cell_of, int* __restrict__ count, double* __restrict__ x0,
-                                const int* __restrict__ cond) {
-    if (*cond == 0) return;
+                                int* __restrict__ cond) {
+    if (cond[0] == 0) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) cond[1] += 1;
     if (i >= n) return;
     const double xx[3] = {x[3 * i], x[3 * i + 1], x[3 * i + 2]};
     const double h[3] = {hbox.x, hbox.y, hbox.z}, il[3] = {ilc.x, ilc.y, ilc.z};
@@ -654,7 +656,8 @@ int setup_skin(simox_ctx* c) {
               cudaMalloc(&c->cs_entries, sizeof(int) * c->ncell_s * kEntries) == cudaSuccess &&
               cudaMalloc(&c->perm, sizeof(int) * N) == cudaSuccess &&
               cudaMalloc(&c->x0, sizeof(double) * 3 * N) == cudaSuccess &&
-              cudaMalloc(&c->skin_flag, sizeof(int)) == cudaSuccess &&
+              cudaMalloc(&c->skin_flag, 2 * sizeof(int)) == cudaSuccess &&
+              cudaMemset(c->skin_flag, 0, 2 * sizeof(int)) == cudaSuccess &&
               cudaMalloc(&c->nn_s, sizeof(int) * 2 * N) == cudaSuccess &&
               cudaMalloc(&c->nbr_s, sizeof(unsigned) * N * (size_t)c->cap_s) == cudaSuccess;
     if (!ok) return SIMOX_E_NOMEM;

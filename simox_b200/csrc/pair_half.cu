@@ -50,11 +50,9 @@ constexpr int kHalfFirst = 13;                            // stencil position of
 constexpr int kHalfCells = 14;                            // positions 13..26
 constexpr int kSelf = 13;
 
-// pass 1: 256 threads; the tile's filter records and split density sums for
-// up to 3,072 tile atoms (72 KB: three CTAs per SM)
+// pass 1: 256 threads, shared density accumulators for up to 4,096 tile atoms
 constexpr int kH1Threads = 256;
-constexpr int kH1Cap = 3072;
-constexpr size_t kH1Smem = (size_t)kH1Cap * (sizeof(float4) + 2 * sizeof(unsigned));
+constexpr int kH1Cap = 4096;
 // pass 2 and the charge solver: 1024 threads (64 registers), one CTA per SM,
 // dynamic tiles; 32 resident warps hide the pair function's latency chains
 // (0.407 ms for the 128k corundum force pass against 0.43 ms at 512 threads)
@@ -173,22 +171,15 @@ __device__ __forceinline__ int filter_group_half(const Half1Params& H, const flo
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     auto ent = [&](int k) { return k < mg ? sp[G == 0 ? k : -k] : 0u; };
-    // tile slot of an entry's partner (TILED: rec is the CTA's tile of records)
-    auto slot_of = [&](unsigned e) {
-        // stencil positions below 13 never occur in a half row: clamp into range anyway
-        int sl = TILED ? (int)(e & kSkinIdxMask) + delta[max((int)(e >> kSkinCodeShift) - kHalfFirst, 0)]
-                       : (int)(e & kSkinIdxMask);
-        return (unsigned)sl < (unsigned)lim ? sl : 0;
-    };
     unsigned E1 = ent(lane), E2 = ent(lane + 32);
-    float4 rb1 = rec[slot_of(E1)];
+    float4 rb1 = rec[E1 & kSkinIdxMask];
     int out = 0;
     for (int base = 0; base < mg; base += 32) {
         const int k = base + lane;
         const unsigned e = E1;
         const float4 rb = rb1;
         E1 = E2;
-        rb1 = rec[slot_of(E1)];
+        rb1 = rec[E1 & kSkinIdxMask];
         E2 = ent(k + 64);
         const unsigned Y = e & kSkinIdxMask;
         const int code = (int)(e >> kSkinCodeShift);
@@ -212,7 +203,12 @@ __device__ __forceinline__ int filter_group_half(const Half1Params& H, const flo
         const float r = r2 * rsqrt_approx(r2);
         const float vX = dens_term<float>(du, r), vY = dens_term<float>(dv, r);
         rho += keep ? (double)vX : 0.0;
-        if (keep) acc.add(0, slot_of(e), __float2ll_rn(vY * kRhoScale));
+        if (keep) {
+            // stencil positions below 13 never occur in a half row: clamp into range anyway
+            int slot = TILED ? (int)Y + delta[max(code - kHalfFirst, 0)] : (int)Y;
+            slot = (unsigned)slot < (unsigned)lim ? slot : 0;
+            acc.add(0, slot, __float2ll_rn(vY * kRhoScale));
+        }
     }
     return out;
 }
@@ -220,7 +216,7 @@ __device__ __forceinline__ int filter_group_half(const Half1Params& H, const flo
 template <bool TILED>
 __device__ __forceinline__ void filter_half_atoms(const Half1Params& H, const float4* ssh, const DensC<float>* dsh,
                                                   int b0, int b1, int a0, int* next, const double4* __restrict__ xq,
-                                                  const float4* __restrict__ rec, const float4* prec,
+                                                  const float4* __restrict__ rec, const int* __restrict__ order,
                                                   const int2* __restrict__ nn_s, const unsigned* __restrict__ nbr_s,
                                                   int2* __restrict__ nn, unsigned* __restrict__ nbr, const int* delta,
                                                   int lim, const Sink<TILED>& acc, int& lmax, unsigned long long& ltot,
@@ -246,10 +242,10 @@ __device__ __forceinline__ void filter_half_atoms(const Half1Params& H, const fl
         unsigned* row = nbr + (size_t)X * F.pp.cap;
         double rho = 0.0;
         const int out0 = filter_group_half<0, TILED>(H, ssh, dsh[(sX << 3) | g0], dsh[(g0 << 3) | sX], sX, g0,
-                                                     srow, ms.x, row, ra, X, xq, prec, delta, lim, acc, rho);
+                                                     srow, ms.x, row, ra, X, xq, rec, delta, lim, acc, rho);
         const int out1 = filter_group_half<1, TILED>(H, ssh, dsh[(sX << 3) | 3], dsh[(3 << 3) | sX], sX, 3,
                                                      srow + (F.cap_s - 1), ms.y, row + (F.pp.cap - 1), ra, X, xq,
-                                                     prec, delta, lim, acc, rho);
+                                                     rec, delta, lim, acc, rho);
         rho = warp_sum(rho);
         if (lane == 0) {
             const int tot = out0 + out1;
@@ -273,10 +269,7 @@ __global__ void __launch_bounds__(kH1Threads)
                        const int2* __restrict__ nn_s, const unsigned* __restrict__ nbr_s, int2* __restrict__ nn,
                        unsigned* __restrict__ nbr, u64* __restrict__ rho_fx, int* __restrict__ status,
                        int* __restrict__ nn_max, unsigned long long* __restrict__ nn_tot) {
-    extern __shared__ __align__(16) unsigned char filter_smem[];
-    float4* trec = reinterpret_cast<float4*>(filter_smem);               // the tile's filter records
-    unsigned* alo = reinterpret_cast<unsigned*>(trec + kH1Cap);          // density sums, low words
-    unsigned* ahi = alo + kH1Cap;                                         // high words
+    __shared__ unsigned alo[kH1Cap], ahi[kH1Cap];
     __shared__ DensC<float> dsh[64];
     __shared__ int dflag[64];
     __shared__ float4 ssh[kEntries];
@@ -308,17 +301,11 @@ __global__ void __launch_bounds__(kH1Threads)
     const int b0 = br.x, b1 = br.y;
     const bool tiled = total <= kH1Cap;
     if (tid < kHalfCells) delta[tid] = T.off[tid] - T.start[tid];
-    if (tiled) {
-        int t = 0;
+    if (tiled)
         for (int i = tid; i < total; i += blockDim.x) {
-            while (T.off[t + 1] <= i) t++;
-            cp_async16(&trec[i], rec + T.start[t] + (i - T.off[t]));
             alo[i] = 0u;
             ahi[i] = 0u;
         }
-        cp_async_commit();
-        cp_async_wait<0>();
-    }
     __syncthreads();
     const int g0 = H.g0;
     const int a0 = T.start[0];
@@ -328,10 +315,10 @@ __global__ void __launch_bounds__(kH1Threads)
         // the four pair kinds of this path (the metal g0 and oxygen)
         bad = dflag[(g0 << 3) | g0] | dflag[(g0 << 3) | 3] | dflag[(3 << 3) | g0] | dflag[(3 << 3) | 3];
         if (tiled)
-            filter_half_atoms<true>(H, ssh, dsh, b0, b1, a0, &next, xq, rec, trec, nn_s, nbr_s, nn, nbr, delta,
+            filter_half_atoms<true>(H, ssh, dsh, b0, b1, a0, &next, xq, rec, order, nn_s, nbr_s, nn, nbr, delta,
                                     total, Sink<true>{alo, ahi, 0, rho_fx, 0}, lmax, ltot, bad);
         else
-            filter_half_atoms<false>(H, ssh, dsh, b0, b1, a0, &next, xq, rec, rec, nn_s, nbr_s, nn, nbr, delta,
+            filter_half_atoms<false>(H, ssh, dsh, b0, b1, a0, &next, xq, rec, order, nn_s, nbr_s, nn, nbr, delta,
                                      H.F.pp.n, Sink<false>{rho_fx, 0}, lmax, ltot, bad);
     }
     if (bad) atomicOr(status, bad);
@@ -876,12 +863,20 @@ __global__ void __launch_bounds__(kHEThreads, 6)
         const unsigned* row = nbr + (size_t)X * P.cap;
         double rho = 0.0;
         if (sX < kSpecies) {
+            // the next entry's partner data is loaded before this entry's arithmetic
+            int Yn = 0, sYn = 0;
+            double4 xbn = make_double4(0.0, 0.0, 0.0, 0.0);
+            auto fetch = [&](int k) {
+                Yn = (int)(row[row_slot(2, k, P.cap, m.x)] & kIdxMask);
+                sYn = ts[Yn];
+                xbn = xq[Yn];
+            };
+            if (lane < mt) fetch(lane);
             for (int k = lane; k < mt; k += 32) {
-                const unsigned ent = row[row_slot(2, k, P.cap, m.x)];
-                const int Y = (int)(ent & kIdxMask);
-                const int sY = ts[Y];
+                const int Y = Yn, sY = sYn;
+                const double4 xb = xbn;
+                if (k + 32 < mt) fetch(k + 32);
                 if (sY >= kSpecies) { bad |= ST_UNKNOWN_PAIR; continue; }
-                const double4 xb = xq[Y];
                 double dx, dy, dz;
                 min_image(xa, xb, P, dx, dy, dz);
                 const double r = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
@@ -925,13 +920,11 @@ bool half_path(const simox_ctx* c) { return c->using_skin && c->skin_half; }
 static int half_prepare(int device) {
     static std::atomic<bool> done[64] = {};   // contexts may run on several host threads
     if (device >= 0 && device < 64 && done[device].load()) return SIMOX_OK;
-    cudaError_t e0 = cudaFuncSetAttribute(filter_half_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kH1Smem);
     cudaError_t e1 = cudaFuncSetAttribute(force_half_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kH2Smem);
     cudaError_t e4 = cudaFuncSetAttribute(force_half_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kH2Smem);
     cudaError_t e2 = cudaFuncSetAttribute(ctip_half_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHCSmem);
     cudaError_t e3 = cudaFuncSetAttribute(ctip_half_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHCSmem);
-    if (e0 != cudaSuccess || e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess || e4 != cudaSuccess)
-        return SIMOX_E_CUDA;
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess || e4 != cudaSuccess) return SIMOX_E_CUDA;
     if (device >= 0 && device < 64) done[device] = true;
     return SIMOX_OK;
 }
@@ -953,7 +946,7 @@ int filter_density_half(simox_ctx* c) {
     if (c->n > 0) {
         Launch L(c, "neighbor_filter_density");
         const int g = c->ncell_s * H.splits;
-        filter_half_kernel<<<g, kH1Threads, kH1Smem, c->stream>>>(
+        filter_half_kernel<<<g, kH1Threads, 0, c->stream>>>(
             H, c->tab_f, c->xq_s, c->rec_s, c->pair_order, c->cs_start, c->cs_entries,
             reinterpret_cast<const int2*>(c->nn_s), c->nbr_s, reinterpret_cast<int2*>(c->nn), c->nbr, c->rho_fx,
             c->status, c->nn_max, c->nn_tot);

@@ -212,7 +212,7 @@ struct simox_ctx {
     int* cs_entries = nullptr;
     int* perm = nullptr;
     double* x0 = nullptr;       // positions at the last skin rebuild (original order)
-    int* skin_flag = nullptr;   // device: rebuild needed
+    int* skin_flag = nullptr;   // device: [0] rebuild needed, [1] rebuilds so far
     int* nn_s = nullptr;        // skin list counts (int2)
     unsigned* nbr_s = nullptr;  // skin list rows [cap*cap_s]
 
