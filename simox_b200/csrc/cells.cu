@@ -23,7 +23,10 @@
 
 namespace sx {
 
-constexpr int LB_THREADS = 128;
+// list build: one thread per home atom of a cell (a skin cell of the 128k
+// corundum holds ~180 atoms: with 128 threads a third of them walked two
+// home atoms one after the other)
+constexpr int LB_THREADS = 256;
 constexpr int LB_TILE = 1024;
 
 // ---------------------------------------------------------------------------
