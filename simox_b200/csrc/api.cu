@@ -134,11 +134,8 @@ int md_step(simox_ctx* c, const simox_md_opts* o, bool sort, bool estep, bool wa
     // adds them: f = f_pair + f_rec - Fsum/N, as FORCE + PME would leave f.
     if ((st = ensure_gathered(c))) return st;
     if ((st = pme_fork(c, estep))) return st;
-    c->estep_pending = estep;
-    st = ensure_list(c);
-    if (!st) st = eam_density(c, estep);
-    c->estep_pending = false;
-    if (st) return st;
+    if ((st = ensure_list(c))) return st;
+    if ((st = eam_density(c, estep))) return st;
     if ((st = pair_forces(c, estep, want_rdf))) return st;
     cudaStreamWaitEvent(c->stream, c->ev_join, 0);
     if (stoch) st = nvt2_stoch(c, o->dt, o->alpha, o->T_given, o->seed, c->md_step_no, true, c->f_rec);
@@ -238,11 +235,8 @@ int md_run(simox_ctx* c, const simox_md_opts* o, int first, int nsteps, simox_en
             // the rest of the step: FORCE, PME, VV2 (VV1 and CELL_SORT done)
             if ((st = ensure_gathered(c))) return st;
             if ((st = pme_fork(c, estep))) return st;
-            c->estep_pending = estep;
-            st = ensure_list(c);
-            if (!st) st = eam_density(c, estep);
-            c->estep_pending = false;
-            if (st) return st;
+            if ((st = ensure_list(c))) return st;
+            if ((st = eam_density(c, estep))) return st;
             if ((st = pair_forces(c, estep, want_rdf))) return st;
             cudaStreamWaitEvent(c->stream, c->ev_join, 0);
             if (stoch) st = nvt2_stoch(c, o2.dt, o2.alpha, o2.T_given, o2.seed, c->md_step_no, true, c->f_rec);
@@ -387,7 +381,7 @@ static void free_ctx(simox_ctx* c) {
                     c->sorted, c->pair13, c->entries, c->xq_s, c->t_s, c->rec_s, c->frec_s, c->xo_s, c->nn, c->nbr, c->nn_max, c->nn_tot,
                     c->cs_count, c->cs_start, c->cs_fill, c->cs_cell_of, c->cs_entries, c->perm, c->x0,
                     c->skin_flag, c->nn_s, c->nbr_s, c->rho_s, c->dF_s, c->dF_f, c->tab_d, c->tab_f, c->c_const, c->g, c->pv, c->Ap, c->qs, c->jp,
-                    c->act, c->line, c->acc, c->status, c->rdf, c->f_rec, c->rho_fx, c->rho64_fx, c->fx_acc};
+                    c->act, c->line, c->acc, c->status, c->rdf, c->f_rec, c->rho_fx, c->fx_acc};
     for (void* p : bufs)
         if (p) cudaFree(p);
     if (c->h_acc) cudaFreeHost(c->h_acc);
@@ -487,7 +481,6 @@ extern "C" int simox_create(const simox_setup* s, const simox_potential* pot, si
               dalloc(&c->xo_s, N) && dalloc(&c->nn, 2 * N) &&
               dalloc(&c->nbr, N * (size_t)c->nnb_cap) && dalloc(&c->nn_max, 1) && dalloc(&c->nn_tot, 1) &&
               dalloc(&c->rho_s, N) && dalloc(&c->dF_s, N) && dalloc(&c->dF_f, N) && dalloc(&c->rho_fx, N) &&
-              dalloc(&c->rho64_fx, N) &&
               dalloc(&c->fx_acc, 3 * N) && dalloc(&c->tab_d, kSpecies * kSpecies) &&
               dalloc(&c->tab_f, kSpecies * kSpecies) && dalloc(&c->line, 64) && dalloc(&c->acc, A_COUNT) &&
               dalloc(&c->status, 1) && dalloc(&c->rdf, SIMOX_RDF_LEN);
@@ -658,11 +651,7 @@ extern "C" int simox_force(simox_ctx* c, simox_energies* e, int* rdf) {
     cudaMemsetAsync(c->acc, 0, sizeof(double) * (A_EGROUP + 1), c->stream);
     if (rdf) cudaMemsetAsync(c->rdf, 0, sizeof(int) * SIMOX_RDF_LEN, c->stream);
     int st;
-    c->estep_pending = eflag;
-    st = ensure_list(c);
-    if (!st) st = eam_density(c, eflag);
-    c->estep_pending = false;
-    if (st || (st = pair_forces(c, eflag, rdf != nullptr))) return st;
+    if ((st = ensure_list(c)) || (st = eam_density(c, eflag)) || (st = pair_forces(c, eflag, rdf != nullptr))) return st;
     if ((st = read_status(c))) return st;
     cudaMemcpyAsync(c->h_acc, c->acc, sizeof(double) * A_COUNT, cudaMemcpyDeviceToHost, c->stream);
     std::vector<int> h;

@@ -159,20 +159,13 @@ struct Half1Params {
 // row front; G = 1: oxygen at the back).  Kept entries are compacted into X's
 // exact half row; their density at X
 // is summed in rho and their density at Y is added to Y's accumulator.
-// FP64 energy terms of an energy step, summed by the filter pass: X's FP64
-// density and the pair energies (Y's FP64 density goes into fixed-point sums)
-struct EnergyAcc {
-    double rhoX, ep, ed, ec;
-};
-
-template <int G, bool TILED, bool E>
+template <int G, bool TILED>
 __device__ __forceinline__ int filter_group_half(const Half1Params& H, const float4* ssh, const DensC<float>& du,
                                                  const DensC<float>& dv, int sX, int sY,
                                                  const unsigned* __restrict__ sp, int mg, unsigned* __restrict__ dp,
                                                  const float4& ra, int X, const double4* __restrict__ xq,
                                                  const float4* __restrict__ rec, const int* delta, int lim,
-                                                 const Sink<TILED>& acc, double& rho, const PairTab<double>* etab,
-                                                 u64* __restrict__ rho64, EnergyAcc& ea) {
+                                                 const Sink<TILED>& acc, double& rho) {
     const FilterParams& F = H.F;
     const PairParams& P = F.pp;
     const int lane = threadIdx.x & 31;
@@ -216,30 +209,18 @@ __device__ __forceinline__ int filter_group_half(const Half1Params& H, const flo
             slot = (unsigned)slot < (unsigned)lim ? slot : 0;
             acc.add(0, slot, __float2ll_rn(vY * kRhoScale));
         }
-        if (E && keep) {   // FP64 energies (force.f90:84-98, 101-140), once per pair
-            const double4 xa = xq[X], xb = xq[Y];
-            double ddx, ddy, ddz;
-            min_image(xa, xb, P, ddx, ddy, ddz);
-            const double rr = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)), __dmul_rn(ddz, ddz)));
-            const PairTab<double>& T = etab[(sX == H.g0 ? 0 : 2) + (sY == H.g0 ? 0 : 1)];
-            ea.rhoX += T.d_fe * zhou_val<double>(rr, T.d_inv_re, T.d_c, T.d_lam);                 // force.f90:84
-            const double rY = T.e_fe * zhou_val<double>(rr, T.e_inv_re, T.e_c, T.e_lam);         // force.f90:85
-            add_fixed(rho64 + Y, __double2ll_rn(rY * kRhoScaleD));
-            pair_energy_fp64(T, rr, 1.0 / rr, xa.w, xb.w, P.a, ea.ep, ea.ed, ea.ec);
-        }
     }
     return out;
 }
 
-template <bool TILED, bool E>
+template <bool TILED>
 __device__ __forceinline__ void filter_half_atoms(const Half1Params& H, const float4* ssh, const DensC<float>* dsh,
                                                   int b0, int b1, int a0, int* next, const double4* __restrict__ xq,
                                                   const float4* __restrict__ rec, const int* __restrict__ order,
                                                   const int2* __restrict__ nn_s, const unsigned* __restrict__ nbr_s,
                                                   int2* __restrict__ nn, unsigned* __restrict__ nbr, const int* delta,
                                                   int lim, const Sink<TILED>& acc, int& lmax, unsigned long long& ltot,
-                                                  int& bad, const PairTab<double>* etab, u64* __restrict__ rho64,
-                                                  EnergyAcc& en) {
+                                                  int& bad) {
     const FilterParams& F = H.F;
     const int lane = threadIdx.x & 31;
     const int g0 = H.g0;
@@ -260,18 +241,12 @@ __device__ __forceinline__ void filter_half_atoms(const Half1Params& H, const fl
         const unsigned* srow = nbr_s + (size_t)X * F.cap_s;
         unsigned* row = nbr + (size_t)X * F.pp.cap;
         double rho = 0.0;
-        en.rhoX = 0.0;
-        const int out0 = filter_group_half<0, TILED, E>(H, ssh, dsh[(sX << 3) | g0], dsh[(g0 << 3) | sX], sX, g0,
-                                                        srow, ms.x, row, ra, X, xq, rec, delta, lim, acc, rho, etab,
-                                                        rho64, en);
-        const int out1 = filter_group_half<1, TILED, E>(H, ssh, dsh[(sX << 3) | 3], dsh[(3 << 3) | sX], sX, 3,
-                                                        srow + (F.cap_s - 1), ms.y, row + (F.pp.cap - 1), ra, X, xq,
-                                                        rec, delta, lim, acc, rho, etab, rho64, en);
+        const int out0 = filter_group_half<0, TILED>(H, ssh, dsh[(sX << 3) | g0], dsh[(g0 << 3) | sX], sX, g0,
+                                                     srow, ms.x, row, ra, X, xq, rec, delta, lim, acc, rho);
+        const int out1 = filter_group_half<1, TILED>(H, ssh, dsh[(sX << 3) | 3], dsh[(3 << 3) | sX], sX, 3,
+                                                     srow + (F.cap_s - 1), ms.y, row + (F.pp.cap - 1), ra, X, xq,
+                                                     rec, delta, lim, acc, rho);
         rho = warp_sum(rho);
-        if (E) {
-            const double r64 = warp_sum(en.rhoX);
-            if (lane == 0) add_fixed(rho64 + X, __double2ll_rn(r64 * kRhoScaleD));
-        }
         if (lane == 0) {
             const int tot = out0 + out1;
             if (tot > F.pp.cap) {
@@ -287,18 +262,14 @@ __device__ __forceinline__ void filter_half_atoms(const Half1Params& H, const fl
     }
 }
 
-template <bool E>
 __global__ void __launch_bounds__(kH1Threads)
     filter_half_kernel(const __grid_constant__ Half1Params H, const PairTab<float>* __restrict__ tab,
                        const double4* __restrict__ xq, const float4* __restrict__ rec, const int* __restrict__ order,
                        const int* __restrict__ cs_start, const int* __restrict__ cs_entries,
                        const int2* __restrict__ nn_s, const unsigned* __restrict__ nbr_s, int2* __restrict__ nn,
                        unsigned* __restrict__ nbr, u64* __restrict__ rho_fx, int* __restrict__ status,
-                       int* __restrict__ nn_max, unsigned long long* __restrict__ nn_tot,
-                       const PairTab<double>* __restrict__ tab_d, u64* __restrict__ rho64, double* __restrict__ eacc) {
+                       int* __restrict__ nn_max, unsigned long long* __restrict__ nn_tot) {
     __shared__ unsigned alo[kH1Cap], ahi[kH1Cap];
-    __shared__ PairTab<double> etab[E ? 4 : 1];   // (metal, metal), (metal, O), (O, metal), (O, O)
-    __shared__ double red[kH1Threads / 32];
     __shared__ DensC<float> dsh[64];
     __shared__ int dflag[64];
     __shared__ float4 ssh[kEntries];
@@ -322,10 +293,6 @@ __global__ void __launch_bounds__(kH1Threads)
         dflag[k] = fl;
     }
     for (int k = tid; k < kEntries; k += blockDim.x) ssh[k] = H.F.sh[k];
-    if (E && tid < 4) {
-        const int a = tid < 2 ? H.g0 : 3, b = (tid & 1) ? 3 : H.g0;
-        etab[tid] = tab_d[a * kSpecies + b];
-    }
     if (tid == 0) next = 0;
     const int cell = blockIdx.x / H.splits, part = blockIdx.x - cell * H.splits;
     half_tile_setup(T, cs_start, cs_entries, cell);
@@ -344,21 +311,15 @@ __global__ void __launch_bounds__(kH1Threads)
     const int a0 = T.start[0];
     int lmax = 0, bad = 0;
     unsigned long long ltot = 0;
-    EnergyAcc en{0.0, 0.0, 0.0, 0.0};
     if (b1 > b0) {
         // the four pair kinds of this path (the metal g0 and oxygen)
         bad = dflag[(g0 << 3) | g0] | dflag[(g0 << 3) | 3] | dflag[(3 << 3) | g0] | dflag[(3 << 3) | 3];
         if (tiled)
-            filter_half_atoms<true, E>(H, ssh, dsh, b0, b1, a0, &next, xq, rec, order, nn_s, nbr_s, nn, nbr, delta,
-                                       total, Sink<true>{alo, ahi, 0, rho_fx, 0}, lmax, ltot, bad, etab, rho64, en);
+            filter_half_atoms<true>(H, ssh, dsh, b0, b1, a0, &next, xq, rec, order, nn_s, nbr_s, nn, nbr, delta,
+                                    total, Sink<true>{alo, ahi, 0, rho_fx, 0}, lmax, ltot, bad);
         else
-            filter_half_atoms<false, E>(H, ssh, dsh, b0, b1, a0, &next, xq, rec, order, nn_s, nbr_s, nn, nbr, delta,
-                                        H.F.pp.n, Sink<false>{rho_fx, 0}, lmax, ltot, bad, etab, rho64, en);
-    }
-    if (E) {
-        block_add<kH1Threads>(en.ep, eacc, A_EPAIR, red);
-        block_add<kH1Threads>(en.ed, eacc, A_EDIR, red);
-        block_add<kH1Threads>(en.ec, eacc, A_ECTIP, red);
+            filter_half_atoms<false>(H, ssh, dsh, b0, b1, a0, &next, xq, rec, order, nn_s, nbr_s, nn, nbr, delta,
+                                     H.F.pp.n, Sink<false>{rho_fx, 0}, lmax, ltot, bad);
     }
     if (bad) atomicOr(status, bad);
     if ((tid & 31) == 0) {
@@ -982,25 +943,14 @@ int filter_density_half(simox_ctx* c) {
     H.splits = std::max(1, std::min(16, c->force_splits));
     H.g0 = c->g0_species;
     cudaMemsetAsync(c->rho_fx, 0, sizeof(u64) * (size_t)c->n, c->stream);
-    // an energy step: the filter also sums the FP64 energies (the caller
-    // cleared the energy slots)
-    const bool E = c->estep_pending;
-    if (E) cudaMemsetAsync(c->rho64_fx, 0, sizeof(u64) * (size_t)c->n, c->stream);
     if (c->n > 0) {
-        Launch L(c, E ? "neighbor_filter_density_energy" : "neighbor_filter_density");
+        Launch L(c, "neighbor_filter_density");
         const int g = c->ncell_s * H.splits;
-        if (E)
-            filter_half_kernel<true><<<g, kH1Threads, 0, c->stream>>>(
-                H, c->tab_f, c->xq_s, c->rec_s, c->pair_order, c->cs_start, c->cs_entries,
-                reinterpret_cast<const int2*>(c->nn_s), c->nbr_s, reinterpret_cast<int2*>(c->nn), c->nbr, c->rho_fx,
-                c->status, c->nn_max, c->nn_tot, c->tab_d, c->rho64_fx, c->acc);
-        else
-            filter_half_kernel<false><<<g, kH1Threads, 0, c->stream>>>(
-                H, c->tab_f, c->xq_s, c->rec_s, c->pair_order, c->cs_start, c->cs_entries,
-                reinterpret_cast<const int2*>(c->nn_s), c->nbr_s, reinterpret_cast<int2*>(c->nn), c->nbr, c->rho_fx,
-                c->status, c->nn_max, c->nn_tot, c->tab_d, c->rho64_fx, c->acc);
+        filter_half_kernel<<<g, kH1Threads, 0, c->stream>>>(
+            H, c->tab_f, c->xq_s, c->rec_s, c->pair_order, c->cs_start, c->cs_entries,
+            reinterpret_cast<const int2*>(c->nn_s), c->nbr_s, reinterpret_cast<int2*>(c->nn), c->nbr, c->rho_fx,
+            c->status, c->nn_max, c->nn_tot);
     }
-    c->filter_energy_ready = E;
     if (c->n > 0) {
         Launch L(c, "eam_embed");
         embed_half_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->n, c->t_s, c->rho_fx, embed_params(c->pot),
@@ -1054,24 +1004,19 @@ int force_half(simox_ctx* c, bool rdf) {
     return check_launch(c);
 }
 
-// Energies of a mixed context: the pair energies and FP64 densities come from
-// this step's filter pass when it ran as an energy step, otherwise from a
-// separate FP64 pass over the list; then the embedding energy.
 int energy_half(simox_ctx* c) {
-    const bool from_filter = c->filter_energy_ready;
-    c->filter_energy_ready = false;   // consumed: a later call without a new filter pass recomputes
-    if (!from_filter) {
-        cudaMemsetAsync(c->rho64_fx, 0, sizeof(u64) * (size_t)c->n, c->stream);
+    cudaMemsetAsync(c->rho_fx, 0, sizeof(u64) * (size_t)c->n, c->stream);
+    {
         Launch L(c, "pair_energy_fp64");
         const int wpb = kHEThreads / 32;
         const int g = std::max(1, std::min((c->n + wpb - 1) / wpb, num_sms(c) * 12));
         energy_half_kernel<<<g, kHEThreads, 0, c->stream>>>(pair_params(c), c->tab_d, c->xq_s, c->t_s,
-                                                           reinterpret_cast<const int2*>(c->nn), c->nbr, c->rho64_fx,
+                                                           reinterpret_cast<const int2*>(c->nn), c->nbr, c->rho_fx,
                                                            c->acc, c->status);
     }
     {
         Launch L(c, "eam_embed_energy");
-        embed_energy_half_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->n, c->t_s, c->rho64_fx,
+        embed_energy_half_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->n, c->t_s, c->rho_fx,
                                                                            embed_params(c->pot), c->acc, c->status);
     }
     return check_launch(c);

@@ -234,9 +234,6 @@ struct simox_ctx {
 
     // fixed-point accumulators of the half-list passes (pair_half.cu)
     unsigned long long* rho_fx = nullptr;   // [cap] densities, 2^40
-    unsigned long long* rho64_fx = nullptr; // [cap] FP64-term densities of an energy step, 2^40
-    bool estep_pending = false;  // the coming FORCE wants energies: the half-list filter computes them
-    bool filter_energy_ready = false;   // the last half-list filter also summed the FP64 energies
     unsigned long long* fx_acc = nullptr;   // [3][cap] forces 2^32, or two charge-solver sums 2^40
 
     // EAM
