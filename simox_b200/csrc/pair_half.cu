@@ -201,7 +201,9 @@ __device__ __forceinline__ int filter_group_half(const Half1Params& H, const flo
         if (keep & (pos < P.cap)) dp[G == 0 ? pos : -pos] = e;
         out += __popc(mask);
         const float r = r2 * rsqrt_approx(r2);
-        const float vX = dens_term<float>(du, r), vY = dens_term<float>(dv, r);
+        // a same-species pair contributes the same density to both atoms
+        // (sX == sY is uniform across the warp: one X, one partner group)
+        const float vX = dens_term<float>(du, r), vY = sX == sY ? vX : dens_term<float>(dv, r);
         rho += keep ? (double)vX : 0.0;
         if (keep) {
             // stencil positions below 13 never occur in a half row: clamp into range anyway
