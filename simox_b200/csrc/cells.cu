@@ -369,67 +369,6 @@ __global__ void __launch_bounds__(LB_THREADS)
             ctag[k] = P.skin ? (unsigned)j | ((unsigned)e << kSkinCodeShift) : (unsigned)j | ((unsigned)edir[e] << 30);
         }
         __syncthreads();
-        if (FAST && P.skin) {
-            // skin list: one warp per home atom, lanes over the candidates;
-            // kept entries are compacted with ballots, so each group's row
-            // segment is written with coalesced stores in candidate order
-            // (the order of the per-thread path below)
-            const int lane = tid & 31, nw = blockDim.x >> 5;
-            const unsigned lt = (1u << lane) - 1u;
-            for (int hl = tid >> 5; hl < nh; hl += nw) {
-                const int h = h0 + hl;
-                const double4 xh = xq[h];
-                const float hx = (float)(xh.x - cen_x), hy = (float)(xh.y - cen_y), hz = (float)(xh.z - cen_z);
-                if (!(fabsf(hx) <= P.hlx && fabsf(hy) <= P.hly && fabsf(hz) <= P.hlz)) {
-                    // a home atom outside its cell (cannot happen right after the skin binning):
-                    // the exact test, one lane
-                    if (lane == 0) {
-                        int2 my = cnt[hl];
-                        unsigned* row = nbr + (size_t)h * P.cap;
-                        for (int k = 0; k < tn; k++) {
-                            const unsigned tag = ctag[k];
-                            const int j = (int)(tag & kSkinIdxMask);
-                            if (j == h || !half_keep(P, tag, j, h)) continue;
-                            if (exact_r2(xh, xq[j], P.box) < P.rcut2)
-                                list_append(row, my, P.cap, tag, __float_as_int(cpos[k].w));
-                        }
-                        cnt[hl] = my;
-                    }
-                    continue;
-                }
-                int2 my = cnt[hl];
-                unsigned* row = nbr + (size_t)h * P.cap;
-                for (int k0 = 0; k0 < tn; k0 += 32) {
-                    const int k = k0 + lane;
-                    bool keep = false;
-                    unsigned tag = 0u;
-                    int sp = 0;
-                    if (k < tn) {
-                        const float4 cp = cpos[k];
-                        const float dx = hx - cp.x, dy = hy - cp.y, dz = hz - cp.z;
-                        tag = ctag[k];
-                        sp = __float_as_int(cp.w);
-                        const int j = (int)(tag & kSkinIdxMask);
-                        keep = dx * dx + dy * dy + dz * dz < P.r2hi && j != h && half_keep(P, tag, j, h);
-                    }
-                    const unsigned mo = __ballot_sync(0xffffffffu, keep && sp == 3);
-                    const unsigned mm = __ballot_sync(0xffffffffu, keep && sp != 3);
-                    if (keep) {
-                        if (sp == 3) {
-                            const int pos = my.y + __popc(mo & lt);
-                            if (pos < P.cap) row[P.cap - 1 - pos] = tag;
-                        } else {
-                            const int pos = my.x + __popc(mm & lt);
-                            if (pos < P.cap) row[pos] = tag;
-                        }
-                    }
-                    my.x += __popc(mm);
-                    my.y += __popc(mo);
-                }
-                if (lane == 0) cnt[hl] = my;
-            }
-            continue;
-        }
         for (int hl = tid; hl < nh; hl += blockDim.x) {
             const int h = h0 + hl;
             const double4 xh = xq[h];
