@@ -612,7 +612,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--ncu", action="store_true",
                     help="profiling run: set-up, then --steps MD steps of the workload (charges as "
-                         "generated, no CTIP, no comparison runs); prints nothing else")
+                         "generated, no CTIP, RDF every step, no comparison runs); prints nothing else")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="precision of --ncu")
     ap.add_argument("--ncu-ctip", type=int, default=0,
                     help="--ncu: after the set-up run this many CTIP_SOLVER CG iterations (host-driven loop) "
@@ -645,9 +645,11 @@ def main():
             g.profile(True)   # host-driven CG loop: every iteration's kernels are plain launches
             g.ctip_solver(max_cg=args.ncu_ctip)
             g.profile(False)
-        else:
+        else:   # as the timed steps: RDF accumulated every step
+            from simox_b200 import _abi
             g.md_run(args.steps, 1.0 / S.TFM, first_step=2, thermostat=True, T_given=600.0 * S.KB,
-                     freq_new=FREQ_NEW, freq_sort=1, freq_stat=args.freq_stat)
+                     freq_new=FREQ_NEW, freq_sort=1, freq_stat=args.freq_stat,
+                     rdf=np.zeros(_abi.RDF_LEN, np.int32))
         g.sync()
         g.close()
         return 0
