@@ -336,7 +336,9 @@ __global__ void __launch_bounds__(LB_THREADS)
         int ent = entries[cc * kEntries + tid];
         int ce = ent & 0x0fffffff;
         es0[tid] = cell_start[ce];
-        epre[tid + 1] = cell_start[ce + 1] - cell_start[ce];
+        // a half skin list keeps nothing from the 13 backward stencil cells
+        // (half_keep): they are not scanned
+        epre[tid + 1] = (P.skin && P.half && tid < 13) ? 0 : cell_start[ce + 1] - cell_start[ce];
         edir[tid] = ent >> 28;
     }
     for (int k = tid; k < nh; k += blockDim.x) cnt[k] = make_int2(0, 0);
