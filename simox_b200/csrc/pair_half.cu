@@ -883,8 +883,10 @@ __global__ void __launch_bounds__(kHEThreads, 6)
                 min_image(xa, xb, P, dx, dy, dz);
                 const double r = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
                 const PairTab<double>& T = st[sX * kSpecies + sY];
-                rho += T.d_fe * zhou_val<double>(r, T.d_inv_re, T.d_c, T.d_lam);                 // force.f90:84
-                const double rY = T.e_fe * zhou_val<double>(r, T.e_inv_re, T.e_c, T.e_lam);       // force.f90:85
+                const double rX = T.d_fe * zhou_val<double>(r, T.d_inv_re, T.d_c, T.d_lam);       // force.f90:84
+                rho += rX;
+                // a same-species pair: the same density at both atoms (force.f90:85)
+                const double rY = sX == sY ? rX : T.e_fe * zhou_val<double>(r, T.e_inv_re, T.e_c, T.e_lam);
                 add_fixed(rho_fx + Y, __double2ll_rn(rY * kRhoScaleD));
                 pair_energy_fp64(T, r, 1.0 / r, xa.w, xb.w, P.a, ep, ed, ec);
             }
