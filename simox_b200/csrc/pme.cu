@@ -287,17 +287,10 @@ __global__ void __launch_bounds__(128)
     gather_force_kernel(PmeParams S, const double4* __restrict__ xq, const R* __restrict__ grid,
                         const int* __restrict__ sorted, double* __restrict__ f, double* __restrict__ acc, int store) {
     __shared__ double red[128 / 32];
-    // two lanes per atom, each over half of the stencil's z planes: twice the
-    // grid reads in flight (the gather waits on L2 latency); the pair's sums
-    // meet by a shuffle that every lane of the warp executes
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int k = t >> 1, half = t & 1;
-    const bool valid = k < S.n;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
     double fo[3] = {0.0, 0.0, 0.0};
-    double sx = 0.0, sy = 0.0, sz = 0.0, q = 0.0;
-    if (valid) {
+    if (k < S.n) {
         const double4 a = xq[k];
-        q = a.w;
         double wx[P], wy[P], wz[P], dx[P], dy[P], dz[P];
         const double ux = (double)S.K.x * (a.x + S.box.x * 0.5) / S.box.x;
         const double uy = (double)S.K.y * (a.y + S.box.y * 0.5) / S.box.y;
@@ -311,16 +304,10 @@ __global__ void __launch_bounds__(128)
         int ix[P];
 #pragma unroll
         for (int s = 0; s < P; s++) ix[s] = wrapi(bx + s, S.K.x);
-        double wzh[P / 2], dzh[P / 2];   // this lane's z planes (selects, no indexed arrays)
+        double sx = 0.0, sy = 0.0, sz = 0.0;
 #pragma unroll
-        for (int j = 0; j < P / 2; j++) {
-            wzh[j] = half ? wz[P / 2 + j] : wz[j];
-            dzh[j] = half ? dz[P / 2 + j] : dz[j];
-        }
-        const int bzh = bz + half * (P / 2);
-#pragma unroll
-        for (int c2 = 0; c2 < P / 2; c2++) {
-            const size_t gz = (size_t)wrapi(bzh + c2, S.K.z) * S.K.y;
+        for (int c = 0; c < P; c++) {
+            const size_t gz = (size_t)wrapi(bz + c, S.K.z) * S.K.y;
 #pragma unroll
             for (int b = 0; b < P; b++) {
                 const size_t gyz = (gz + wrapi(by + b, S.K.y)) * S.K.x;
@@ -331,17 +318,12 @@ __global__ void __launch_bounds__(128)
                     tx += (R)dx[aa] * g;
                     tw += (R)wx[aa] * g;
                 }
-                sx += (double)tx * wy[b] * wzh[c2];
-                sy += (double)tw * dy[b] * wzh[c2];
-                sz += (double)tw * wy[b] * dzh[c2];
+                sx += (double)tx * wy[b] * wz[c];
+                sy += (double)tw * dy[b] * wz[c];
+                sz += (double)tw * wy[b] * dz[c];
             }
         }
-    }
-    sx += __shfl_xor_sync(0xffffffffu, sx, 1);
-    sy += __shfl_xor_sync(0xffffffffu, sy, 1);
-    sz += __shfl_xor_sync(0xffffffffu, sz, 1);
-    if (valid && !half) {
-        const double pre = -S.cst * q;
+        const double pre = -S.cst * a.w;
         fo[0] = pre * sx * S.kx.x;
         fo[1] = pre * sy * S.kx.y;
         fo[2] = pre * sz * S.kx.z;
@@ -407,14 +389,9 @@ __global__ void __launch_bounds__(128)
     gather_pot_ctip_kernel(PmeParams S, const double4* __restrict__ xq, const R* __restrict__ grid, double scale,
                            CtipFinish F) {
     __shared__ double red[128 / 32];
-    // two lanes per atom, each over half of the stencil's z planes (the
-    // gather waits on L2 latency); the pair's sums meet by a shuffle that
-    // every lane executes
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int k = t >> 1, half = t & 1;
-    const bool valid = k < S.n;
-    double gp = 0.0, pap = 0.0, sum = 0.0;
-    if (valid) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    double gp = 0.0, pap = 0.0;
+    if (k < S.n) {
         const double4 a = xq[k];
         double wx[P], wy[P], wz[P], d[P];
         const double ux = (double)S.K.x * (a.x + S.box.x * 0.5) / S.box.x;
@@ -429,25 +406,19 @@ __global__ void __launch_bounds__(128)
         int ix[P];
 #pragma unroll
         for (int s = 0; s < P; s++) ix[s] = wrapi(bx + s, S.K.x);
-        double wzh[P / 2];
+        double sum = 0.0;
 #pragma unroll
-        for (int j = 0; j < P / 2; j++) wzh[j] = half ? wz[P / 2 + j] : wz[j];
-        const int bzh = bz + half * (P / 2);
-#pragma unroll
-        for (int c2 = 0; c2 < P / 2; c2++) {
-            const size_t gz = (size_t)wrapi(bzh + c2, S.K.z) * S.K.y;
+        for (int c = 0; c < P; c++) {
+            const size_t gz = (size_t)wrapi(bz + c, S.K.z) * S.K.y;
 #pragma unroll
             for (int b = 0; b < P; b++) {
                 const size_t gyz = (gz + wrapi(by + b, S.K.y)) * S.K.x;
                 R tw = 0;
 #pragma unroll
                 for (int aa = 0; aa < P; aa++) tw += (R)wx[aa] * grid[gyz + ix[aa]];
-                sum += (double)tw * wy[b] * wzh[c2];
+                sum += (double)tw * wy[b] * wz[c];
             }
         }
-    }
-    sum += __shfl_xor_sync(0xffffffffu, sum, 1);
-    if (valid && !half) {
         const int sp = min(F.ts[k], 4);
         const double p = F.pv[k];
         const double sr = (double)(long long)F.sr_fx[k] * F.sr_unit;
@@ -703,7 +674,7 @@ static int pme_forces_t(simox_ctx* c, PmeRes& Rs, bool eflag, double* f_store) {
     if (!st) st = run_convolution(c, Rs, eflag);
     if (st) return st;
     Launch L(c, "pme_gather_force");
-    gather_force_kernel<R, P><<<(2 * S.n + 127) / 128, 128, 0, c->stream>>>(
+    gather_force_kernel<R, P><<<(S.n + 127) / 128, 128, 0, c->stream>>>(
         S, c->xq_s, (const R*)Rs.grid, c->pair_order, f_store ? f_store : c->f, c->acc, f_store ? 1 : 0);
     return SIMOX_OK;
 }
@@ -952,8 +923,7 @@ int pme_potential_grid(simox_ctx* c, const double* qalt) {
 template <typename R, int P>
 static void finish_t(simox_ctx* c, PmeRes& Rs, double scale, const CtipFinish& F) {
     PmeParams S = pme_params(c);
-    gather_pot_ctip_kernel<R, P><<<(2 * S.n + 127) / 128, 128, 0, c->stream>>>(S, c->xq_s, (const R*)Rs.grid, scale,
-                                                                               F);
+    gather_pot_ctip_kernel<R, P><<<(S.n + 127) / 128, 128, 0, c->stream>>>(S, c->xq_s, (const R*)Rs.grid, scale, F);
 }
 
 int pme_potential_finish(simox_ctx* c, double scale, const CtipFinish& F) {
