@@ -57,8 +57,8 @@ constexpr int kH1Cap = 4096;
 // dynamic tiles; 32 resident warps hide the pair function's latency chains
 // (0.407 ms for the 128k corundum force pass against 0.43 ms at 512 threads)
 constexpr int kH2Threads = 1024;
-constexpr int kH2Cap = 3584;                              // 56 B per atom: 196 KB
-constexpr size_t kH2Smem = (size_t)kH2Cap * (2 * sizeof(float4) + 6 * sizeof(unsigned));   // 56 B per atom
+constexpr int kH2Cap = 3584;                              // 60 B per atom: 210 KB
+constexpr size_t kH2Smem = (size_t)kH2Cap * (sizeof(double4) + sizeof(float) + 6 * sizeof(unsigned));
 constexpr int kHCCap = 4608;                              // 40 B per atom: 184 KB
 constexpr size_t kHCSmem = (size_t)kHCCap * (sizeof(float4) + sizeof(double) + 4 * sizeof(unsigned));
 
@@ -401,36 +401,20 @@ __device__ __forceinline__ double3 stencil_shift(int e, double3 lcs) {
     return make_double3((e % 3 - 1) * lcs.x, ((e / 3) % 3 - 1) * lcs.y, (e / 9 - 1) * lcs.z);
 }
 
-// A position (a cell offset plus the stencil shift, |x| < 4096 A) split into
-// an FP32 part on a 2^-11 A grid and the FP32 remainder.  The difference of
-// two grid parts is exact in FP32 and the remainders are below 2^-12 A, so
-// (hi_X - hi_Y) + (lo_X - lo_Y) rounds the exact separation once, as the FP64
-// difference rounded to FP32 does, with packed FP32 adds instead of FP64
-// subtractions and conversions.  w: the charge (hi) and F' (lo).
-__device__ __forceinline__ float pos_hi(double x) { return (float)(rint(x * 2048.0) * (1.0 / 2048.0)); }
-
-__device__ __forceinline__ void split_pos(const double4& p, float dF, float4& hi, float4& lo) {
-    hi = make_float4(pos_hi(p.x), pos_hi(p.y), pos_hi(p.z), (float)p.w);
-    lo = make_float4((float)(p.x - (double)hi.x), (float)(p.y - (double)hi.y), (float)(p.z - (double)hi.z), dF);
-}
-
 // Two entries of X's half row as the halves of packed FP32 values: f/r of
 // each pair, X's share into the compensated FP32 sums, Y's share (the
-// opposite force) into Y's fixed-point sums.  TILED: partner records from
-// the CTA's tile (phi, plo); otherwise from the global offsets xo and F'.
+// opposite force) into Y's fixed-point sums.
 template <bool SAME, bool MHOMO, bool RDF, bool TILED, int TI>
 __device__ __forceinline__ void force_half_batch(const Half2Params& H, const int* edelta, const double3* esh,
-                                                 const float4* __restrict__ phi, const float4* __restrict__ plo,
-                                                 const double4* __restrict__ xo, const float* __restrict__ dF_f,
+                                                 const double4* __restrict__ psrc, const float* __restrict__ dsrc,
                                                  int lim, unsigned E1, unsigned E2, bool v1, bool v2ok,
-                                                 const float4& hX, const float4& lX, float dFX,
-                                                 const Sink<TILED>& acc, v2 (&fh)[3],
+                                                 const double4& ra, float dFX, const Sink<TILED>& acc, v2 (&fh)[3],
                                                  v2 (&fl)[3], int* hist, const RefX& RX, const float4* __restrict__ rec,
                                                  const int* __restrict__ order, int& bad) {
     constexpr int NB = SIMOX_NRDF + 2;
     const PackParams& Q = H.Q;
     const PackTab& T = Q.tab[TI];
-    const float qa = hX.w;
+    const float qa = (float)ra.w;
     const float kcqa = Q.kc * qa;
     const float kcqaZY = T.kcZY * qa;
     const int c1 = min((int)((E1 >> kSkinCodeShift) & kCodeMask), kEntries - 1);
@@ -440,23 +424,18 @@ __device__ __forceinline__ void force_half_batch(const Half2Params& H, const int
     // keep every access inside the tile (or the atom range)
     i1 = (unsigned)i1 < (unsigned)lim ? i1 : 0;
     i2 = (unsigned)i2 < (unsigned)lim ? i2 : 0;
-    float4 H1, L1, H2, L2;
-    if (TILED) {
-        H1 = phi[i1]; L1 = plo[i1];
-        H2 = phi[i2]; L2 = plo[i2];
-    } else {   // global offsets: add the stencil shift here
+    double4 P1 = psrc[i1], P2 = psrc[i2];
+    if (!TILED) {   // global offsets: add the stencil shift here
         const double3 s1 = esh[c1], s2 = esh[c2];
-        double4 P1 = xo[i1], P2 = xo[i2];
         P1.x += s1.x; P1.y += s1.y; P1.z += s1.z;
         P2.x += s2.x; P2.y += s2.y; P2.z += s2.z;
-        split_pos(P1, dF_f[i1], H1, L1);
-        split_pos(P2, dF_f[i2], H2, L2);
     }
-    const v2 dx = (bc(hX.x) - mk2(H1.x, H2.x)) + (bc(lX.x) - mk2(L1.x, L2.x));
-    const v2 dy = (bc(hX.y) - mk2(H1.y, H2.y)) + (bc(lX.y) - mk2(L1.y, L2.y));
-    const v2 dz = (bc(hX.z) - mk2(H1.z, H2.z)) + (bc(lX.z) - mk2(L1.z, L2.z));
+    const float D1 = dsrc[i1], D2 = dsrc[i2];
+    const v2 dx = mk2((float)(ra.x - P1.x), (float)(ra.x - P2.x));
+    const v2 dy = mk2((float)(ra.y - P1.y), (float)(ra.y - P2.y));
+    const v2 dz = mk2((float)(ra.z - P1.z), (float)(ra.z - P2.z));
     const v2 r2 = fma2(dx, dx, fma2(dy, dy, dz * dz));
-    v2 fs = pair_fs_pk<SAME, MHOMO>(T, Q, r2, mk2(H1.w, H2.w), mk2(L1.w, L2.w), dFX, kcqa, kcqaZY);
+    v2 fs = pair_fs_pk<SAME, MHOMO>(T, Q, r2, mk2((float)P1.w, (float)P2.w), mk2(D1, D2), dFX, kcqa, kcqaZY);
     fs = mk2(v1 ? fs.v.x : 0.f, v2ok ? fs.v.y : 0.f);   // slots past the end of a group: placeholders
     const v2 px = fs * dx, py = fs * dy, pz = fs * dz;
     two_sum2(fh[0], fl[0], px);
@@ -493,7 +472,7 @@ __device__ __forceinline__ void force_half_batch(const Half2Params& H, const int
 
 template <bool TILED, bool RDF>
 __device__ __forceinline__ void force_half_atoms(const Half2Params& H, const int* edelta, const double3* esh,
-                                                 const float4* __restrict__ phi, const float4* __restrict__ plo,
+                                                 const double4* __restrict__ psrc, const float* __restrict__ dsrc,
                                                  int lim, int b0, int b1, int a0, int* next,
                                                  const double4* __restrict__ xo, const int* __restrict__ ts,
                                                  const int2* __restrict__ nn, const unsigned* __restrict__ nbr,
@@ -508,10 +487,9 @@ __device__ __forceinline__ void force_half_atoms(const Half2Params& H, const int
         if (lane == 0) X = atomicAdd(next, 1);
         X = __shfl_sync(0xffffffffu, X, 0) + b0;
         if (X >= b1) break;
+        const double4 ra = xo[X];
         const int sX = ts[X];
         const float dFX = dF_f[X];
-        float4 hX, lX;
-        split_pos(xo[X], dFX, hX, lX);
         const RefX RX = RDF ? ref_x(H, rec, order, X) : RefX{};
         const int2 m = nn[X];
         const unsigned* row = nbr + (size_t)X * cap;
@@ -541,11 +519,11 @@ __device__ __forceinline__ void force_half_atoms(const Half2Params& H, const int
                 const int kb = (g1 ? j - nb0 : j) << 6, mg = g1 ? m.y : m.x;
                 const bool v1 = kb + lane < mg, v2ok = kb + 32 + lane < mg;
                 if (metal) {
-                    if (!g1) force_half_batch<true, true, RDF, TILED, 0>(H, edelta, esh, phi, plo, xo, dF_f, lim, E1, E2, v1, v2ok, hX, lX, dFX, acc, fh, fl, hist, RX, rec, order, bad);
-                    else force_half_batch<false, false, RDF, TILED, 1>(H, edelta, esh, phi, plo, xo, dF_f, lim, E1, E2, v1, v2ok, hX, lX, dFX, acc, fh, fl, hist, RX, rec, order, bad);
+                    if (!g1) force_half_batch<true, true, RDF, TILED, 0>(H, edelta, esh, psrc, dsrc, lim, E1, E2, v1, v2ok, ra, dFX, acc, fh, fl, hist, RX, rec, order, bad);
+                    else force_half_batch<false, false, RDF, TILED, 1>(H, edelta, esh, psrc, dsrc, lim, E1, E2, v1, v2ok, ra, dFX, acc, fh, fl, hist, RX, rec, order, bad);
                 } else {
-                    if (!g1) force_half_batch<false, false, RDF, TILED, 2>(H, edelta, esh, phi, plo, xo, dF_f, lim, E1, E2, v1, v2ok, hX, lX, dFX, acc, fh, fl, hist, RX, rec, order, bad);
-                    else force_half_batch<true, false, RDF, TILED, 3>(H, edelta, esh, phi, plo, xo, dF_f, lim, E1, E2, v1, v2ok, hX, lX, dFX, acc, fh, fl, hist, RX, rec, order, bad);
+                    if (!g1) force_half_batch<false, false, RDF, TILED, 2>(H, edelta, esh, psrc, dsrc, lim, E1, E2, v1, v2ok, ra, dFX, acc, fh, fl, hist, RX, rec, order, bad);
+                    else force_half_batch<true, false, RDF, TILED, 3>(H, edelta, esh, psrc, dsrc, lim, E1, E2, v1, v2ok, ra, dFX, acc, fh, fl, hist, RX, rec, order, bad);
                 }
             }
         }
@@ -572,10 +550,10 @@ __global__ void __launch_bounds__(kH2Threads, 1)
                       const float4* __restrict__ rec, const int* __restrict__ order, int* __restrict__ status) {
     constexpr int NB = SIMOX_NRDF + 2;
     extern __shared__ __align__(16) unsigned char half_smem[];
-    float4* phi = reinterpret_cast<float4*>(half_smem);                    // partner position grid parts, charge
-    float4* plo = phi + kH2Cap;                                            // remainders, F'
-    unsigned* tlo = reinterpret_cast<unsigned*>(plo + kH2Cap);             // [3][cap] low words
+    double4* tpos = reinterpret_cast<double4*>(half_smem);                 // partner offsets + shift, charge
+    unsigned* tlo = reinterpret_cast<unsigned*>(tpos + kH2Cap);            // [3][cap] low words
     unsigned* thi = tlo + 3 * kH2Cap;                                      // [3][cap] high words
+    float* tdf = reinterpret_cast<float*>(thi + 3 * kH2Cap);               // F'
     __shared__ double3 esh[kEntries];          // o_e * Lcs
     __shared__ int edelta[kEntries];           // tile index delta of each stencil position
     __shared__ HalfTile T;
@@ -608,10 +586,8 @@ __global__ void __launch_bounds__(kH2Threads, 1)
             p.x += sh.x;
             p.y += sh.y;
             p.z += sh.z;
-            float4 h, l;
-            split_pos(p, dF_f[src], h, l);
-            phi[i] = h;
-            plo[i] = l;
+            tpos[i] = p;
+            tdf[i] = dF_f[src];
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 tlo[c * kH2Cap + i] = 0u;
@@ -623,10 +599,10 @@ __global__ void __launch_bounds__(kH2Threads, 1)
     const int a0 = T.start[0];
     int bad = 0;
     if (tiled)
-        force_half_atoms<true, RDF>(H, edelta, esh, phi, plo, total, b0, b1, a0, &next, xo, ts, nn, nbr, dF_f,
+        force_half_atoms<true, RDF>(H, edelta, esh, tpos, tdf, total, b0, b1, a0, &next, xo, ts, nn, nbr, dF_f,
                                     Sink<true>{tlo, thi, kH2Cap, f_fx, H.fstride}, hist, rec, order, bad);
     else
-        force_half_atoms<false, RDF>(H, edelta, esh, nullptr, nullptr, H.n, b0, b1, a0, &next, xo, ts, nn, nbr, dF_f,
+        force_half_atoms<false, RDF>(H, edelta, esh, xo, dF_f, H.n, b0, b1, a0, &next, xo, ts, nn, nbr, dF_f,
                                      Sink<false>{f_fx, H.fstride}, hist, rec, order, bad);
     if (bad) atomicOr(status, bad);
     __syncthreads();
