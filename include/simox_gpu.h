@@ -356,6 +356,13 @@ int simox_set_ctip_xi(simox_ctx* ctx, int species, double xi);
  * an optimiser's line search), which then all stay on the branch of the
  * charge minimum the held charges lie on.  on = 0 (the default): CG first. */
 int simox_adjoint_warm_start(simox_ctx* ctx, int on);
+/* Precision of simox_adjoint_eval's forward pair passes (no counterpart in
+ * the reference).  SIMOX_FP64 (the default): every term FP64.  SIMOX_MIXED:
+ * the pair terms of the density and force passes in FP32 (separations formed
+ * in FP64 and rounded once), summed in FP64; the charge solve, PME, the
+ * embedding and the adjoint solve and gradients stay FP64.  The context
+ * itself stays an FP64 context. */
+int simox_adjoint_forward_precision(simox_ctx* ctx, int precision);
 /* Charges q*, energy, forces (original order, [n][3], may be NULL) and the
  * gradients of E (grad_E) and of L = sum |F - T|^2 (grad_L; needs f_target
  * [n][3]) with respect to the parameters; either gradient may be NULL.  The

@@ -148,7 +148,7 @@ EXPORTED = [
     "simox_set_eam_spline", "simox_set_ctip_params", "simox_set_ctip_xi", "simox_adjoint_eval",
     "simox_adjoint_eval_many",
     "simox_remove_rigid_motion", "simox_oxide_check", "simox_new_o2", "simox_md_run_oxidation",
-    "simox_adjoint_warm_start",
+    "simox_adjoint_forward_precision", "simox_adjoint_warm_start",
 ]
 
 

@@ -98,6 +98,7 @@ def lib():
         "simox_adjoint_eval_many": [C.POINTER(_vp), C.c_int, C.POINTER(_dp), C.POINTER(AdjointReport),
                                     C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp), C.c_int],
         "simox_adjoint_warm_start": [_vp, C.c_int],
+        "simox_adjoint_forward_precision": [_vp, C.c_int],
         "simox_remove_rigid_motion": [_vp],
         "simox_oxide_check": [_vp, C.c_int, C.c_double, _ip],
         "simox_new_o2": [_vp, C.c_int, C.c_double, C.c_double, C.c_ulonglong, C.c_ulonglong],
@@ -461,6 +462,12 @@ class Simox:
     def adjoint_warm_start(self, on: bool = True):
         """Refine the held charges by Newton steps (no CG first) in adjoint_eval."""
         _check(lib().simox_adjoint_warm_start(self._ctx, 1 if on else 0), "adjoint_warm_start")
+
+    def adjoint_forward_precision(self, precision: str = "fp64"):
+        """Pair terms of adjoint_eval's forward passes in FP64 ("fp64") or FP32
+        ("mixed", FP64 sums); the charge solve, PME and the adjoint stay FP64."""
+        code = {"fp64": SIMOX_FP64, "mixed": SIMOX_MIXED}[precision]
+        _check(lib().simox_adjoint_forward_precision(self._ctx, code), "adjoint_forward_precision")
 
     def set_ctip_xi(self, species: int, xi: float):
         """Slater exponent xi of species 1..5 (recomputes the fafb coefficients)."""

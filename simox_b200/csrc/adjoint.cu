@@ -285,6 +285,183 @@ __global__ void __launch_bounds__(AT)
     block_add<AT>(ep, acc, A_EPAIR, red);
 }
 
+// ---------------------------------------------------------------------------
+// FP32 forward (simox_adjoint_forward_precision(ctx, SIMOX_MIXED)): the pair
+// terms of the two forward passes in FP32 -- each separation formed in FP64
+// and its length rounded once, the spline, Zhou, erfc and Slater terms in FP32
+// (CUDA's single-precision expf and erfcf) -- with FP64 sums per atom.  The
+// charge solve, PME, the embedding and every adjoint and gradient kernel stay
+// FP64.
+
+__device__ __forceinline__ int bsp_f(float t, float b[4], float db[4]) {
+    int i = (int)floorf(t);
+    i = i < 0 ? 0 : (i > NS - 4 ? NS - 4 : i);
+    const float u = t - (float)i, v = 1.f - u, u2 = u * u, u3 = u2 * u;
+    b[0] = v * v * v * (1.f / 6.f);
+    b[1] = (3.f * u3 - 6.f * u2 + 4.f) * (1.f / 6.f);
+    b[2] = (-3.f * u3 + 3.f * u2 + 3.f * u + 1.f) * (1.f / 6.f);
+    b[3] = u3 * (1.f / 6.f);
+    db[0] = -0.5f * v * v;
+    db[1] = 1.5f * u2 - 2.f * u;
+    db[2] = -1.5f * u2 + u + 0.5f;
+    db[3] = 0.5f * u2;
+    return i;
+}
+
+__device__ __forceinline__ float spl_f(const double* c, float t, float ih, float& d1) {
+    float b[4], db[4];
+    const int i = bsp_f(t, b, db);
+    float sv = 0.f, s1 = 0.f;
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        const float cm = (float)c[i + m];
+        sv = fmaf(cm, b[m], sv);
+        s1 = fmaf(cm, db[m], s1);
+    }
+    d1 = s1 * ih;
+    return sv;
+}
+
+__device__ __forceinline__ void zhou_f(float r, float ire, float c, float lam, float& g, float& dg) {
+    const float rr = r * ire, t = rr - lam;
+    const float t2 = t * t, t4 = t2 * t2, t8 = t4 * t4, t16 = t8 * t8, t19 = t16 * t2 * t, t20 = t19 * t;
+    const float u = 1.f / (1.f + t20);
+    g = expf(-c * (rr - 1.f)) * u;
+    dg = g * ire * (-c - 20.f * t19 * u);
+}
+
+__device__ __forceinline__ void dens_f(const SplineDev& S, bool spline, float fe, float ire, float c, float lam, float r,
+                                       float& f, float& df) {
+    if (spline) {
+        f = spl_f(S.dens, (r - (float)S.r0) * (float)S.ihr, (float)S.ihr, df);
+    } else {
+        float g, dg;
+        zhou_f(r, ire, c, lam, g, dg);
+        f = fe * g;
+        df = fe * dg;
+    }
+}
+
+__device__ __forceinline__ void pair_phi_f(const SplineDev& S, const PairTab<double>& T, int sX, int sY, float r,
+                                           float& p, float& dp) {
+    if (sX == S.metal && sY == S.metal) {
+        p = spl_f(S.phi, (r - (float)S.r0) * (float)S.ihr, (float)S.ihr, dp);
+    } else {
+        float gA, dgA, gB, dgB;
+        zhou_f(r, (float)T.p_inv_re, (float)T.p_alpha, (float)T.p_kappa, gA, dgA);
+        zhou_f(r, (float)T.p_inv_re, (float)T.p_beta, (float)T.p_lambda, gB, dgB);
+        p = (float)T.p_A * gA - (float)T.p_B * gB;
+        dp = (float)T.p_A * dgA - (float)T.p_B * dgB;
+    }
+}
+
+// the Ewald real-space + CTIP force scalar of es_pair in FP32
+__device__ __forceinline__ float es_fs_f(const PairTab<double>& T, float r, float qa, float qb, float a, float kc) {
+    const float ir = 1.f / r, ir2 = ir * ir;
+    const float erfcv = erfcf(a * r), ea = expf(-a * a * r * r);
+    const float ew = (2.f * a / (float)SX_SQRTPI * r * ea + erfcv) * ir2 * ir;
+    const float xx = (float)T.xi_x, xy = (float)T.xi_y;
+    const float eX = expf(-2.f * xx * r), eY = expf(-2.f * xy * r);
+    const float djfi = eX * (2.f * xx * xx + (1.f + 2.f * xx * r) * ir2);
+    const float difj = eY * (2.f * xy * xy + (1.f + 2.f * xy * r) * ir2);
+    const float QX = (float)T.Qx[0] + r * ((float)T.Qx[1] + r * (float)T.Qx[2]) + ir * ((float)T.Qx[3] + ir * (float)T.Qx[4]);
+    const float QY = (float)T.Qy[0] + ir * ((float)T.Qy[3] + ir * (float)T.Qy[4]);
+    const float dfifj = eX * QX + eY * QY;
+    const float ZX = (float)T.Z_x, ZY = (float)T.Z_y;
+    return kc * qa * qb * ew + kc * ((qa * ZY + qb * ZX - qa * qb) * dfifj - qa * ZY * djfi - qb * ZX * difj) * ir;
+}
+
+// pass 1 with FP32 pair terms: rho (FP64 sum), F, F', F'' (FP64), Egroup
+__global__ void __launch_bounds__(AT)
+    adj_density_f_kernel(AdjParams P, const SplineDev* __restrict__ S, const PairTab<double>* __restrict__ tab,
+                         const double4* __restrict__ xq, const int* __restrict__ ts, const int2* __restrict__ nn,
+                         const unsigned* __restrict__ nbr, double* __restrict__ rho_s, double* __restrict__ dF,
+                         double* __restrict__ d2F, double* __restrict__ acc, int* __restrict__ status) {
+    __shared__ double red[AT / 32];
+    const SplineDev& Sp = *S;
+    const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    double eg = 0.0;
+    int bad = 0;
+    for (int X = blockIdx.x * wpb + (threadIdx.x >> 5); X < P.n; X += gridDim.x * wpb) {
+        const double4 xa = xq[X];
+        const int sX = ts[X];
+        const int2 m = nn[X];
+        const unsigned* row = nbr + (size_t)X * P.cap;
+        double rho = 0.0;
+        for (int k = lane; k < m.x + m.y; k += 32) {
+            const int Y = (int)(row[slot(k, P.cap, m.x)] & kIdxMask);
+            const int sY = ts[Y];
+            double dx, dy, dz;
+            sep(xa, xq[Y], P, dx, dy, dz);
+            const float r = (float)sqrt(dx * dx + dy * dy + dz * dz);
+            const PairTab<double>& T = tab[sX * kSpecies + sY];
+            float f, df;
+            dens_f(Sp, sY == Sp.metal, (float)T.d_fe, (float)T.d_inv_re, (float)T.d_c, (float)T.d_lam, r, f, df);
+            rho += (double)f;
+        }
+        rho = warp_sum(rho);
+        if (lane == 0) {
+            double F, d1, d2;
+            if (embed2(Sp, P, sX, rho, F, d1, d2)) bad |= ST_UNSUPPORTED;
+            rho_s[X] = rho;
+            dF[X] = d1;
+            d2F[X] = d2;
+            eg += F;
+        }
+    }
+    if (bad) atomicOr(status, bad);
+    block_add<AT>(eg, acc, A_EGROUP, red);
+}
+
+// pass 2 with FP32 pair terms: forces (FP64 sums) into f (original order), Epair
+__global__ void __launch_bounds__(AT)
+    adj_force_f_kernel(AdjParams P, const SplineDev* __restrict__ S, const PairTab<double>* __restrict__ tab,
+                       const double4* __restrict__ xq, const int* __restrict__ ts, const int2* __restrict__ nn,
+                       const unsigned* __restrict__ nbr, const double* __restrict__ dF, const int* __restrict__ sorted,
+                       double* __restrict__ f, double* __restrict__ acc) {
+    __shared__ double red[AT / 32];
+    const SplineDev& Sp = *S;
+    const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    const float a = (float)P.a, kc = (float)P.kc;
+    double ep = 0.0;
+    for (int X = blockIdx.x * wpb + (threadIdx.x >> 5); X < P.n; X += gridDim.x * wpb) {
+        const double4 xa = xq[X];
+        const int sX = ts[X];
+        const float dFX = (float)dF[X];
+        const int2 m = nn[X];
+        const unsigned* row = nbr + (size_t)X * P.cap;
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+        for (int k = lane; k < m.x + m.y; k += 32) {
+            const int Y = (int)(row[slot(k, P.cap, m.x)] & kIdxMask);
+            const int sY = ts[Y];
+            const double4 xb = xq[Y];
+            double dx, dy, dz;
+            sep(xa, xb, P, dx, dy, dz);
+            const float r = (float)sqrt(dx * dx + dy * dy + dz * dz);
+            const PairTab<double>& T = tab[sX * kSpecies + sY];
+            float p, dp, fa, dfa, fb, dfb;
+            pair_phi_f(Sp, T, sX, sY, r, p, dp);
+            dens_f(Sp, sY == Sp.metal, (float)T.d_fe, (float)T.d_inv_re, (float)T.d_c, (float)T.d_lam, r, fa, dfa);
+            dens_f(Sp, sX == Sp.metal, (float)T.e_fe, (float)T.e_inv_re, (float)T.e_c, (float)T.e_lam, r, fb, dfb);
+            const float fs = -(dp + dFX * dfa + (float)dF[Y] * dfb) / r + es_fs_f(T, r, (float)xa.w, (float)xb.w, a, kc);
+            fx += (double)fs * dx;
+            fy += (double)fs * dy;
+            fz += (double)fs * dz;
+            ep += 0.5 * (double)p;
+        }
+        fx = warp_sum(fx);
+        fy = warp_sum(fy);
+        fz = warp_sum(fz);
+        if (lane == 0) {
+            const int o = sorted[X];
+            f[3 * o] = fx;
+            f[3 * o + 1] = fy;
+            f[3 * o + 2] = fz;
+        }
+    }
+    block_add<AT>(ep, acc, A_EPAIR, red);
+}
+
 // U = sum_i [c_i q_i + J'_i q_i^2/2 + pen_i(q_i)] + 1/2 sum_i q_i (sr_i + phi_i)
 // and the gradient G_i = c_i + J'_i q_i + pen'_i + sr_i + phi_i (sorted order)
 __global__ void adj_u_kernel(int n, const int* __restrict__ ts, const double* __restrict__ q,
@@ -1109,16 +1286,27 @@ int adjoint_eval(simox_ctx* c, const double* f_target, simox_adjoint_report* rep
     const int wpb = AT / 32;
     const int g = std::max(1, std::min((n + wpb - 1) / wpb, num_sms(c) * 16));
     cudaMemsetAsync(c->acc, 0, sizeof(double) * (A_EREC + 1), s);
-    {
-        Launch L(c, "adjoint_density");
-        adj_density_kernel<<<g, AT, 0, s>>>(P, A->spl, c->tab_d, c->xq_s, c->t_s,
-                                            reinterpret_cast<const int2*>(c->nn), c->nbr, c->rho_s, c->dF_s, A->d2F,
-                                            c->acc, c->status);
-    }
-    {
-        Launch L(c, "adjoint_force");
-        adj_force_kernel<<<g, AT, 0, s>>>(P, A->spl, c->tab_d, c->xq_s, c->t_s, reinterpret_cast<const int2*>(c->nn),
-                                          c->nbr, c->dF_s, c->pair_order, c->f, c->acc);
+    if (c->adj_fwd32) {   // FP32 pair terms in the forward passes
+        Launch L(c, "adjoint_forward_fp32");
+        adj_density_f_kernel<<<g, AT, 0, s>>>(P, A->spl, c->tab_d, c->xq_s, c->t_s,
+                                              reinterpret_cast<const int2*>(c->nn), c->nbr, c->rho_s, c->dF_s, A->d2F,
+                                              c->acc, c->status);
+        adj_force_f_kernel<<<g, AT, 0, s>>>(P, A->spl, c->tab_d, c->xq_s, c->t_s,
+                                            reinterpret_cast<const int2*>(c->nn), c->nbr, c->dF_s, c->pair_order, c->f,
+                                            c->acc);
+    } else {
+        {
+            Launch L(c, "adjoint_density");
+            adj_density_kernel<<<g, AT, 0, s>>>(P, A->spl, c->tab_d, c->xq_s, c->t_s,
+                                                reinterpret_cast<const int2*>(c->nn), c->nbr, c->rho_s, c->dF_s,
+                                                A->d2F, c->acc, c->status);
+        }
+        {
+            Launch L(c, "adjoint_force");
+            adj_force_kernel<<<g, AT, 0, s>>>(P, A->spl, c->tab_d, c->xq_s, c->t_s,
+                                              reinterpret_cast<const int2*>(c->nn), c->nbr, c->dF_s, c->pair_order,
+                                              c->f, c->acc);
+        }
     }
     if ((st = pme_forces(c, true, false))) return st;
     if ((st = read_status(c))) return st;
@@ -1241,6 +1429,12 @@ extern "C" int simox_set_ctip_xi(simox_ctx* c, int species, double xi) {
 }
 
 // warm start of the adjoint's charge solve (see the header)
+extern "C" int simox_adjoint_forward_precision(simox_ctx* c, int precision) {
+    if (!c || (precision != SIMOX_FP64 && precision != SIMOX_MIXED)) return SIMOX_E_ARG;
+    c->adj_fwd32 = precision == SIMOX_MIXED;
+    return SIMOX_OK;
+}
+
 extern "C" int simox_adjoint_warm_start(simox_ctx* c, int on) {
     if (!c) return SIMOX_E_ARG;
     c->adj_warm = on != 0;

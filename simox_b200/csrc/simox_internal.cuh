@@ -167,6 +167,7 @@ struct simox_ctx {
     unsigned long long md_step_no = 0;   // md_run's current step: the stochastic thermostat's draw counter
     sx::AdjointState* adj = nullptr;   // parameter-adjoint model (simox_set_eam_spline)
     bool adj_warm = false;             // adjoint: refine the held charges by Newton, no CG first
+    bool adj_fwd32 = false;            // adjoint: FP32 pair terms in the forward passes
     bool coop_brent = true;            // the charge solver's line search as one cooperative grid
     bool spline_on = false;
 

@@ -192,6 +192,45 @@ def test_gradients_match_cpu_reference_at_2000_atoms():
           f"max |dL/dc - ref| {errL.max():.2e} (largest {np.abs(refL).max():.2e})")
 
 
+def test_fp32_forward_against_fp64_forward():
+    """simox_adjoint_forward_precision(SIMOX_MIXED): the forward pair terms in
+    FP32 (FP64 sums), the charge solve and the adjoint in FP64, at a
+    2000-atom snapshot.  Forces within 1e-5 of the FP64 forward (relative
+    norm; largest per-atom deviation within 3e-5 of the RMS force); the
+    energy gradient within 1e-5 (relative norm: the gradient kernels are FP64
+    and take only rho, F' and q from the forward).  The loss gradient moves
+    by the force difference relative to F - T (targets are the FP64 forces
+    plus 0.05 eV/A noise): within 1e-2 (relative norm).  The FP64 forward
+    stays the one the finite-difference and reference checks pin."""
+    s = S.replica(31, 2000, 0.3, 600.0)
+    P = api.default_potential()
+    spl = spline.fit(P)
+    rng = np.random.default_rng(11)
+    out = {}
+    with _ctx(s) as g:
+        g.set_eam_spline(spl)
+        _, f0, _, _ = g.adjoint_eval(gradients=False)
+        target = f0 + rng.normal(0.0, 0.05, f0.shape)
+        q0 = g.get_state()["q"]
+        for prec in ("fp64", "mixed"):
+            g.adjoint_forward_precision(prec)
+            g.set_state(q=q0)
+            out[prec] = g.adjoint_eval(target)
+        g.adjoint_forward_precision("fp64")
+    (r64, F64, gE64, gL64), (r32, F32, gE32, gL32) = out["fp64"], out["mixed"]
+    frms = np.linalg.norm(F64) / np.sqrt(s.n)
+    fnorm = np.linalg.norm(F32 - F64) / np.linalg.norm(F64)
+    fatom = np.linalg.norm(F32 - F64, axis=1).max() / frms
+    gEn = np.linalg.norm(gE32 - gE64) / np.linalg.norm(gE64)
+    gLn = np.linalg.norm(gL32 - gL64) / np.linalg.norm(gL64)
+    print(f"\nFP32 forward vs FP64: forces {fnorm:.2e} (norm), {fatom:.2e} of F_rms (atom); "
+          f"grad E {gEn:.2e}, grad L {gLn:.2e}, E {abs(r32['E'] - r64['E']) / s.n:.2e} eV/atom")
+    assert fnorm <= 1e-5, fnorm
+    assert fatom <= 3e-5, fatom
+    assert gEn <= 1e-5, gEn
+    assert gLn <= 1e-2, gLn
+
+
 def test_adjoint_eval_many_matches_one_by_one():
     """Three snapshots through simox_adjoint_eval_many (host threads, a stream
     each) against the same snapshots one after another: equal losses and
