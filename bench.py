@@ -521,6 +521,16 @@ def adjoint_object(nsnap, sequential=True):
         res["sequential"] = {"value": len(ctxs) / el_seq, "unit": "snapshots/s",
                              "api": "simox_adjoint_eval, one snapshot after another"}
         res["grad_L_rel_diff_concurrent_vs_sequential"] = float(np.linalg.norm(gL - gL_seq) / np.linalg.norm(gL_seq))
+    # the same with FP32 pair terms in the forward passes (FP64 adjoint)
+    for g in ctxs:
+        g.adjoint_forward_precision("mixed")
+    t0 = time.perf_counter()
+    out32 = api.adjoint_eval_many(ctxs, targets)
+    el32 = time.perf_counter() - t0
+    gL32 = np.sum([o[3] for o in out32], axis=0)
+    res["fp32_forward"] = {"value": len(ctxs) / el32, "unit": "snapshots/s",
+                           "api": "simox_adjoint_forward_precision(SIMOX_MIXED) + simox_adjoint_eval_many",
+                           "grad_L_rel_diff_vs_fp64_forward": float(np.linalg.norm(gL32 - gL) / np.linalg.norm(gL))}
     for g in ctxs:
         g.close()
     return res
