@@ -97,6 +97,49 @@ def test_c1_slab_order6_fp64_vs_oracle():
     assert abs(e["mv2"] - mv2_o) <= 1e-9 * mv2_o
 
 
+def test_c1_slab_200_nve_steps_vs_oracle():
+    """The configuration's full length: 200 NVE steps (dt = 1 fs, CELL_SORT
+    every step, FP64, the oracle's converged charges held) on the GPU and in
+    the oracle from the same state.  Round-off differences grow along the
+    trajectory, so the bars are wider than the 20-step test's: positions
+    within 1e-6 A, velocities within 1e-6 of the largest, the kinetic and
+    potential energies of the last step within 1e-8 relative."""
+    s = _c1()
+    gold = _c1_golden(s)
+    o = oracle_system(s)
+    o.pme_self()
+    o.cell_sort()
+    o.q = np.array(gold["q"])
+    f_step, *_ = o.force()
+    f_step, _ = o.pme(f_step)
+    v = s.v.copy()
+    nsteps = 200
+    for step in range(nsteps):
+        v = o.vv_nve1(v, f_step, DT)
+        o.cell_sort()
+        f_step, e_o, *_ = o.force()
+        f_step, erec_o = o.pme(f_step)
+        v, mv2_o = o.vv_nve2(v, f_step, DT)
+    with gpu_context(s) as g:
+        g.pme_self()
+        g.cell_sort()
+        g.set_state(q=o.q)
+        g.force(energies=False)
+        g.pme(energies=False)
+        e = g.md_run(nsteps, DT, first_step=2, thermostat=False, freq_new=0, freq_sort=1, freq_stat=nsteps)
+        st = g.get_state()
+    dx = np.abs(st["x"] - o.x).max()
+    dv = np.abs(st["v"] - v).max() / np.abs(v).max()
+    print(f"\nC1 200 NVE steps vs oracle: max |dx| {dx:.2e} A, max |dv| {dv:.2e} of max |v|, "
+          f"mv2 {abs(e['mv2'] - mv2_o) / mv2_o:.2e}")
+    assert dx <= 1e-6, dx
+    assert dv <= 1e-6, dv
+    assert abs(e["mv2"] - mv2_o) <= 1e-8 * mv2_o
+    for k in ("Epair", "Edir", "Ectip", "Egroup"):
+        assert abs(e[k] - e_o[k]) <= 1e-8 * max(1.0, abs(e_o[k])), (k, e[k], e_o[k])
+    assert abs(e["Erec"] - erec_o) <= 1e-8 * abs(erec_o)
+
+
 def test_c1_slab_mixed_half_list_vs_oracle():
     """The same slab in mixed precision runs the half-list kernels (each pair
     once, partner shares in fixed-point sums): the charge solve must take the
