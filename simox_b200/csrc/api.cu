@@ -595,6 +595,7 @@ extern "C" int simox_cell_sort(simox_ctx* c) {
 extern "C" int simox_get_cells(simox_ctx* c, int* npt, int* link, int link_stride) {
     if (!c || !npt || !c->cells_valid) return c ? SIMOX_E_STATE : SIMOX_E_ARG;
     cudaSetDevice(c->device);
+    if (int e = ensure_cell_lists(c)) return e;
     std::vector<int> start(c->ncell + 1), srt(std::max(c->n, 1));
     cudaMemcpyAsync(start.data(), c->cell_start, sizeof(int) * (c->ncell + 1), cudaMemcpyDeviceToHost, c->stream);
     cudaMemcpyAsync(srt.data(), c->sorted, sizeof(int) * c->n, cudaMemcpyDeviceToHost, c->stream);

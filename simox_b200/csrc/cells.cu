@@ -178,6 +178,25 @@ int cell_sort(simox_ctx* c) {
         scan_cells_kernel<<<1, 1024, 0, c->stream>>>(c->cell_count, c->cell_start, c->cell_fill, c->ncell, c->npt_max,
                                                      c->status, nullptr);
     }
+    int st = check_launch(c);
+    if (st) return st;
+    c->cells_valid = true;
+    c->cells_fresh = true;
+    c->cells_listed = false;   // the link lists themselves are filled when something reads them
+    c->gathered = false;
+    c->list_valid = false;
+    return SIMOX_OK;
+}
+
+// The reference cells' link lists (sorted: atoms cell by cell, ascending
+// within a cell, cellsort.f90:69-78) of the last CELL_SORT.  In skin mode the
+// pair kernels run in the skin order and only simox_get_cells reads them, so
+// CELL_SORT leaves them to this call (the binning, the counts and the
+// over-full-cell check run every time).
+int ensure_cell_lists(simox_ctx* c) {
+    if (!c->cells_valid) return SIMOX_E_STATE;
+    if (c->cells_listed) return SIMOX_OK;
+    const int n = c->n;
     if (n > 0) {
         Launch L(c, "cell_scatter");
         scatter_atoms_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, c->cell_of, c->cell_fill, c->sorted, nullptr);
@@ -189,10 +208,7 @@ int cell_sort(simox_ctx* c) {
     }
     int st = check_launch(c);
     if (st) return st;
-    c->cells_valid = true;
-    c->cells_fresh = true;
-    c->gathered = false;
-    c->list_valid = false;
+    c->cells_listed = true;
     return SIMOX_OK;
 }
 
@@ -535,6 +551,7 @@ static int prepare_order(simox_ctx* c) {
     const int n = c->n;
     cudaStream_t s = c->stream;
     if (!skin) {
+        if (int st = ensure_cell_lists(c)) return st;
         c->pair_order = c->sorted;
         c->using_skin = false;
         return gather_sorted(c);

@@ -272,6 +272,7 @@ struct simox_ctx {
 
     // validity
     bool have_ids = false, cells_valid = false, gathered = false, list_valid = false, psi_valid = false;
+    bool cells_listed = false;   // the reference link lists (sorted) belong to the last binning
     bool eam_valid = false;
 
     // timing / counters
@@ -325,6 +326,7 @@ struct Launch {
 // cells.cu
 int build_cell_tables(simox_ctx* c);
 int cell_sort(simox_ctx* c);
+int ensure_cell_lists(simox_ctx* c);
 int gather_sorted(simox_ctx* c);
 int build_list(simox_ctx* c);
 int ensure_list(simox_ctx* c);
