@@ -606,7 +606,7 @@ def c3_object(steps=2, device=0):
             "unit": UNIT, "n_atoms": s.n, "steps": steps, "ms_per_step": ms / steps,
             "first_solve": {"n_cg": rep0["n_cg"], "seconds": first_s, "from": "zero charges"},
             "total_charge_change_e": float(abs(q.sum() - q0)),
-            "energies_last_step": e}
+            "energies_last_status_step": e}
 
 
 def main():
@@ -776,7 +776,7 @@ def main():
                        "parallelism": "replicas" if world > 1 else "single",
                        "precision": "mixed: FP32 pair/PME terms, FP64 sums, energies, CG",
                        "charges": "CTIP at step 1 (warm-up), freq_new > run length; re-solve timed separately (ctip)",
-                       "energies": "FP64 energies on every 10th step (status rule) and the last; RDF every step",
+                       "energies": "FP64 energies on steps with MOD(step, 10) == 0 (status rule); RDF every step",
                        "l2": "inputs larger than L2 (exact neighbour list %.0f MB rebuilt every step)" % (
                            tot_nnb * (2 if half else 4) / 1e6),
                        "mean_neighbours": round(nnb, 1),
@@ -805,7 +805,7 @@ def main():
             "ctip": {"mixed": ctip_mixed, "fp64": ctip_fp64},
             "cpu_baseline": cpu,
             "clocks": clk,
-            "energies_last_step": e,
+            "energies_last_status_step": e,
             "warmup_seconds": warm_s,
         }
         line.update(extras)

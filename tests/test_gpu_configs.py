@@ -126,7 +126,8 @@ def test_c1_slab_200_nve_steps_vs_oracle():
         g.set_state(q=o.q)
         g.force(energies=False)
         g.pme(energies=False)
-        e = g.md_run(nsteps, DT, first_step=2, thermostat=False, freq_new=0, freq_sort=1, freq_stat=nsteps)
+        # steps 2..201; energies on status steps only (MOD(step, freq_stat) == 0): the last one
+        e = g.md_run(nsteps, DT, first_step=2, thermostat=False, freq_new=0, freq_sort=1, freq_stat=nsteps + 1)
         st = g.get_state()
     dx = np.abs(st["x"] - o.x).max()
     dv = np.abs(st["v"] - v).max() / np.abs(v).max()
