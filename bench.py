@@ -443,6 +443,11 @@ def batch_object(nsys, steps, sequential=True):
            "autotune_ms_per_step": [round(t, 3) for t in times], "autotune_best_rule": int(best),
            "gpu_launches_per_step": launches}
     if sequential:
+        # untimed: each context captures its own step graphs (energy step and plain step)
+        for k, g in enumerate(members):
+            g.md_run(10, dt, first_step=step, thermostat=True, T_given=systems[k].meta["T"] * S.KB, freq_stat=10)
+            g.sync()
+        step += 10
         t1 = time.perf_counter()
         for k, g in enumerate(members):
             g.md_run(10, dt, first_step=step, thermostat=True, T_given=systems[k].meta["T"] * S.KB, freq_stat=10)
