@@ -395,12 +395,19 @@ int simox_get_tuning(simox_ctx* ctx, simox_tuning* t);
  * independent systems of different sizes, each a context created and set up
  * by the caller (simox_create, simox_set_state, simox_pme_self,
  * simox_cell_sort, charges), advanced together.  After one eager step per
- * system, one MD step of ALL systems is captured into one CUDA graph (one
- * branch per system, each with its PME side branch) and every further step
- * is a single graph launch.  The contexts must live on one device, use the
- * same freq_new/freq_sort/freq_stat, and have freq_new = 0 (charges held).
- * The batch does not own the contexts; after changing a member's atom set,
- * destroy and recreate the batch. */
+ * system, one MD step of ALL systems becomes one CUDA graph and every
+ * further step is a single graph launch.  In the per-pass mode (the
+ * default) the graph launches each kernel of the step ONCE for all systems
+ * (a work list of system blocks; each block reads its system's arguments
+ * from a device table) and each FFT once per group of systems with the same
+ * PME grid (batched cuFFT plans); this needs every system to take the same
+ * kernel sequence (mixed precision on the half list, the same PME order,
+ * thermostat and reflect setting), and a batch whose systems differ falls
+ * back to the per-system mode: one graph branch per system holding its own
+ * launches.  The contexts must live on one device, use the same
+ * freq_new/freq_sort/freq_stat, and have freq_new = 0 (charges held).  The
+ * batch does not own the contexts; destroy it before its members, and after
+ * changing a member's atom set destroy and recreate it. */
 typedef struct simox_batch simox_batch;
 int simox_batch_create(int nsys, simox_ctx* const* ctxs, simox_batch** out);
 int simox_batch_destroy(simox_batch* b);
@@ -415,8 +422,15 @@ int simox_batch_md_run(simox_batch* b, const simox_md_opts* opts, int first_step
  * (may be NULL) receives the per-step time of each candidate; *best the index. */
 int simox_batch_autotune(simox_batch* b, const simox_md_opts* opts, int first_step, int trial_steps,
                          double* times_ms, int* best);
-/* Kernels launched by the batch (graph kernel nodes counted per replay). */
+/* Kernels launched by the batch (graph kernel nodes counted per replay; a
+ * cuFFT execution counts as one). */
 int simox_batch_launch_count(simox_batch* b, long long* n);
+enum { SIMOX_BATCH_PER_PASS = 0, SIMOX_BATCH_PER_SYSTEM = 1 };
+/* Request a mode (SIMOX_BATCH_PER_PASS, the default, or
+ * SIMOX_BATCH_PER_SYSTEM); takes effect at the next step. */
+int simox_batch_set_mode(simox_batch* b, int mode);
+/* The mode of the last step the batch launched as a graph. */
+int simox_batch_get_mode(simox_batch* b, int* mode);
 
 /* ---- oxidation mode (main.f90:63-84), device-resident ------------------
  * The atom arrays hold the context's capacity, so NEW_O2 appends in place

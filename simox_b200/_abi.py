@@ -144,7 +144,7 @@ EXPORTED = [
     "simox_neighbor_stats", "simox_skin_rebuilds", "simox_cell_sort_noalloc",
     "simox_set_tuning", "simox_get_tuning",
     "simox_batch_create", "simox_batch_destroy", "simox_batch_md_run", "simox_batch_autotune",
-    "simox_batch_launch_count",
+    "simox_batch_launch_count", "simox_batch_set_mode", "simox_batch_get_mode",
     "simox_set_eam_spline", "simox_set_ctip_params", "simox_set_ctip_xi", "simox_adjoint_eval",
     "simox_adjoint_eval_many",
     "simox_remove_rigid_motion", "simox_oxide_check", "simox_new_o2", "simox_md_run_oxidation",

@@ -91,6 +91,8 @@ def lib():
         "simox_batch_md_run": [_vp, C.POINTER(MdOpts), C.c_int, C.c_int, C.POINTER(Energies)],
         "simox_batch_autotune": [_vp, C.POINTER(MdOpts), C.c_int, C.c_int, _dp, _ip],
         "simox_batch_launch_count": [_vp, C.POINTER(C.c_longlong)],
+        "simox_batch_set_mode": [_vp, C.c_int],
+        "simox_batch_get_mode": [_vp, _ip],
         "simox_set_eam_spline": [_vp, C.POINTER(EamSpline)],
         "simox_set_ctip_params": [_vp, C.c_int, C.c_double, C.c_double, C.c_double],
         "simox_set_ctip_xi": [_vp, C.c_int, C.c_double],
@@ -614,3 +616,18 @@ class Batch:
         n = C.c_longlong(0)
         _check(lib().simox_batch_launch_count(self._b, C.byref(n)), "batch_launch_count")
         return n.value
+
+    MODES = {"per_pass": 0, "per_system": 1}
+
+    def set_mode(self, mode: str) -> None:
+        """'per_pass' (default): each kernel of a step launched once for all
+        systems; 'per_system': one graph branch per system."""
+        if mode not in self.MODES:
+            raise ValueError(f"mode must be one of {sorted(self.MODES)}")
+        _check(lib().simox_batch_set_mode(self._b, self.MODES[mode]), "batch_set_mode")
+
+    def mode(self) -> str:
+        """The mode of the last step launched as a graph."""
+        m = C.c_int(0)
+        _check(lib().simox_batch_get_mode(self._b, C.byref(m)), "batch_get_mode")
+        return {v: k for k, v in self.MODES.items()}[m.value]

@@ -104,18 +104,18 @@ void prof_collect(simox_ctx* c) {
 static int pme_fork(simox_ctx* c, bool estep) {
     if (c->profiling) {
         const int st = pme_forces(c, false, estep, c->f_rec);
-        cudaEventRecord(c->ev_join, c->stream);
+        event_record(c, c->ev_join, c->stream);
         return st;
     }
-    cudaEventRecord(c->ev_fork, c->stream);
-    cudaStreamWaitEvent(c->side, c->ev_fork, 0);
+    event_record(c, c->ev_fork, c->stream);
+    stream_wait(c, c->side, c->ev_fork);
     std::swap(c->stream, c->side);
     pme_bind_stream(c);
     const int st = pme_forces(c, false, estep, c->f_rec);
     std::swap(c->stream, c->side);
     pme_bind_stream(c);
     if (st) return st;
-    cudaEventRecord(c->ev_join, c->side);
+    event_record(c, c->ev_join, c->side);
     return SIMOX_OK;
 }
 
@@ -125,7 +125,7 @@ static int pme_fork(simox_ctx* c, bool estep) {
 // captured into one CUDA graph.
 int md_step(simox_ctx* c, const simox_md_opts* o, bool sort, bool estep, bool want_rdf) {
     int st;
-    if (estep) cudaMemsetAsync(c->acc, 0, sizeof(double) * (A_EREC + 1), c->stream);
+    if (estep) memset_async(c, c->acc, 0, sizeof(double) * (A_EREC + 1), c->stream);
     const bool stoch = o->thermostat && o->thermo_stoch;
     if ((st = stoch ? nvt1_stoch(c, o->dt, o->alpha) : vv1(c, o->dt, o->reflect != 0))) return st;
     if (sort && (st = cell_sort(c))) return st;
@@ -137,7 +137,7 @@ int md_step(simox_ctx* c, const simox_md_opts* o, bool sort, bool estep, bool wa
     if ((st = ensure_list(c))) return st;
     if ((st = eam_density(c, estep))) return st;
     if ((st = pair_forces(c, estep, want_rdf))) return st;
-    cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+    stream_wait(c, c->stream, c->ev_join);
     if (stoch) st = nvt2_stoch(c, o->dt, o->alpha, o->T_given, o->seed, c->md_step_no, true, c->f_rec);
     else if (o->thermostat) st = nvt2_berend(c, o->dt, o->T_given, true, c->f_rec);
     else st = vv2(c, o->dt, true, c->f_rec);

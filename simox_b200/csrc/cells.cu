@@ -81,10 +81,10 @@ int build_cell_tables(simox_ctx* c) {
 
 // ---------------------------------------------------------------------------
 // CELL_SORT kernels
-__global__ void bin_atoms_kernel(int n, const double* __restrict__ x, double3 hbox, double3 lc, int3 nc,
-                                 int* __restrict__ cell_of, int* __restrict__ cell_xyz, int* __restrict__ count,
-                                 int* __restrict__ status) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void bin_atoms_body(Blk B, int n, const double* __restrict__ x, double3 hbox, double3 lc,
+                                               int3 nc, int* __restrict__ cell_of, int* __restrict__ cell_xyz,
+                                               int* __restrict__ count, int* __restrict__ status) {
+    int i = B.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int id[3];
     const double hb[3] = {hbox.x, hbox.y, hbox.z};
@@ -106,11 +106,17 @@ __global__ void bin_atoms_kernel(int n, const double* __restrict__ x, double3 hb
     cell_xyz[i] = id[0] | (id[1] << 10) | (id[2] << 20);   // Ncell <= 1024 per axis (checked at set-up)
     atomicAdd(count + cell, 1);
 }
+__global__ void bin_atoms_kernel(int n, const double* __restrict__ x, double3 hbox, double3 lc, int3 nc,
+                                 int* __restrict__ cell_of, int* __restrict__ cell_xyz, int* __restrict__ count,
+                                 int* __restrict__ status) {
+    bin_atoms_body(own_blk(), n, x, hbox, lc, nc, cell_of, cell_xyz, count, status);
+}
 
 // cond: nullptr, or a device flag that must be non-zero for the kernel to run
 // (the skin-list rebuild is decided on the device, without a host round trip)
-__global__ void scan_cells_kernel(const int* __restrict__ count, int* __restrict__ start, int* __restrict__ fill,
-                                  int ncell, int npt_max, int* __restrict__ status, const int* __restrict__ cond) {
+__device__ __forceinline__ void scan_cells_body(Blk B, const int* __restrict__ count, int* __restrict__ start,
+                                                int* __restrict__ fill, int ncell, int npt_max,
+                                                int* __restrict__ status, const int* __restrict__ cond) {
     if (cond && *cond == 0) return;
     __shared__ int sm[1024];
     __shared__ int carry;
@@ -136,22 +142,31 @@ __global__ void scan_cells_kernel(const int* __restrict__ count, int* __restrict
     }
     if (t == 0) start[ncell] = carry;
 }
+__global__ void scan_cells_kernel(const int* __restrict__ count, int* __restrict__ start, int* __restrict__ fill,
+                                  int ncell, int npt_max, int* __restrict__ status, const int* __restrict__ cond) {
+    scan_cells_body(own_blk(), count, start, fill, ncell, npt_max, status, cond);
+}
 
-__global__ void scatter_atoms_kernel(int n, const int* __restrict__ cell_of, int* __restrict__ fill,
-                                     int* __restrict__ sorted, const int* __restrict__ cond) {
+__device__ __forceinline__ void scatter_atoms_body(Blk B, int n, const int* __restrict__ cell_of,
+                                                   int* __restrict__ fill, int* __restrict__ sorted,
+                                                   const int* __restrict__ cond) {
     if (cond && *cond == 0) return;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int i = B.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int slot = atomicAdd(fill + cell_of[i], 1);
     sorted[slot] = i;
 }
+__global__ void scatter_atoms_kernel(int n, const int* __restrict__ cell_of, int* __restrict__ fill,
+                                     int* __restrict__ sorted, const int* __restrict__ cond) {
+    scatter_atoms_body(own_blk(), n, cell_of, fill, sorted, cond);
+}
 
 // Rank sort inside each cell: ascending original index (= CELL_SORT order).
-__global__ void cell_rank_sort_kernel(const int* __restrict__ start, int* __restrict__ sorted, int npt_max,
-                                      const int* __restrict__ cond) {
+__device__ __forceinline__ void cell_rank_sort_body(Blk B, const int* __restrict__ start, int* __restrict__ sorted,
+                                                    int npt_max, const int* __restrict__ cond) {
     if (cond && *cond == 0) return;
     extern __shared__ int buf[];
-    const int cc = blockIdx.x;
+    const int cc = B.x;
     const int s0 = start[cc], n = start[cc + 1] - s0;
     if (n <= 1 || n > npt_max) return;
     for (int k = threadIdx.x; k < n; k += blockDim.x) buf[k] = sorted[s0 + k];
@@ -162,21 +177,25 @@ __global__ void cell_rank_sort_kernel(const int* __restrict__ start, int* __rest
         sorted[s0 + rank] = v;
     }
 }
+__global__ void cell_rank_sort_kernel(const int* __restrict__ start, int* __restrict__ sorted, int npt_max,
+                                      const int* __restrict__ cond) {
+    cell_rank_sort_body(own_blk(), start, sorted, npt_max, cond);
+}
 
 int cell_sort(simox_ctx* c) {
     if (!c->have_ids) return SIMOX_E_STATE;
     const int n = c->n;
-    cudaMemsetAsync(c->cell_count, 0, sizeof(int) * c->ncell, c->stream);
+    memset_async(c, c->cell_count, 0, sizeof(int) * c->ncell, c->stream);
     if (n > 0) {
         Launch L(c, "cell_bin");
-        bin_atoms_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(
-            n, c->x, make_double3(c->hbox[0], c->hbox[1], c->hbox[2]), make_double3(c->lc[0], c->lc[1], c->lc[2]),
+        launch_k<256, 1, bin_atoms_body>(c, bin_atoms_kernel, (n + 255) / 256, 0, c->stream, n, c->x,
+            make_double3(c->hbox[0], c->hbox[1], c->hbox[2]), make_double3(c->lc[0], c->lc[1], c->lc[2]),
             make_int3(c->nc[0], c->nc[1], c->nc[2]), c->cell_of, c->cell_xyz, c->cell_count, c->status);
     }
     {
         Launch L(c, "cell_scan");
-        scan_cells_kernel<<<1, 1024, 0, c->stream>>>(c->cell_count, c->cell_start, c->cell_fill, c->ncell, c->npt_max,
-                                                     c->status, nullptr);
+        launch_k<1024, 1, scan_cells_body>(c, scan_cells_kernel, 1, 0, c->stream, c->cell_count, c->cell_start,
+            c->cell_fill, c->ncell, c->npt_max, c->status, nullptr);
     }
     int st = check_launch(c);
     if (st) return st;
@@ -199,12 +218,13 @@ int ensure_cell_lists(simox_ctx* c) {
     const int n = c->n;
     if (n > 0) {
         Launch L(c, "cell_scatter");
-        scatter_atoms_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, c->cell_of, c->cell_fill, c->sorted, nullptr);
+        launch_k<256, 1, scatter_atoms_body>(c, scatter_atoms_kernel, (n + 255) / 256, 0, c->stream, n, c->cell_of,
+            c->cell_fill, c->sorted, nullptr);
     }
     {
         Launch L(c, "cell_order");
-        cell_rank_sort_kernel<<<c->ncell, 128, sizeof(int) * c->npt_max, c->stream>>>(c->cell_start, c->sorted,
-                                                                                      c->npt_max, nullptr);
+        launch_k<128, 1, cell_rank_sort_body>(c, cell_rank_sort_kernel, c->ncell, sizeof(int) * c->npt_max, c->stream,
+            c->cell_start, c->sorted, c->npt_max, nullptr);
     }
     int st = check_launch(c);
     if (st) return st;
@@ -226,12 +246,14 @@ struct RecParams {
     int3 ncs;
 };
 
-__global__ void gather_sorted_kernel(int n, const int* __restrict__ sorted, const double* __restrict__ x,
-                                     const double* __restrict__ q, const int* __restrict__ id,
-                                     double4* __restrict__ xq, int* __restrict__ ts, const int* __restrict__ cell_xyz,
-                                     const int* __restrict__ cs_cell_of, RecParams R, float4* __restrict__ rec,
-                                     float4* __restrict__ frec, double4* __restrict__ xo) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void gather_sorted_body(Blk B, int n, const int* __restrict__ sorted,
+                                                   const double* __restrict__ x, const double* __restrict__ q,
+                                                   const int* __restrict__ id, double4* __restrict__ xq,
+                                                   int* __restrict__ ts, const int* __restrict__ cell_xyz,
+                                                   const int* __restrict__ cs_cell_of, const RecParams& R,
+                                                   float4* __restrict__ rec, float4* __restrict__ frec,
+                                                   double4* __restrict__ xo) {
+    int k = B.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     int o = sorted[k];
     const double x0 = x[3 * o], x1 = x[3 * o + 1], x2 = x[3 * o + 2];
@@ -255,6 +277,13 @@ __global__ void gather_sorted_kernel(int n, const int* __restrict__ sorted, cons
         xo[k] = make_double4(ox, oy, oz, q[o]);
     }
 }
+__global__ void gather_sorted_kernel(int n, const int* __restrict__ sorted, const double* __restrict__ x,
+                                     const double* __restrict__ q, const int* __restrict__ id,
+                                     double4* __restrict__ xq, int* __restrict__ ts, const int* __restrict__ cell_xyz,
+                                     const int* __restrict__ cs_cell_of, const __grid_constant__ RecParams R,
+                                     float4* __restrict__ rec, float4* __restrict__ frec, double4* __restrict__ xo) {
+    gather_sorted_body(own_blk(), n, sorted, x, q, id, xq, ts, cell_xyz, cs_cell_of, R, rec, frec, xo);
+}
 
 int gather_sorted(simox_ctx* c) {
     if (!c->cells_valid) return SIMOX_E_STATE;
@@ -267,8 +296,8 @@ int gather_sorted(simox_ctx* c) {
         R.lc = make_double3(c->lcs[0], c->lcs[1], c->lcs[2]);
         R.ncs = make_int3(c->ncs[0], c->ncs[1], c->ncs[2]);
         const bool skin = c->pair_order == c->perm && c->skin_mode;
-        gather_sorted_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(
-            c->n, c->pair_order, c->x, c->q, c->id, c->xq_s, c->t_s, c->cell_xyz, c->cs_cell_of, R,
+        launch_k<256, 1, gather_sorted_body>(c, gather_sorted_kernel, (c->n + 255) / 256, 0, c->stream, c->n,
+            c->pair_order, c->x, c->q, c->id, c->xq_s, c->t_s, c->cell_xyz, c->cs_cell_of, R,
             skin ? c->rec_s : nullptr, c->frec_s, c->xo_s);
     }
     c->gathered = true;
@@ -328,11 +357,12 @@ __device__ __forceinline__ void list_append(unsigned* row, int2& my, int cap, un
 // squared norm.  Pairs within 4e-5 of Rcut^2, home atoms outside their cell
 // and the generic (multi-image) path use the reference's exact FP64 r2.
 template <bool FAST>
-__global__ void __launch_bounds__(LB_THREADS)
-    build_list_kernel(const int* __restrict__ cell_start, const int* __restrict__ entries,
-                      const double4* __restrict__ xq, const int* __restrict__ ts, unsigned* __restrict__ nbr,
-                      int2* __restrict__ nn, LBParams P, int* __restrict__ status, int* __restrict__ nn_max,
-                      unsigned long long* __restrict__ nn_tot, const int* __restrict__ cond) {
+__device__ __forceinline__ void build_list_body(Blk B, const int* __restrict__ cell_start,
+                                                const int* __restrict__ entries, const double4* __restrict__ xq,
+                                                const int* __restrict__ ts, unsigned* __restrict__ nbr,
+                                                int2* __restrict__ nn, const LBParams& P, int* __restrict__ status,
+                                                int* __restrict__ nn_max, unsigned long long* __restrict__ nn_tot,
+                                                const int* __restrict__ cond) {
     if (cond && *cond == 0) return;
     extern __shared__ __align__(16) unsigned char smem[];
     float4* cpos = reinterpret_cast<float4*>(smem);
@@ -340,7 +370,7 @@ __global__ void __launch_bounds__(LB_THREADS)
     int2* cnt = reinterpret_cast<int2*>(ctag + LB_TILE);
     __shared__ int es0[kEntries], edir[kEntries], epre[kEntries + 1];
 
-    const int cc = blockIdx.x;
+    const int cc = B.x;
     const int h0 = cell_start[cc], nh = cell_start[cc + 1] - h0;
     if (nh <= 0) return;
     const int tid = threadIdx.x;
@@ -446,14 +476,23 @@ __global__ void __launch_bounds__(LB_THREADS)
     atomicMax(nn_max, lmax);
     atomicAdd(nn_tot, ltot);
 }
+template <bool FAST>
+__global__ void __launch_bounds__(LB_THREADS)
+    build_list_kernel(const int* __restrict__ cell_start, const int* __restrict__ entries,
+                      const double4* __restrict__ xq, const int* __restrict__ ts, unsigned* __restrict__ nbr,
+                      int2* __restrict__ nn, const __grid_constant__ LBParams P, int* __restrict__ status,
+                      int* __restrict__ nn_max, unsigned long long* __restrict__ nn_tot,
+                      const int* __restrict__ cond) {
+    build_list_body<FAST>(own_blk(), cell_start, entries, xq, ts, nbr, nn, P, status, nn_max, nn_tot, cond);
+}
 
 int build_list(simox_ctx* c) {
     if (!c->gathered) {
         int st = gather_sorted(c);
         if (st) return st;
     }
-    cudaMemsetAsync(c->nn_max, 0, sizeof(int), c->stream);
-    cudaMemsetAsync(c->nn_tot, 0, sizeof(unsigned long long), c->stream);
+    memset_async(c, c->nn_max, 0, sizeof(int), c->stream);
+    memset_async(c, c->nn_tot, 0, sizeof(unsigned long long), c->stream);
     LBParams P;
     P.box = make_double3(c->box[0], c->box[1], c->box[2]);
     P.ibox = make_double3(c->inv_box[0], c->inv_box[1], c->inv_box[2]);
@@ -474,11 +513,11 @@ int build_list(simox_ctx* c) {
     {
         Launch L(c, "neighbor_list");
         if (c->fast_cells)
-            build_list_kernel<true><<<c->ncell, LB_THREADS, smem, c->stream>>>(
+            launch_k<LB_THREADS, 1, build_list_body<true>>(c, build_list_kernel<true>, c->ncell, smem, c->stream,
                 c->cell_start, c->entries, c->xq_s, c->t_s, c->nbr, reinterpret_cast<int2*>(c->nn), P, c->status,
                 c->nn_max, c->nn_tot, nullptr);
         else
-            build_list_kernel<false><<<c->ncell, LB_THREADS, smem, c->stream>>>(
+            launch_k<LB_THREADS, 1, build_list_body<false>>(c, build_list_kernel<false>, c->ncell, smem, c->stream,
                 c->cell_start, c->entries, c->xq_s, c->t_s, c->nbr, reinterpret_cast<int2*>(c->nn), P, c->status,
                 c->nn_max, c->nn_tot, nullptr);
     }
@@ -504,9 +543,10 @@ int build_list(simox_ctx* c) {
 
 // rebuild flag: 1 if any atom moved more than skin/2 since the last rebuild
 // (minimum image: an atom that VV_NVE1 wrapped across the box has not moved by L)
-__global__ void skin_check_kernel(int n, const double* __restrict__ x, const double* __restrict__ x0, double3 box,
-                                  double3 ibox, double lim2, int* __restrict__ flag) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void skin_check_body(Blk B, int n, const double* __restrict__ x,
+                                                const double* __restrict__ x0, double3 box, double3 ibox, double lim2,
+                                                int* __restrict__ flag) {
+    const int i = B.x * blockDim.x + threadIdx.x;
     bool need = false;
     if (i < n) {
         double dx = x[3 * i] - x0[3 * i], dy = x[3 * i + 1] - x0[3 * i + 1], dz = x[3 * i + 2] - x0[3 * i + 2];
@@ -517,14 +557,18 @@ __global__ void skin_check_kernel(int n, const double* __restrict__ x, const dou
     }
     if (__any_sync(0xffffffffu, need) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
 }
+__global__ void skin_check_kernel(int n, const double* __restrict__ x, const double* __restrict__ x0, double3 box,
+                                  double3 ibox, double lim2, int* __restrict__ flag) {
+    skin_check_body(own_blk(), n, x, x0, box, ibox, lim2, flag);
+}
 
 // bin on the skin grid and remember the positions of this rebuild;
 // cond[0] = rebuild flag, cond[1] counts the rebuilds
-__global__ void skin_bin_kernel(int n, const double* __restrict__ x, double3 hbox, double3 ilc, int3 nc,
-                                int* __restrict__ cell_of, int* __restrict__ count, double* __restrict__ x0,
-                                int* __restrict__ cond) {
+__device__ __forceinline__ void skin_bin_body(Blk B, int n, const double* __restrict__ x, double3 hbox, double3 ilc,
+                                              int3 nc, int* __restrict__ cell_of, int* __restrict__ count,
+                                              double* __restrict__ x0, int* __restrict__ cond) {
     if (cond[0] == 0) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = B.x * blockDim.x + threadIdx.x;
     if (i == 0) cond[1] += 1;
     if (i >= n) return;
     const double xx[3] = {x[3 * i], x[3 * i + 1], x[3 * i + 2]};
@@ -541,6 +585,11 @@ __global__ void skin_bin_kernel(int n, const double* __restrict__ x, double3 hbo
     const int c = id[0] + id[1] * m[0] + id[2] * m[0] * m[1];
     cell_of[i] = c;
     atomicAdd(count + c, 1);
+}
+__global__ void skin_bin_kernel(int n, const double* __restrict__ x, double3 hbox, double3 ilc, int3 nc,
+                                int* __restrict__ cell_of, int* __restrict__ count, double* __restrict__ x0,
+                                int* __restrict__ cond) {
+    skin_bin_body(own_blk(), n, x, hbox, ilc, nc, cell_of, count, x0, cond);
 }
 
 // Choose the pair-kernel order for the current state and gather into it.  In
@@ -564,41 +613,43 @@ static int prepare_order(simox_ctx* c) {
     c->skin_half = c->precision != SIMOX_FP64 && c->g0_species >= 0;
     int* flag = c->skin_flag;
     if (!c->skin_valid) {
+        // a new atom set: the first list is seeded from the host (not batched)
+        if (c->rec) c->rec->bad = true;
         const int one = 1;
         cudaMemcpyAsync(flag, &one, sizeof(int), cudaMemcpyHostToDevice, s);
     } else {
-        cudaMemsetAsync(flag, 0, sizeof(int), s);
+        memset_async(c, flag, 0, sizeof(int), s);
         if (n > 0) {
             Launch L(c, "skin_check");
             const double h = 0.5 * c->skin;
-            skin_check_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, c->x, c->x0,
-                                                              make_double3(c->box[0], c->box[1], c->box[2]),
-                                                              make_double3(c->inv_box[0], c->inv_box[1], c->inv_box[2]),
-                                                              h * h, flag);
+            launch_k<256, 1, skin_check_body>(c, skin_check_kernel, (n + 255) / 256, 0, s, n, c->x, c->x0,
+                make_double3(c->box[0], c->box[1], c->box[2]),
+                make_double3(c->inv_box[0], c->inv_box[1], c->inv_box[2]), h * h, flag);
         }
     }
     // conditional rebuild of the order (binning on the skin grid)
-    cudaMemsetAsync(c->cs_count, 0, sizeof(int) * c->ncell_s, s);
+    memset_async(c, c->cs_count, 0, sizeof(int) * c->ncell_s, s);
     if (n > 0) {
         Launch L(c, "skin_bin");
-        skin_bin_kernel<<<(n + 255) / 256, 256, 0, s>>>(
-            n, c->x, make_double3(c->hbox[0], c->hbox[1], c->hbox[2]),
-            make_double3(1.0 / c->lcs[0], 1.0 / c->lcs[1], 1.0 / c->lcs[2]), make_int3(c->ncs[0], c->ncs[1], c->ncs[2]),
-            c->cs_cell_of, c->cs_count, c->x0, flag);
+        launch_k<256, 1, skin_bin_body>(c, skin_bin_kernel, (n + 255) / 256, 0, s, n, c->x,
+            make_double3(c->hbox[0], c->hbox[1], c->hbox[2]),
+            make_double3(1.0 / c->lcs[0], 1.0 / c->lcs[1], 1.0 / c->lcs[2]),
+            make_int3(c->ncs[0], c->ncs[1], c->ncs[2]), c->cs_cell_of, c->cs_count, c->x0, flag);
     }
     {
         Launch L(c, "skin_scan");
-        scan_cells_kernel<<<1, 1024, 0, s>>>(c->cs_count, c->cs_start, c->cs_fill, c->ncell_s, c->npt_max_s, c->status,
-                                             flag);
+        launch_k<1024, 1, scan_cells_body>(c, scan_cells_kernel, 1, 0, s, c->cs_count, c->cs_start, c->cs_fill,
+            c->ncell_s, c->npt_max_s, c->status, flag);
     }
     if (n > 0) {
         Launch L(c, "skin_scatter");
-        scatter_atoms_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, c->cs_cell_of, c->cs_fill, c->perm, flag);
+        launch_k<256, 1, scatter_atoms_body>(c, scatter_atoms_kernel, (n + 255) / 256, 0, s, n, c->cs_cell_of,
+            c->cs_fill, c->perm, flag);
     }
     {
         Launch L(c, "skin_order");
-        cell_rank_sort_kernel<<<c->ncell_s, 128, sizeof(int) * c->npt_max_s, s>>>(c->cs_start, c->perm, c->npt_max_s,
-                                                                                  flag);
+        launch_k<128, 1, cell_rank_sort_body>(c, cell_rank_sort_kernel, c->ncell_s, sizeof(int) * c->npt_max_s, s,
+            c->cs_start, c->perm, c->npt_max_s, flag);
     }
     int st = gather_sorted(c);
     if (st) return st;
@@ -622,17 +673,17 @@ static int prepare_order(simox_ctx* c) {
     const size_t smem = LB_TILE * (sizeof(float4) + sizeof(unsigned)) + sizeof(int2) * c->npt_max_s;
     {
         Launch L(c, "skin_list");
-        build_list_kernel<true><<<c->ncell_s, LB_THREADS, smem, s>>>(
-            c->cs_start, c->cs_entries, c->xq_s, c->t_s, c->nbr_s, reinterpret_cast<int2*>(c->nn_s), P, c->status,
-            c->nn_max, c->nn_tot, flag);
+        launch_k<LB_THREADS, 1, build_list_body<true>>(c, build_list_kernel<true>, c->ncell_s, smem, s, c->cs_start,
+            c->cs_entries, c->xq_s, c->t_s, c->nbr_s, reinterpret_cast<int2*>(c->nn_s), P, c->status, c->nn_max,
+            c->nn_tot, flag);
     }
     c->skin_valid = true;
     return check_launch(c);
 }
 
 static int filter_list(simox_ctx* c) {
-    cudaMemsetAsync(c->nn_max, 0, sizeof(int), c->stream);
-    cudaMemsetAsync(c->nn_tot, 0, sizeof(unsigned long long), c->stream);
+    memset_async(c, c->nn_max, 0, sizeof(int), c->stream);
+    memset_async(c, c->nn_tot, 0, sizeof(unsigned long long), c->stream);
     int st = filter_density(c);
     if (st) return st;
     c->list_valid = true;

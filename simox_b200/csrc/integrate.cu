@@ -24,9 +24,10 @@ __device__ __forceinline__ double half_kick(double v, double f, double dt, doubl
     return __dadd_rn(v, __ddiv_rn(__dmul_rn(__dmul_rn(0.5, dt), f), xm));
 }
 
-__global__ void vv1_kernel(int n, const int* __restrict__ id, double* __restrict__ x, double* __restrict__ v,
-                           const double* __restrict__ f, double dt, double3 box, Masses M, int reflect) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void vv1_body(Blk B, int n, const int* __restrict__ id, double* __restrict__ x,
+                                         double* __restrict__ v, const double* __restrict__ f, double dt, double3 box,
+                                         const Masses& M, int reflect) {
+    const int i = B.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double xm = M.xm[id[i] - 1];
     const double L[3] = {box.x, box.y, box.z};
@@ -51,17 +52,22 @@ __global__ void vv1_kernel(int n, const int* __restrict__ id, double* __restrict
         x[3 * i + 2] = z;
     }
 }
+__global__ void __launch_bounds__(256) vv1_kernel(int n, const int* __restrict__ id, double* __restrict__ x,
+                                                  double* __restrict__ v, const double* __restrict__ f, double dt,
+                                                  double3 box, const __grid_constant__ Masses M, int reflect) {
+    vv1_body(own_blk(), n, id, x, v, f, dt, box, M, reflect);
+}
 
 // second half kick (+ optional mean-force removal); mv2 and per-species sums
 template <bool BEREND>
-__global__ void __launch_bounds__(256)
-    vv2_kernel(int n, const int* __restrict__ id, double* __restrict__ v, double* __restrict__ f,
-               const double* __restrict__ f_add, double dt, Masses M, double* __restrict__ acc, int subtract_mean) {
+__device__ __forceinline__ void vv2_body(Blk B, int n, const int* __restrict__ id, double* __restrict__ v,
+                                         double* __restrict__ f, const double* __restrict__ f_add, double dt,
+                                         const Masses& M, double* __restrict__ acc, int subtract_mean) {
     __shared__ double red[256 / 32];
     double mv2 = 0.0;
     double ms[5] = {0, 0, 0, 0, 0};
     double ns[5] = {0, 0, 0, 0, 0};
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = B.x * blockDim.x + threadIdx.x;
     if (i < n) {
         const int s = id[i] - 1;
         const double xm = M.xm[s];
@@ -95,11 +101,17 @@ __global__ void __launch_bounds__(256)
         block_add<256>(mv2, acc, A_MV2, red);
     }
 }
+template <bool BEREND>
+__global__ void __launch_bounds__(256)
+    vv2_kernel(int n, const int* __restrict__ id, double* __restrict__ v, double* __restrict__ f,
+               const double* __restrict__ f_add, double dt, const __grid_constant__ Masses M,
+               double* __restrict__ acc, int subtract_mean) {
+    vv2_body<BEREND>(own_blk(), n, id, v, f, f_add, dt, M, acc, subtract_mean);
+}
 
 // Berendsen rescale (vverlet.f90:188-205)
-__global__ void __launch_bounds__(256)
-    berend_scale_kernel(int n, const int* __restrict__ id, double* __restrict__ v, Masses M, double T_given,
-                        double* __restrict__ acc) {
+__device__ __forceinline__ void berend_scale_body(Blk B, int n, const int* __restrict__ id, double* __restrict__ v,
+                                                  const Masses& M, double T_given, double* __restrict__ acc) {
     __shared__ double red[256 / 32];
     __shared__ double lam[5];
     if (threadIdx.x < 5) {
@@ -114,7 +126,7 @@ __global__ void __launch_bounds__(256)
     }
     __syncthreads();
     double mv2 = 0.0;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = B.x * blockDim.x + threadIdx.x;
     if (i < n) {
         const int s = id[i] - 1;
         const double xm = M.xm[s];
@@ -128,6 +140,11 @@ __global__ void __launch_bounds__(256)
         mv2 = t;
     }
     block_add<256>(mv2, acc, A_MV2, red);
+}
+__global__ void __launch_bounds__(256)
+    berend_scale_kernel(int n, const int* __restrict__ id, double* __restrict__ v, const __grid_constant__ Masses M,
+                        double T_given, double* __restrict__ acc) {
+    berend_scale_body(own_blk(), n, id, v, M, T_given, acc);
 }
 
 // ---------------------------------------------------------------------------
@@ -266,9 +283,9 @@ __global__ void vv1_stoch_kernel(int n, const int* __restrict__ id, double* __re
 // mean force as in vv2_kernel.
 __global__ void __launch_bounds__(256)
     vv2_stoch_kernel(int n, const int* __restrict__ id, double* __restrict__ v, double* __restrict__ f,
-                     const double* __restrict__ f_add, double dt, double alpha, double beta,
-                     unsigned long long seed, unsigned long long step, Masses M, double* __restrict__ acc,
-                     int subtract_mean, int* __restrict__ status) {
+                     const double* __restrict__ f_add, double dt, double alpha, double beta, unsigned long long seed,
+                     unsigned long long step, Masses M, double* __restrict__ acc, int subtract_mean,
+                     int* __restrict__ status) {
     __shared__ double red[256 / 32];
     double mv2 = 0.0;
     int bad = 0;
@@ -306,9 +323,8 @@ int vv1(simox_ctx* c, double dt, bool reflect) {
     if (c->n == 0) return SIMOX_OK;
     {
         Launch L(c, reflect ? "vv_nve1_reflect" : "vv_nve1");
-        vv1_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->n, c->id, c->x, c->v, c->f, dt,
-                                                              make_double3(c->box[0], c->box[1], c->box[2]), masses(c),
-                                                              reflect ? 1 : 0);
+        launch_k<256, 1, vv1_body>(c, vv1_kernel, (c->n + 255) / 256, 0, c->stream, c->n, c->id, c->x, c->v, c->f, dt,
+            make_double3(c->box[0], c->box[1], c->box[2]), masses(c), reflect ? 1 : 0);
     }
     c->gathered = false;
     c->list_valid = false;
@@ -319,27 +335,28 @@ int vv1(simox_ctx* c, double dt, bool reflect) {
 }
 
 int vv2(simox_ctx* c, double dt, bool subtract_mean, const double* f_add) {
-    cudaMemsetAsync(c->acc + A_MV2, 0, sizeof(double), c->stream);
+    memset_async(c, c->acc + A_MV2, 0, sizeof(double), c->stream);
     if (c->n == 0) return SIMOX_OK;
     {
         Launch L(c, "vv_nve2");
-        vv2_kernel<false><<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->n, c->id, c->v, c->f, f_add, dt, masses(c),
-                                                                     c->acc, subtract_mean ? 1 : 0);
+        launch_k<256, 1, vv2_body<false>>(c, vv2_kernel<false>, (c->n + 255) / 256, 0, c->stream, c->n, c->id, c->v,
+            c->f, f_add, dt, masses(c), c->acc, subtract_mean ? 1 : 0);
     }
     return check_launch(c);
 }
 
 int nvt2_berend(simox_ctx* c, double dt, double T_given, bool subtract_mean, const double* f_add) {
-    cudaMemsetAsync(c->acc + A_MV2, 0, sizeof(double) * (A_NS4 + 1 - A_MV2), c->stream);
+    memset_async(c, c->acc + A_MV2, 0, sizeof(double) * (A_NS4 + 1 - A_MV2), c->stream);
     if (c->n == 0) return SIMOX_OK;
     {
         Launch L(c, "vv_nvt2_kick");
-        vv2_kernel<true><<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->n, c->id, c->v, c->f, f_add, dt, masses(c),
-                                                                    c->acc, subtract_mean ? 1 : 0);
+        launch_k<256, 1, vv2_body<true>>(c, vv2_kernel<true>, (c->n + 255) / 256, 0, c->stream, c->n, c->id, c->v,
+            c->f, f_add, dt, masses(c), c->acc, subtract_mean ? 1 : 0);
     }
     {
         Launch L(c, "vv_nvt2_scale");
-        berend_scale_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->n, c->id, c->v, masses(c), T_given, c->acc);
+        launch_k<256, 1, berend_scale_body>(c, berend_scale_kernel, (c->n + 255) / 256, 0, c->stream, c->n, c->id,
+            c->v, masses(c), T_given, c->acc);
     }
     return check_launch(c);
 }

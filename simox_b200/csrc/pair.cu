@@ -913,8 +913,8 @@ int eam_density(simox_ctx* c, bool eflag) {
     // a half list carries each pair once: its densities come only from the
     // half-list filter pass (both atoms of each pair)
     if (!c->rho_ready && half_path(c)) {
-        cudaMemsetAsync(c->nn_max, 0, sizeof(int), c->stream);
-        cudaMemsetAsync(c->nn_tot, 0, sizeof(unsigned long long), c->stream);
+        memset_async(c, c->nn_max, 0, sizeof(int), c->stream);
+        memset_async(c, c->nn_tot, 0, sizeof(unsigned long long), c->stream);
         if ((st = filter_density(c))) return st;
     }
     // the skin filter already produced rho and F' in the context's precision

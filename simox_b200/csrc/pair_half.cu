@@ -264,13 +264,14 @@ __device__ __forceinline__ void filter_half_atoms(const Half1Params& H, const fl
     }
 }
 
-__global__ void __launch_bounds__(kH1Threads)
-    filter_half_kernel(const __grid_constant__ Half1Params H, const PairTab<float>* __restrict__ tab,
-                       const double4* __restrict__ xq, const float4* __restrict__ rec, const int* __restrict__ order,
-                       const int* __restrict__ cs_start, const int* __restrict__ cs_entries,
-                       const int2* __restrict__ nn_s, const unsigned* __restrict__ nbr_s, int2* __restrict__ nn,
-                       unsigned* __restrict__ nbr, u64* __restrict__ rho_fx, int* __restrict__ status,
-                       int* __restrict__ nn_max, unsigned long long* __restrict__ nn_tot) {
+__device__ __forceinline__ void filter_half_body(Blk B, const Half1Params& H, const PairTab<float>* __restrict__ tab,
+                                                 const double4* __restrict__ xq, const float4* __restrict__ rec,
+                                                 const int* __restrict__ order, const int* __restrict__ cs_start,
+                                                 const int* __restrict__ cs_entries, const int2* __restrict__ nn_s,
+                                                 const unsigned* __restrict__ nbr_s, int2* __restrict__ nn,
+                                                 unsigned* __restrict__ nbr, u64* __restrict__ rho_fx,
+                                                 int* __restrict__ status, int* __restrict__ nn_max,
+                                                 unsigned long long* __restrict__ nn_tot) {
     __shared__ unsigned alo[kH1Cap], ahi[kH1Cap];
     __shared__ DensC<float> dsh[64];
     __shared__ int dflag[64];
@@ -296,7 +297,7 @@ __global__ void __launch_bounds__(kH1Threads)
     }
     for (int k = tid; k < kEntries; k += blockDim.x) ssh[k] = H.F.sh[k];
     if (tid == 0) next = 0;
-    const int cell = blockIdx.x / H.splits, part = blockIdx.x - cell * H.splits;
+    const int cell = B.x / H.splits, part = B.x - cell * H.splits;
     half_tile_setup(T, cs_start, cs_entries, cell);
     const int total = T.off[kHalfCells];
     const int2 br = half_range(T, part, H.splits);
@@ -331,12 +332,23 @@ __global__ void __launch_bounds__(kH1Threads)
     __syncthreads();
     if (tiled) half_tile_flush(T, total, alo, ahi, 0, 1, rho_fx, 0);
 }
+__global__ void __launch_bounds__(kH1Threads)
+    filter_half_kernel(const __grid_constant__ Half1Params H, const PairTab<float>* __restrict__ tab,
+                       const double4* __restrict__ xq, const float4* __restrict__ rec, const int* __restrict__ order,
+                       const int* __restrict__ cs_start, const int* __restrict__ cs_entries,
+                       const int2* __restrict__ nn_s, const unsigned* __restrict__ nbr_s, int2* __restrict__ nn,
+                       unsigned* __restrict__ nbr, u64* __restrict__ rho_fx, int* __restrict__ status,
+                       int* __restrict__ nn_max, unsigned long long* __restrict__ nn_tot) {
+    filter_half_body(own_blk(), H, tab, xq, rec, order, cs_start, cs_entries, nn_s, nbr_s, nn, nbr, rho_fx, status,
+        nn_max, nn_tot);
+}
 
 // rho from the fixed-point sums, then F'(rho) (force.f90:256-351)
-__global__ void embed_half_kernel(int n, const int* __restrict__ ts, const u64* __restrict__ rho_fx, EmbedParams E,
-                                  double* __restrict__ rho_s, double* __restrict__ dF_s, float* __restrict__ dF_f,
-                                  int* __restrict__ status) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void embed_half_body(Blk B, int n, const int* __restrict__ ts,
+                                                const u64* __restrict__ rho_fx, const EmbedParams& E,
+                                                double* __restrict__ rho_s, double* __restrict__ dF_s,
+                                                float* __restrict__ dF_f, int* __restrict__ status) {
+    const int k = B.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const double rho = (double)(long long)rho_fx[k] * kRhoUnit;
     double F, dF;
@@ -344,6 +356,11 @@ __global__ void embed_half_kernel(int n, const int* __restrict__ ts, const u64* 
     rho_s[k] = rho;
     dF_s[k] = dF;
     dF_f[k] = (float)dF;
+}
+__global__ void embed_half_kernel(int n, const int* __restrict__ ts, const u64* __restrict__ rho_fx,
+                                  const __grid_constant__ EmbedParams E, double* __restrict__ rho_s,
+                                  double* __restrict__ dF_s, float* __restrict__ dF_f, int* __restrict__ status) {
+    embed_half_body(own_blk(), n, ts, rho_fx, E, rho_s, dF_s, dF_f, status);
 }
 
 // ---------------------------------------------------------------------------
@@ -542,12 +559,13 @@ __device__ __forceinline__ void force_half_atoms(const Half2Params& H, const int
 }
 
 template <bool RDF>
-__global__ void __launch_bounds__(kH2Threads, 1)
-    force_half_kernel(const __grid_constant__ Half2Params H, const int* __restrict__ cs_start,
-                      const int* __restrict__ cs_entries, const double4* __restrict__ xo,
-                      const int* __restrict__ ts, const int2* __restrict__ nn, const unsigned* __restrict__ nbr,
-                      const float* __restrict__ dF_f, u64* __restrict__ f_fx, int* __restrict__ rdf,
-                      const float4* __restrict__ rec, const int* __restrict__ order, int* __restrict__ status) {
+__device__ __forceinline__ void force_half_body(Blk B, const Half2Params& H, const int* __restrict__ cs_start,
+                                                const int* __restrict__ cs_entries, const double4* __restrict__ xo,
+                                                const int* __restrict__ ts, const int2* __restrict__ nn,
+                                                const unsigned* __restrict__ nbr, const float* __restrict__ dF_f,
+                                                u64* __restrict__ f_fx, int* __restrict__ rdf,
+                                                const float4* __restrict__ rec, const int* __restrict__ order,
+                                                int* __restrict__ status) {
     constexpr int NB = SIMOX_NRDF + 2;
     extern __shared__ __align__(16) unsigned char half_smem[];
     double4* tpos = reinterpret_cast<double4*>(half_smem);                 // partner offsets + shift, charge
@@ -560,7 +578,7 @@ __global__ void __launch_bounds__(kH2Threads, 1)
     __shared__ int next;
     __shared__ int hist[RDF ? 4 * NB : 1];     // (metal, O) x (metal, O) kinds of the reference's (i, j)
     const int tid = threadIdx.x;
-    const int cell = blockIdx.x / H.splits, part = blockIdx.x - cell * H.splits;
+    const int cell = B.x / H.splits, part = B.x - cell * H.splits;
     if (tid == 0) next = 0;
     if (RDF)
         for (int k = tid; k < 4 * NB; k += kH2Threads) hist[k] = 0;
@@ -619,16 +637,29 @@ __global__ void __launch_bounds__(kH2Threads, 1)
         }
     }
 }
+template <bool RDF>
+__global__ void __launch_bounds__(kH2Threads, 1)
+    force_half_kernel(const __grid_constant__ Half2Params H, const int* __restrict__ cs_start,
+                      const int* __restrict__ cs_entries, const double4* __restrict__ xo, const int* __restrict__ ts,
+                      const int2* __restrict__ nn, const unsigned* __restrict__ nbr, const float* __restrict__ dF_f,
+                      u64* __restrict__ f_fx, int* __restrict__ rdf, const float4* __restrict__ rec,
+                      const int* __restrict__ order, int* __restrict__ status) {
+    force_half_body<RDF>(own_blk(), H, cs_start, cs_entries, xo, ts, nn, nbr, dF_f, f_fx, rdf, rec, order, status);
+}
 
 // forces from the fixed-point sums into the original atom order
-__global__ void force_half_finalize_kernel(int n, const u64* __restrict__ f_fx, int fstride,
-                                           const int* __restrict__ order, double* __restrict__ f) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void force_half_finalize_body(Blk B, int n, const u64* __restrict__ f_fx, int fstride,
+                                                         const int* __restrict__ order, double* __restrict__ f) {
+    const int k = B.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const int o = order[k];
     f[3 * o] = (double)(long long)f_fx[k] * kForceUnit;
     f[3 * o + 1] = (double)(long long)f_fx[fstride + k] * kForceUnit;
     f[3 * o + 2] = (double)(long long)f_fx[2 * fstride + k] * kForceUnit;
+}
+__global__ void force_half_finalize_kernel(int n, const u64* __restrict__ f_fx, int fstride,
+                                           const int* __restrict__ order, double* __restrict__ f) {
+    force_half_finalize_body(own_blk(), n, f_fx, fstride, order, f);
 }
 
 // ---------------------------------------------------------------------------
@@ -776,9 +807,9 @@ __device__ __forceinline__ void ctip_half_atoms(const CtipHalfParams& C, const f
 template <bool WITH_C>
 __global__ void __launch_bounds__(kH2Threads, 1)
     ctip_half_kernel(const __grid_constant__ CtipHalfParams C, const int* __restrict__ cs_start,
-                     const int* __restrict__ cs_entries, const float4* __restrict__ frec,
-                     const int* __restrict__ ts, const int2* __restrict__ nn, const unsigned* __restrict__ nbr,
-                     const double* __restrict__ vin, u64* __restrict__ gacc, int gstride) {
+                     const int* __restrict__ cs_entries, const float4* __restrict__ frec, const int* __restrict__ ts,
+                     const int2* __restrict__ nn, const unsigned* __restrict__ nbr, const double* __restrict__ vin,
+                     u64* __restrict__ gacc, int gstride) {
     extern __shared__ __align__(16) unsigned char ctip_smem[];
     float4* trec = reinterpret_cast<float4*>(ctip_smem);
     double* tv = reinterpret_cast<double*>(trec + kHCCap);
@@ -846,10 +877,11 @@ __global__ void ctip_half_finalize_kernel(int n, const u64* __restrict__ gacc, i
 // embedding energy from the completed densities.
 constexpr int kHEThreads = 128;
 
-__global__ void __launch_bounds__(kHEThreads, 6)
-    energy_half_kernel(PairParams P, const PairTab<double>* __restrict__ tab, const double4* __restrict__ xq,
-                       const int* __restrict__ ts, const int2* __restrict__ nn, const unsigned* __restrict__ nbr,
-                       u64* __restrict__ rho_fx, double* __restrict__ acc, int* __restrict__ status) {
+__device__ __forceinline__ void energy_half_body(Blk B, const PairParams& P, const PairTab<double>* __restrict__ tab,
+                                                 const double4* __restrict__ xq, const int* __restrict__ ts,
+                                                 const int2* __restrict__ nn, const unsigned* __restrict__ nbr,
+                                                 u64* __restrict__ rho_fx, double* __restrict__ acc,
+                                                 int* __restrict__ status) {
     __shared__ PairTab<double> st[kSpecies * kSpecies];
     __shared__ double red[kHEThreads / 32];
     for (int k = threadIdx.x; k < kSpecies * kSpecies; k += blockDim.x) st[k] = tab[k];
@@ -857,7 +889,7 @@ __global__ void __launch_bounds__(kHEThreads, 6)
     const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
     double ep = 0.0, ed = 0.0, ec = 0.0;
     int bad = 0;
-    for (int X = blockIdx.x * wpb + (threadIdx.x >> 5); X < P.n; X += gridDim.x * wpb) {
+    for (int X = B.x * wpb + (threadIdx.x >> 5); X < P.n; X += B.n * wpb) {
         const double4 xa = xq[X];
         const int sX = ts[X];
         const int2 m = nn[X];
@@ -901,19 +933,32 @@ __global__ void __launch_bounds__(kHEThreads, 6)
     block_add<kHEThreads>(ed, acc, A_EDIR, red);
     block_add<kHEThreads>(ec, acc, A_ECTIP, red);
 }
+__global__ void __launch_bounds__(kHEThreads, 6)
+    energy_half_kernel(const __grid_constant__ PairParams P, const PairTab<double>* __restrict__ tab,
+                       const double4* __restrict__ xq, const int* __restrict__ ts, const int2* __restrict__ nn,
+                       const unsigned* __restrict__ nbr, u64* __restrict__ rho_fx, double* __restrict__ acc,
+                       int* __restrict__ status) {
+    energy_half_body(own_blk(), P, tab, xq, ts, nn, nbr, rho_fx, acc, status);
+}
 
-__global__ void __launch_bounds__(256)
-    embed_energy_half_kernel(int n, const int* __restrict__ ts, const u64* __restrict__ rho_fx, EmbedParams E,
-                             double* __restrict__ acc, int* __restrict__ status) {
+__device__ __forceinline__ void embed_energy_half_body(Blk B, int n, const int* __restrict__ ts,
+                                                       const u64* __restrict__ rho_fx, const EmbedParams& E,
+                                                       double* __restrict__ acc, int* __restrict__ status) {
     __shared__ double red[256 / 32];
     double eg = 0.0;
-    const int X = blockIdx.x * blockDim.x + threadIdx.x;
+    const int X = B.x * blockDim.x + threadIdx.x;
     if (X < n) {
         double Fe, dF;
         if (embed(E, ts[X], (double)(long long)rho_fx[X] * kRhoUnit, Fe, dF)) atomicOr(status, ST_UNKNOWN_ELEMENT);
         eg = Fe;
     }
     block_add<256>(eg, acc, A_EGROUP, red);
+}
+__global__ void __launch_bounds__(256)
+    embed_energy_half_kernel(int n, const int* __restrict__ ts, const u64* __restrict__ rho_fx,
+                             const __grid_constant__ EmbedParams E, double* __restrict__ acc,
+                             int* __restrict__ status) {
+    embed_energy_half_body(own_blk(), n, ts, rho_fx, E, acc, status);
 }
 
 // ---------------------------------------------------------------------------
@@ -946,19 +991,18 @@ int filter_density_half(simox_ctx* c) {
     stencil_shifts(c, H.F.sh);
     H.splits = std::max(1, std::min(16, c->force_splits));
     H.g0 = c->g0_species;
-    cudaMemsetAsync(c->rho_fx, 0, sizeof(u64) * (size_t)c->n, c->stream);
+    memset_async(c, c->rho_fx, 0, sizeof(u64) * (size_t)c->n, c->stream);
     if (c->n > 0) {
         Launch L(c, "neighbor_filter_density");
         const int g = c->ncell_s * H.splits;
-        filter_half_kernel<<<g, kH1Threads, 0, c->stream>>>(
-            H, c->tab_f, c->xq_s, c->rec_s, c->pair_order, c->cs_start, c->cs_entries,
-            reinterpret_cast<const int2*>(c->nn_s), c->nbr_s, reinterpret_cast<int2*>(c->nn), c->nbr, c->rho_fx,
-            c->status, c->nn_max, c->nn_tot);
+        launch_k<kH1Threads, 3, filter_half_body>(c, filter_half_kernel, g, 0, c->stream, H, c->tab_f, c->xq_s,
+            c->rec_s, c->pair_order, c->cs_start, c->cs_entries, reinterpret_cast<const int2*>(c->nn_s), c->nbr_s,
+            reinterpret_cast<int2*>(c->nn), c->nbr, c->rho_fx, c->status, c->nn_max, c->nn_tot);
     }
     if (c->n > 0) {
         Launch L(c, "eam_embed");
-        embed_half_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->n, c->t_s, c->rho_fx, embed_params(c->pot),
-                                                                     c->rho_s, c->dF_s, c->dF_f, c->status);
+        launch_k<256, 1, embed_half_body>(c, embed_half_kernel, (c->n + 255) / 256, 0, c->stream, c->n, c->t_s,
+            c->rho_fx, embed_params(c->pot), c->rho_s, c->dF_s, c->dF_f, c->status);
     }
     return check_launch(c);
 }
@@ -987,41 +1031,40 @@ int force_half(simox_ctx* c, bool rdf) {
     H.g0 = g0;
     H.n = c->n;
     H.fstride = c->cap;
-    cudaMemsetAsync(c->fx_acc, 0, sizeof(u64) * 3 * (size_t)H.fstride, c->stream);
+    memset_async(c, c->fx_acc, 0, sizeof(u64) * 3 * (size_t)H.fstride, c->stream);
     {
         Launch L(c, "pair_force");
         const int g = c->ncell_s * H.splits;
         if (rdf)
-            force_half_kernel<true><<<g, kH2Threads, kH2Smem, c->stream>>>(
-                H, c->cs_start, c->cs_entries, c->xo_s, c->t_s, reinterpret_cast<const int2*>(c->nn), c->nbr,
-                c->dF_f, c->fx_acc, c->rdf, c->rec_s, c->pair_order, c->status);
+            launch_k<kH2Threads, 1, force_half_body<true>>(c, force_half_kernel<true>, g, kH2Smem, c->stream, H,
+                c->cs_start, c->cs_entries, c->xo_s, c->t_s, reinterpret_cast<const int2*>(c->nn), c->nbr, c->dF_f,
+                c->fx_acc, c->rdf, c->rec_s, c->pair_order, c->status);
         else
-            force_half_kernel<false><<<g, kH2Threads, kH2Smem, c->stream>>>(
-                H, c->cs_start, c->cs_entries, c->xo_s, c->t_s, reinterpret_cast<const int2*>(c->nn), c->nbr,
-                c->dF_f, c->fx_acc, c->rdf, c->rec_s, c->pair_order, c->status);
+            launch_k<kH2Threads, 1, force_half_body<false>>(c, force_half_kernel<false>, g, kH2Smem, c->stream, H,
+                c->cs_start, c->cs_entries, c->xo_s, c->t_s, reinterpret_cast<const int2*>(c->nn), c->nbr, c->dF_f,
+                c->fx_acc, c->rdf, c->rec_s, c->pair_order, c->status);
     }
     {
         Launch L(c, "pair_force_finalize");
-        force_half_finalize_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->n, c->fx_acc, H.fstride,
-                                                                               c->pair_order, c->f);
+        launch_k<256, 1, force_half_finalize_body>(c, force_half_finalize_kernel, (c->n + 255) / 256, 0, c->stream,
+            c->n, c->fx_acc, H.fstride, c->pair_order, c->f);
     }
     return check_launch(c);
 }
 
 int energy_half(simox_ctx* c) {
-    cudaMemsetAsync(c->rho_fx, 0, sizeof(u64) * (size_t)c->n, c->stream);
+    memset_async(c, c->rho_fx, 0, sizeof(u64) * (size_t)c->n, c->stream);
     {
         Launch L(c, "pair_energy_fp64");
         const int wpb = kHEThreads / 32;
         const int g = std::max(1, std::min((c->n + wpb - 1) / wpb, num_sms(c) * 12));
-        energy_half_kernel<<<g, kHEThreads, 0, c->stream>>>(pair_params(c), c->tab_d, c->xq_s, c->t_s,
-                                                           reinterpret_cast<const int2*>(c->nn), c->nbr, c->rho_fx,
-                                                           c->acc, c->status);
+        launch_k<kHEThreads, 6, energy_half_body>(c, energy_half_kernel, g, 0, c->stream, pair_params(c), c->tab_d,
+            c->xq_s, c->t_s, reinterpret_cast<const int2*>(c->nn), c->nbr, c->rho_fx, c->acc, c->status);
     }
     {
         Launch L(c, "eam_embed_energy");
-        embed_energy_half_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->n, c->t_s, c->rho_fx,
-                                                                           embed_params(c->pot), c->acc, c->status);
+        launch_k<256, 1, embed_energy_half_body>(c, embed_energy_half_kernel, (c->n + 255) / 256, 0, c->stream, c->n,
+            c->t_s, c->rho_fx, embed_params(c->pot), c->acc, c->status);
     }
     return check_launch(c);
 }
@@ -1081,7 +1124,7 @@ int ctip_pair_half(simox_ctx* c, const double* vin, double* out, double* cconst,
     if (int st = half_prepare(c->device)) return st;
     const CtipHalfParams C = ctip_half_params(c);
     const int gstride = c->cap;
-    cudaMemsetAsync(c->fx_acc, 0, sizeof(u64) * (cconst ? 2 : 1) * (size_t)gstride, c->stream);
+    memset_async(c, c->fx_acc, 0, sizeof(u64) * (cconst ? 2 : 1) * (size_t)gstride, c->stream);
     const int g = c->ncell_s * C.splits;
     if (cconst)
         ctip_half_kernel<true><<<g, kH2Threads, kHCSmem, c->stream>>>(C, c->cs_start, c->cs_entries, c->frec_s, c->t_s,

@@ -19,6 +19,7 @@
 // as force.f90:406 / ctip.f90:359 do with a default-kind CMPLX().
 #include "simox_internal.cuh"
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <type_traits>
@@ -146,21 +147,38 @@ __device__ __noinline__ void spread_atom_global(const PmeParams& S, double q, co
     }
 }
 
+// The periodic image of grid base b nearest to ref.  The atoms of one cell
+// lie within a third of the box of each other (at least three cells per
+// axis), but VV_NVE1 wraps an atom that crossed a face of the box to the
+// opposite face: taken as is, its base would stretch the cell's patch over
+// the whole grid and send the cell to the global-atomics path.
+__device__ __forceinline__ int near_image(int b, int ref, int K) {
+    const int d = b - ref;
+    return d > K / 2 ? b - K : (d < -(K / 2) ? b + K : b);
+}
+
 template <typename R, int P>
-__global__ void __launch_bounds__(SP_THREADS, sizeof(R) == 8 ? 2 : 3)
-    spread_patch_kernel(PmeParams S, const double4* __restrict__ xq, const double* __restrict__ qalt,
-                        const int* __restrict__ ranges, unsigned long long* __restrict__ acc) {
+__device__ __forceinline__ void spread_patch_body(Blk B, const PmeParams& S, const double4* __restrict__ xq,
+                                                  const double* __restrict__ qalt, const int* __restrict__ ranges,
+                                                  unsigned long long* __restrict__ acc) {
     constexpr bool ROUND = sizeof(R) == 8;   // FP64 grid: the reference's FP32 weight products
     extern __shared__ unsigned sp_words[];  // [SP_CAP] low words, [SP_CAP] high words
-    __shared__ int lo3[3], hi3[3];
-    const int a0 = ranges[blockIdx.x], a1 = ranges[blockIdx.x + 1];
+    __shared__ int lo3[3], hi3[3], ref3[3];
+    const int a0 = ranges[B.x], a1 = ranges[B.x + 1];
     if (a1 <= a0) return;
     const int tid = threadIdx.x;
     if (tid < 3) {
         lo3[tid] = 0x7fffffff;
         hi3[tid] = -0x7fffffff;
+        // bases are taken at the image nearest to the cell's first atom
+        const double4 a = xq[a0];
+        const double x = tid == 0 ? a.x : (tid == 1 ? a.y : a.z);
+        const double L = tid == 0 ? S.box.x : (tid == 1 ? S.box.y : S.box.z);
+        const int K = tid == 0 ? S.K.x : (tid == 1 ? S.K.y : S.K.z);
+        ref3[tid] = __double2int_rz((double)K * (x + L * 0.5) / L) - P / 2 + 1;
     }
     __syncthreads();
+    const int Kd[3] = {S.K.x, S.K.y, S.K.z};
     int mn[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, mx[3] = {-0x7fffffff, -0x7fffffff, -0x7fffffff};
     for (int k = a0 + tid; k < a1; k += SP_THREADS) {
         const double4 a = xq[k];
@@ -171,7 +189,7 @@ __global__ void __launch_bounds__(SP_THREADS, sizeof(R) == 8 ? 2 : 3)
                              (double)S.K.z * (a.z + S.box.z * 0.5) / S.box.z};
 #pragma unroll
         for (int d = 0; d < 3; d++) {
-            const int b = __double2int_rz(u[d]) - P / 2 + 1;
+            const int b = near_image(__double2int_rz(u[d]) - P / 2 + 1, ref3[d], Kd[d]);
             mn[d] = min(mn[d], b);
             mx[d] = max(mx[d], b);
         }
@@ -211,9 +229,9 @@ __global__ void __launch_bounds__(SP_THREADS, sizeof(R) == 8 ? 2 : 3)
         bspline_w<P>(ux, wx, d);
         bspline_w<P>(uy, wy, d);
         bspline_w<P>(uz, wz, d);
-        const int bx = __double2int_rz(ux) - P / 2 + 1;
-        const int by = __double2int_rz(uy) - P / 2 + 1;
-        const int bz = __double2int_rz(uz) - P / 2 + 1;
+        const int bx = near_image(__double2int_rz(ux) - P / 2 + 1, ref3[0], Kd[0]);
+        const int by = near_image(__double2int_rz(uy) - P / 2 + 1, ref3[1], Kd[1]);
+        const int bz = near_image(__double2int_rz(uz) - P / 2 + 1, ref3[2], Kd[2]);
         if (!tiled) {
             spread_atom_global<R, P>(S, q, wx, wy, wz, bx, by, bz, acc);
             continue;
@@ -248,25 +266,37 @@ __global__ void __launch_bounds__(SP_THREADS, sizeof(R) == 8 ? 2 : 3)
         }
     }
 }
+template <typename R, int P>
+__global__ void __launch_bounds__(SP_THREADS, sizeof(R) == 8 ? 2 : 3)
+    spread_patch_kernel(const __grid_constant__ PmeParams S, const double4* __restrict__ xq,
+                        const double* __restrict__ qalt, const int* __restrict__ ranges,
+                        unsigned long long* __restrict__ acc) {
+    spread_patch_body<R, P>(own_blk(), S, xq, qalt, ranges, acc);
+}
 
 // grid = acc in the grid's type; acc cleared for the next spread
 template <typename R>
-__global__ void spread_convert_kernel(size_t n, unsigned long long* __restrict__ acc, R* __restrict__ grid) {
-    const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+__device__ __forceinline__ void spread_convert_body(Blk B, size_t n, unsigned long long* __restrict__ acc,
+                                                    R* __restrict__ grid) {
+    const size_t i = B.x * (size_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     grid[i] = (R)((double)(long long)acc[i] * kSpreadUnit);
     acc[i] = 0ull;
 }
+template <typename R>
+__global__ void spread_convert_kernel(size_t n, unsigned long long* __restrict__ acc, R* __restrict__ grid) {
+    spread_convert_body<R>(own_blk(), n, acc, grid);
+}
 
 // half-spectrum multiply by G/N and energy sum_k G |Q^|^2 (Hermitian weights)
 template <typename R>
-__global__ void __launch_bounds__(256)
-    influence_kernel(size_t nhalf, int kx_half, int K1,
-                     typename std::conditional<sizeof(R) == 8, double2, float2>::type* __restrict__ cg,
-                     const R* __restrict__ infl, double Ngrid, double* __restrict__ acc, int eflag) {
+__device__ __forceinline__ void influence_body(Blk B, size_t nhalf, int kx_half, int K1,
+                                               typename std::conditional<sizeof(R) == 8, double2,
+                                               float2>::type* __restrict__ cg, const R* __restrict__ infl,
+                                               double Ngrid, double* __restrict__ acc, int eflag) {
     __shared__ double red[256 / 32];
     double e = 0.0;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nhalf; i += (size_t)gridDim.x * blockDim.x) {
+    for (size_t i = (size_t)B.x * blockDim.x + threadIdx.x; i < nhalf; i += (size_t)B.n * blockDim.x) {
         const int kx = (int)(i % kx_half);
         auto c = cg[i];
         const R g = infl[i];
@@ -280,14 +310,21 @@ __global__ void __launch_bounds__(256)
     }
     if (eflag) block_add<256>(e * Ngrid, acc, A_EREC, red);
 }
+template <typename R>
+__global__ void __launch_bounds__(256)
+    influence_kernel(size_t nhalf, int kx_half, int K1, typename std::conditional<sizeof(R) == 8, double2,
+                     float2>::type* __restrict__ cg, const R* __restrict__ infl, double Ngrid,
+                     double* __restrict__ acc, int eflag) {
+    influence_body<R>(own_blk(), nhalf, kx_half, K1, cg, infl, Ngrid, acc, eflag);
+}
 
 // gather forces: f[o] += -cst q sum (dW_x W_y W_z kx, ...) Qfin  (force.f90:439-456)
 template <typename R, int P>
-__global__ void __launch_bounds__(128)
-    gather_force_kernel(PmeParams S, const double4* __restrict__ xq, const R* __restrict__ grid,
-                        const int* __restrict__ sorted, double* __restrict__ f, double* __restrict__ acc, int store) {
+__device__ __forceinline__ void gather_force_body(Blk B, const PmeParams& S, const double4* __restrict__ xq,
+                                                  const R* __restrict__ grid, const int* __restrict__ sorted,
+                                                  double* __restrict__ f, double* __restrict__ acc, int store) {
     __shared__ double red[128 / 32];
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = B.x * blockDim.x + threadIdx.x;
     double fo[3] = {0.0, 0.0, 0.0};
     if (k < S.n) {
         const double4 a = xq[k];
@@ -341,6 +378,13 @@ __global__ void __launch_bounds__(128)
     block_add<128>(fo[0], acc, A_FSUM0, red);
     block_add<128>(fo[1], acc, A_FSUM1, red);
     block_add<128>(fo[2], acc, A_FSUM2, red);
+}
+template <typename R, int P>
+__global__ void __launch_bounds__(128)
+    gather_force_kernel(const __grid_constant__ PmeParams S, const double4* __restrict__ xq,
+                        const R* __restrict__ grid, const int* __restrict__ sorted, double* __restrict__ f,
+                        double* __restrict__ acc, int store) {
+    gather_force_body<R, P>(own_blk(), S, xq, grid, sorted, f, acc, store);
 }
 
 // gather potential: phi[k] = scale * sum W Qfin  (ctip.f90:381-393)
@@ -619,16 +663,30 @@ static int run_spread(simox_ctx* c, PmeRes& Rs, const PmeParams& S, const double
         const bool skin = c->using_skin && c->pair_order == c->perm;
         const int* ranges = skin ? c->cs_start : c->cell_start;
         const int nr = skin ? c->ncell_s : c->ncell;
-        spread_patch_kernel<R, P><<<nr, SP_THREADS, 2 * SP_CAP * sizeof(unsigned), c->stream>>>(S, c->xq_s, qalt,
-                                                                                               ranges, Rs.acc);
+        launch_k<SP_THREADS, sizeof(R) == 8 ? 2 : 3, spread_patch_body<R, P>>(c, spread_patch_kernel<R, P>, nr,
+            2 * SP_CAP * sizeof(unsigned), c->stream, S, c->xq_s, qalt, ranges, Rs.acc);
     }
-    spread_convert_kernel<R><<<(unsigned)((c->ngrid + 255) / 256), 256, 0, c->stream>>>(c->ngrid, Rs.acc, (R*)Rs.grid);
+    launch_k<256, 1, spread_convert_body<R>>(c, spread_convert_kernel<R>, (unsigned)((c->ngrid + 255) / 256), 0,
+        c->stream, c->ngrid, Rs.acc, (R*)Rs.grid);
     return check_launch(c);
 }
 
+// an FFT of a recorded step: written down for the batch to issue
+static void record_fft(simox_ctx* c, cufftHandle plan, int kind, void* in, void* out) {
+    RecOp op;
+    op.kind = RecOp::FFT;
+    op.lane = c->rec->lane(c->stream);
+    op.plan = plan;
+    op.fft = kind;
+    op.in = in;
+    op.out = out;
+    c->rec->ops.push_back(std::move(op));
+}
+
 static int run_convolution(simox_ctx* c, PmeRes& Rs, bool eflag) {
-    cufftResult r;
-    {
+    cufftResult r = CUFFT_SUCCESS;
+    if (c->rec) record_fft(c, Rs.r2c, Rs.dbl ? 2 : 0, Rs.grid, Rs.cgrid);
+    else {
         Launch L(c, "pme_fft_r2c");
         if (Rs.dbl) r = cufftExecD2Z(Rs.r2c, (cufftDoubleReal*)Rs.grid, (cufftDoubleComplex*)Rs.cgrid);
         else r = cufftExecR2C(Rs.r2c, (cufftReal*)Rs.grid, (cufftComplex*)Rs.cgrid);
@@ -637,17 +695,16 @@ static int run_convolution(simox_ctx* c, PmeRes& Rs, bool eflag) {
     {
         Launch L(c, "pme_influence");
         int kxh = c->fft[0] / 2 + 1;
-        int g = num_sms(c) * 4;
+        const int g = (int)std::min<size_t>((size_t)num_sms(c) * 4, (c->nhalf + 255) / 256);
         if (Rs.dbl)
-            influence_kernel<double><<<g, 256, 0, c->stream>>>(c->nhalf, kxh, c->fft[0], (double2*)Rs.cgrid,
-                                                               (const double*)Rs.infl, (double)c->ngrid, c->acc,
-                                                               eflag ? 1 : 0);
+            launch_k<256, 1, influence_body<double>>(c, influence_kernel<double>, g, 0, c->stream, c->nhalf, kxh,
+                c->fft[0], (double2*)Rs.cgrid, (const double*)Rs.infl, (double)c->ngrid, c->acc, eflag ? 1 : 0);
         else
-            influence_kernel<float><<<g, 256, 0, c->stream>>>(c->nhalf, kxh, c->fft[0], (float2*)Rs.cgrid,
-                                                              (const float*)Rs.infl, (double)c->ngrid, c->acc,
-                                                              eflag ? 1 : 0);
+            launch_k<256, 1, influence_body<float>>(c, influence_kernel<float>, g, 0, c->stream, c->nhalf, kxh,
+                c->fft[0], (float2*)Rs.cgrid, (const float*)Rs.infl, (double)c->ngrid, c->acc, eflag ? 1 : 0);
     }
-    {
+    if (c->rec) record_fft(c, Rs.c2r, Rs.dbl ? 3 : 1, Rs.cgrid, Rs.grid);
+    else {
         Launch L(c, "pme_fft_c2r");
         if (Rs.dbl) r = cufftExecZ2D(Rs.c2r, (cufftDoubleComplex*)Rs.cgrid, (cufftDoubleReal*)Rs.grid);
         else r = cufftExecC2R(Rs.c2r, (cufftComplex*)Rs.cgrid, (cufftReal*)Rs.grid);
@@ -674,8 +731,8 @@ static int pme_forces_t(simox_ctx* c, PmeRes& Rs, bool eflag, double* f_store) {
     if (!st) st = run_convolution(c, Rs, eflag);
     if (st) return st;
     Launch L(c, "pme_gather_force");
-    gather_force_kernel<R, P><<<(S.n + 127) / 128, 128, 0, c->stream>>>(
-        S, c->xq_s, (const R*)Rs.grid, c->pair_order, f_store ? f_store : c->f, c->acc, f_store ? 1 : 0);
+    launch_k<128, 1, gather_force_body<R, P>>(c, gather_force_kernel<R, P>, (S.n + 127) / 128, 0, c->stream, S,
+        c->xq_s, (const R*)Rs.grid, c->pair_order, f_store ? f_store : c->f, c->acc, f_store ? 1 : 0);
     return SIMOX_OK;
 }
 
@@ -721,7 +778,7 @@ int pme_forces(simox_ctx* c, bool finalize, bool eflag, double* f_store) {
     if (!c->psi_valid) return SIMOX_E_STATE;
     if (int st0 = ensure_gathered(c)) return st0;
     if (c->n == 0) return SIMOX_OK;
-    cudaMemsetAsync(c->acc + A_FSUM0, 0, 3 * sizeof(double), c->stream);
+    memset_async(c, c->acc + A_FSUM0, 0, 3 * sizeof(double), c->stream);
     int st;
     // energies are FP64: a mixed context uses its FP64 twin when they are requested
     PmeRes& Rs = (eflag && c->pme[1].ready) ? c->pme[1] : c->pme[0];

@@ -141,6 +141,7 @@ struct Profile {
 
 namespace sx {
 struct AdjointState;
+struct Recorder;
 }
 
 struct simox_ctx {
@@ -295,6 +296,9 @@ struct simox_ctx {
     int graph_next = 0;
     bool graphs_on = true;
     unsigned long long graph_gen = 0;   // bumped whenever captured launches go stale (drop_graphs)
+    // set while a batch records this context's step: launches, memsets, event
+    // records and waits and FFTs are written down instead of issued
+    sx::Recorder* rec = nullptr;
     double eself = 0.0;         // sys%Eself of the last PME_SELF or CTIP_SOLVER
     int last_max_nnb = 0;
     long long last_tot_nnb = 0;
@@ -438,3 +442,5 @@ __device__ __forceinline__ void block_add(double v, double* acc, int slot, doubl
 __device__ __forceinline__ double dnint(double x) { return round(x); }
 
 }  // namespace sx
+
+#include "simox_batched.cuh"

@@ -5,7 +5,11 @@ change any result.
 
 Bars: FP64 positions within 1e-9 A and energies within 1e-9 relative after 8
 steps (the PME spread's FP64 atomics may add in a different order); mixed
-positions within 1e-6 A; forces for CTA splits 1 and 8 bit-identical.
+positions within 1e-6 A (batched cuFFT plans may round differently from one
+system's plan); forces for CTA splits 1 and 8 bit-identical.  A mixed batch
+runs in the per-pass mode (each kernel of a step launched once for all
+systems); an FP64 batch, whose full-list kernels have no batched form, in the
+per-system mode.
 """
 import numpy as np
 import pytest
@@ -53,6 +57,7 @@ def test_batch_matches_single_systems(precision, tol):
         with api.Batch(members) as b:
             es = b.md_run([_opts(s) for s in systems], 8, first_step=1)
             assert b.launch_count() > 0
+            assert b.mode() == ("per_pass" if precision == "mixed" else "per_system")
         for k, g in enumerate(members):
             x = g.get_state()["x"]
             d = x - alone[k][0]
@@ -126,3 +131,30 @@ def test_batch_follows_changed_step_options():
     finally:
         for g in members:
             g.close()
+
+
+def test_per_pass_and_per_system_batches_agree():
+    """The per-pass graph (one launch per kernel of the step for all systems,
+    batched FFT plans) against the per-system graph of the same members:
+    positions within 1e-6 A after 8 mixed steps and far fewer launches."""
+    systems = _members()
+    runs = {}
+    for mode in ("per_pass", "per_system"):
+        members = [_prepared(s, "mixed") for s in systems]
+        try:
+            with api.Batch(members) as b:
+                b.set_mode(mode)
+                opts = [_opts(s) for s in systems]
+                b.md_run(opts, 2, first_step=1)
+                l0 = b.launch_count()
+                b.md_run(opts, 6, first_step=3)
+                assert b.mode() == mode
+                runs[mode] = ([g.get_state()["x"] for g in members], (b.launch_count() - l0) / 6)
+        finally:
+            for g in members:
+                g.close()
+    for k, s in enumerate(systems):
+        d = runs["per_pass"][0][k] - runs["per_system"][0][k]
+        d -= s.box * np.round(d / s.box)
+        assert np.abs(d).max() <= 1e-6, (k, np.abs(d).max())
+    assert runs["per_pass"][1] < 0.6 * runs["per_system"][1], (runs["per_pass"][1], runs["per_system"][1])
