@@ -477,11 +477,44 @@ def batch_object(nsys, steps, sequential=True):
     return out
 
 
+def batch_profile(nsys, mode):
+    """--batch N --ncu: the batch set up as in batch_object (no autotuning),
+    its step graphs captured, then ONE step without energies between
+    cudaProfilerStart and cudaProfilerStop (ncu --profile-from-start off)."""
+    import torch
+    from simox_b200 import api, systems as S
+    systems = S.replica_batch(seed=7, nsys=nsys)
+    dt = 1.0 / S.TFM
+    members = []
+    for s in systems:
+        g = api.from_system(s, precision="mixed")
+        g.pme_self()
+        g.cell_sort()
+        g.force()
+        g.pme()
+        members.append(g)
+    opts = [api.md_opts(dt, thermostat=True, T_given=s.meta["T"] * S.KB, freq_stat=10) for s in systems]
+    b = api.Batch(members)
+    b.set_mode(mode)
+    b.md_run(opts, 14, first_step=1)          # eager first step, both step graphs captured
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    b.md_run(opts, 1, first_step=15)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    b.close()
+    for g in members:
+        g.close()
+
+
 def run_batch(args):
     """--batch N: the batched-replica workload alone (256 systems in its
     configuration).  Not the headline metric."""
     from simox_b200 import build
     build.build()
+    if args.ncu:
+        batch_profile(args.batch, args.batch_mode)
+        return 0
     o = batch_object(args.batch, args.steps)
     line = {"metric": o.pop("metric"), "value": o.pop("value"), "unit": UNIT, "n_gpus": 1,
             "steps": o.pop("steps"), "higher_is_better": True, "dtype": "f32+f64", "data": "synthetic",
@@ -652,6 +685,8 @@ def main():
                     help="--ncu: energies on steps with MOD(step, freq_stat) == 0 (1: every step)")
     ap.add_argument("--batch", type=int, default=0,
                     help="run the batched-replica workload with this many systems (256 in its configuration)")
+    ap.add_argument("--batch-mode", default="per_pass", choices=["per_pass", "per_system"],
+                    help="--batch with --ncu: the batch mode of the profiled step")
     ap.add_argument("--adjoint", type=int, default=0,
                     help="run the parameter-gradient workload with this many snapshots (32 in its configuration)")
     ap.add_argument("--no-ctip", action="store_true", help="skip the timed CTIP re-solves")
