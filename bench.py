@@ -691,7 +691,7 @@ def main():
                     help="run the parameter-gradient workload with this many snapshots (32 in its configuration)")
     ap.add_argument("--no-ctip", action="store_true", help="skip the timed CTIP re-solves")
     ap.add_argument("--no-extras", action="store_true",
-                    help="skip the 32-system batch and 32-snapshot adjoint objects of the default line")
+                    help="skip the 256-system batch and 32-snapshot adjoint objects of the default line")
     ap.add_argument("--c3", action="store_true",
                     help="add the 472k oxidation slab with the charge solve on every step")
     args = ap.parse_args()
@@ -818,7 +818,7 @@ def main():
 
     extras = {}
     if rank == 0 and world == 1 and not args.no_extras:
-        extras["batch"] = batch_object(32, 20, sequential=True)
+        extras["batch"] = batch_object(256, 20, sequential=True)
         extras["adjoint"] = adjoint_object(32, sequential=False)
         if args.c3:
             extras["slab_charges_every_step"] = c3_object(steps=2, device=local)
