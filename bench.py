@@ -68,6 +68,12 @@ def reduce_max(dist, v, device=None):
     return float(t.item())
 
 
+def replicas_value(world, n_atoms, steps, ms_max):
+    """Whole-job atom-steps/s of `world` independent replicas of n_atoms,
+    each timed over `steps` steps, from the slowest rank's milliseconds."""
+    return world * n_atoms * steps / (ms_max / 1e3)
+
+
 def barrier(dist, device=None):
     if dist is None:
         return
@@ -626,7 +632,8 @@ def ctip_object(g, label):
     prof = g.profile_read()
     g.profile(False)
     it = max(rep2["n_cg"], 1)
-    out["kernels_ms_per_cg_iteration"] = {k: round(v[0] / it, 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
+    out["kernels_ms_per_cg_iteration"] = {k: round(v[0] / it, 4)
+                                          for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
     out["kernels_note"] = f"host-driven loop, {it} iterations, event span per launch family"
     g.set_state(q=q1)
     return out
@@ -738,7 +745,7 @@ def main():
     rebuilds = time_device.rebuilds
     clk = clocks.stop()
     ms_max = reduce_max(dist, ms, device)
-    value = world * s.n * args.steps / (ms_max / 1e3)
+    value = replicas_value(world, s.n, args.steps, ms_max)
     mx_nnb, tot_nnb = g.neighbor_stats()
     half = g.get_tuning().get("half_list", 0) == 1
     if half:   # the statistics count pairs: both atoms' rows would hold each once
@@ -748,7 +755,7 @@ def main():
     # e2e through the C ABI with host buffers
     e2e_s, nbytes = time_e2e(g, s, max(3, args.steps // 2), args.warmup + args.steps + 1)
     e2e_s = reduce_max(dist, e2e_s, device)
-    e2e_val = world * s.n * max(3, args.steps // 2) / e2e_s
+    e2e_val = replicas_value(world, s.n, max(3, args.steps // 2), e2e_s * 1e3)
 
     # per-kernel profile (separate pass; event-bracketed launches)
     nprof = min(args.steps, 5)
@@ -804,7 +811,7 @@ def main():
             ctip_fp64 = ctip_object(g64, "fp64")
         g64.close()
         ms64 = reduce_max(dist, ms64, device)
-        fp64 = {"value": world * s.n * args.steps / (ms64 / 1e3), "unit": UNIT, "ms_per_step": ms64 / args.steps,
+        fp64 = {"value": replicas_value(world, s.n, args.steps, ms64), "unit": UNIT, "ms_per_step": ms64 / args.steps,
                 "skin_rebuilds_in_timed_steps": time_device.rebuilds}
 
     ferr = force_error(s, device=local)
