@@ -253,8 +253,12 @@ const FftGroup* fft_group_of(const FftPool& pool, const sx::RecOp& op, int k, in
 int capture_per_pass(simox_batch* b, const simox_md_opts* o, bool sort, bool estep, FftPool& pool,
                      simox_batch::G& out) {
     const int nsys = (int)b->ctx.size();
-    if (pool.groups.empty())
-        if (int st = make_fft_groups(b, pool)) return st;
+    // without the batched plans' buffers (no memory for them, or a plan
+    // cuFFT refuses) every member's FFTs run on its own plan
+    if (pool.groups.empty() && make_fft_groups(b, pool) != SIMOX_OK) {
+        pool.release();
+        cudaGetLastError();
+    }
     // record with the members' grids lent from the batched plans' buffers
     std::vector<sx::Recorder> rec(nsys);
     bool ok = true;
