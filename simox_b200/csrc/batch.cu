@@ -238,7 +238,9 @@ const FftGroup* fft_group_of(const FftPool& pool, const sx::RecOp& op, int k, in
             const char* re = static_cast<const char*>(g.real) + j * g.ngrid * es;
             const char* cx = static_cast<const char*>(g.cplx) + j * g.nhalf * 2 * es;
             const bool fwd = op.fft == 0 || op.fft == 2;
-            if (op.in == (fwd ? (const void*)re : (const void*)cx) && op.out == (fwd ? (const void*)cx : (const void*)re)) {
+            const void* src = fwd ? (const void*)re : (const void*)cx;
+            const void* dst = fwd ? (const void*)cx : (const void*)re;
+            if (op.in == src && op.out == dst) {
                 *slot = (int)j;
                 return &g;
             }
@@ -559,7 +561,8 @@ extern "C" int simox_batch_create(int nsys, simox_ctx* const* ctxs, simox_batch*
               cudaEventCreateWithFlags(&b->lane_ev[1], cudaEventDisableTiming) == cudaSuccess &&
               cudaEventCreate(&b->t0) == cudaSuccess && cudaEventCreate(&b->t1) == cudaSuccess;
     b->join.assign(nsys, nullptr);
-    for (int k = 0; ok && k < nsys; k++) ok = cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming) == cudaSuccess;
+    for (int k = 0; ok && k < nsys; k++)
+        ok = cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming) == cudaSuccess;
     if (!ok) {
         simox_batch_destroy(b);
         return SIMOX_E_CUDA;
