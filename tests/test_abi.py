@@ -73,3 +73,30 @@ def test_adjoint_eval_many_argument_checks(simox_lib):
     assert simox_lib.simox_adjoint_eval_many(arr, 2, None, None, None, None, None, 0) == _abi.SIMOX_E_ARG
     arr = (_vp * 2)(fake, None)
     assert simox_lib.simox_adjoint_eval_many(arr, 2, None, None, None, None, None, 0) == _abi.SIMOX_E_ARG
+
+
+def test_batch_entry_points_argument_checks(simox_lib):
+    """Host-side checks of the batch entry points (no context or device is
+    touched): E_ARG for no members, a NULL member, a NULL batch, an unknown
+    mode."""
+    import ctypes as C
+    from simox_b200.api import Batch, _vp
+    out = _vp()
+    assert simox_lib.simox_batch_create(0, None, C.byref(out)) == _abi.SIMOX_E_ARG
+    assert simox_lib.simox_batch_create(1, (_vp * 1)(None), C.byref(out)) == _abi.SIMOX_E_ARG
+    assert simox_lib.simox_batch_destroy(None) == _abi.SIMOX_E_ARG
+    assert simox_lib.simox_batch_md_run(None, None, 1, 1, None) == _abi.SIMOX_E_ARG
+    assert simox_lib.simox_batch_set_mode(None, Batch.MODES["per_pass"]) == _abi.SIMOX_E_ARG
+    m = C.c_int(-1)
+    assert simox_lib.simox_batch_get_mode(None, C.byref(m)) == _abi.SIMOX_E_ARG
+    n = C.c_longlong(0)
+    assert simox_lib.simox_batch_launch_count(None, C.byref(n)) == _abi.SIMOX_E_ARG
+    assert sorted(Batch.MODES.values()) == [0, 1]
+
+
+def test_batch_mode_constants_match_header():
+    from simox_b200.api import Batch
+    txt = open(HEADER).read()
+    vals = dict(re.findall(r"\b(SIMOX_BATCH_PER_\w+)\s*=\s*(\d+)", txt))
+    assert {k: int(v) for k, v in vals.items()} == {"SIMOX_BATCH_PER_PASS": Batch.MODES["per_pass"],
+                                                     "SIMOX_BATCH_PER_SYSTEM": Batch.MODES["per_system"]}
