@@ -825,10 +825,17 @@ def main():
 
     extras = {}
     if rank == 0 and world == 1 and not args.no_extras:
-        extras["batch"] = batch_object(256, 20, sequential=True)
-        extras["adjoint"] = adjoint_object(32, sequential=False)
+        # the headline is measured by now: a failing side workload is reported
+        # in its object instead of costing the whole line
+        jobs = [("batch", lambda: batch_object(256, 20, sequential=True)),
+                ("adjoint", lambda: adjoint_object(32, sequential=False))]
         if args.c3:
-            extras["slab_charges_every_step"] = c3_object(steps=2, device=local)
+            jobs.append(("slab_charges_every_step", lambda: c3_object(steps=2, device=local)))
+        for key, job in jobs:
+            try:
+                extras[key] = job()
+            except Exception as exc:   # noqa: BLE001 - reported, not hidden
+                extras[key] = {"error": f"{type(exc).__name__}: {exc}"}
 
     if rank == 0:
         line = {
