@@ -559,8 +559,11 @@ def adjoint_eval_many(ctxs, targets=None, threads: int = 0, gradients: bool = Tr
 
 class Batch:
     """Independent systems advanced together: one CUDA graph launch per MD
-    step for all of them (simox_batch_*).  The member contexts stay owned by
-    the caller and must outlive the batch."""
+    step for all of them (simox_batch_*).  By default each kernel of the step
+    is launched once for all systems ("per_pass"); members whose steps take
+    different kernel sequences run as one graph branch per system
+    ("per_system").  The member contexts stay owned by the caller and must
+    outlive the batch."""
 
     def __init__(self, members):
         self.members = list(members)
